@@ -1,0 +1,391 @@
+// libcatn_b200: C ABI over the device engine (engine.cuh).
+//
+// One persistent kernel runs every instance of a launch: each CTA owns one
+// "slot" of HBM (control state + tensor arena), pulls instance ids from a
+// device-side atomic work queue and contracts them start to finish.  A
+// single network (catn_net) is the same kernel with one instance and one
+// slot that stays resident afterwards for result_tensor.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "engine.cuh"
+#include "host_image.h"
+
+using namespace catn;
+
+namespace {
+
+thread_local std::string g_err;
+
+catn_status fail(catn_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+catn_status cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return CATN_ECUDA;
+}
+#define CUDA_TRY(expr)                                   \
+  do {                                                   \
+    cudaError_t _e = (expr);                             \
+    if (_e != cudaSuccess) return cuda_fail(_e, #expr);  \
+  } while (0)
+
+const char* status_text(int s) {
+  switch (s) {
+    case CATN_OK: return "ok";
+    case CATN_EINVAL: return "invalid argument";
+    case CATN_ENOMEM: return "device arena or control capacity exhausted";
+    case CATN_ENOCONV: return "Jacobi SVD did not converge";
+    case CATN_ETIMEOUT: return "device wait timed out";
+    case CATN_ECUDA: return "CUDA error";
+    case CATN_ESTATE: return "reference error path (invalid network state)";
+  }
+  return "unknown";
+}
+
+constexpr int kThreads = 256;
+constexpr int kSmemBytes = 64 * 8 + GEMM_STAGE_BYTES;
+
+__global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
+    const InstDesc* __restrict__ descs, int ninst, const long long* i64, const int* i32, const double* dat,
+    char* slots, SlotLayout L, catn_result* res, int* trace, int* queue) {
+  extern __shared__ double smem[];
+  Team T;
+  T.red = smem;
+  T.stage = (char*)(smem + 64);
+  T.stage_bytes = GEMM_STAGE_BYTES;
+  char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
+  for (;;) {
+    long long inst = 0;
+    if (threadIdx.x == 0) inst = atomicAdd(queue, 1);
+    inst = T.bcast(inst);
+    if (inst >= ninst) break;
+    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
+    char* slot, SlotLayout L, catn_params P, int n, double* out, long long cap, long long* meta) {
+  extern __shared__ double smem[];
+  Team T;
+  T.red = smem;
+  T.stage = (char*)(smem + 64);
+  T.stage_bytes = GEMM_STAGE_BYTES;
+  Ctx C = make_ctx(T, slot, L, P, n);
+  int nd = 0;
+  long long dims[64];
+  long long tot = result_tensor_dev(C, out, cap, dims, &nd);
+  if (threadIdx.x == 0) {
+    meta[0] = tot;
+    meta[1] = nd;
+    meta[2] = C.ctl[CTL_STATUS];
+    for (int q = 0; q < nd && q < 64; ++q) meta[3 + q] = dims[q];
+  }
+}
+
+// Device copy of an Image plus slots and results.
+struct DeviceRun {
+  InstDesc* d_desc = nullptr;
+  long long* d_i64 = nullptr;
+  int* d_i32 = nullptr;
+  double* d_dat = nullptr;
+  char* d_slots = nullptr;
+  catn_result* d_res = nullptr;
+  int* d_trace = nullptr;
+  int* d_queue = nullptr;
+  SlotLayout L;
+  int nslots = 0;
+  int ninst = 0;
+  long long input_bytes = 0;
+
+  void release() {
+    cudaFree(d_desc); cudaFree(d_i64); cudaFree(d_i32); cudaFree(d_dat);
+    cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
+    d_desc = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
+    d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
+  }
+};
+
+catn_status prepare(const Image& im, long long arena_bytes, int max_slots, DeviceRun& R) {
+  R.ninst = (int)im.desc.size();
+  if (R.ninst == 0) return fail(CATN_EINVAL, "no instances");
+  R.L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
+  int dev = 0, nsm = 0, per_sm = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  CUDA_TRY(cudaFuncSetAttribute(catn_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, catn_persistent_kernel, kThreads, kSmemBytes));
+  if (per_sm < 1) per_sm = 1;
+  long long resident = (long long)nsm * per_sm;
+  long long ns = R.ninst < resident ? R.ninst : resident;
+  if (max_slots > 0 && ns > max_slots) ns = max_slots;
+  size_t freeb = 0, totalb = 0;
+  CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+  long long budget = (long long)(freeb * 0.85);
+  if (ns * R.L.slot_bytes > budget) ns = budget / R.L.slot_bytes;
+  if (ns < 1) return fail(CATN_ENOMEM, "not enough device memory for one slot");
+  R.nslots = (int)ns;
+  CUDA_TRY(cudaMalloc(&R.d_desc, sizeof(InstDesc) * im.desc.size()));
+  CUDA_TRY(cudaMalloc(&R.d_i64, sizeof(long long) * (im.i64.size() + 1)));
+  CUDA_TRY(cudaMalloc(&R.d_i32, sizeof(int) * (im.i32.size() + 1)));
+  CUDA_TRY(cudaMalloc(&R.d_dat, sizeof(double) * (im.dat.size() + 1)));
+  CUDA_TRY(cudaMalloc(&R.d_slots, (size_t)(R.L.slot_bytes * ns)));
+  CUDA_TRY(cudaMalloc(&R.d_res, sizeof(catn_result) * im.desc.size()));
+  CUDA_TRY(cudaMalloc(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
+  CUDA_TRY(cudaMalloc(&R.d_queue, sizeof(int)));
+  R.input_bytes = (long long)(sizeof(InstDesc) * im.desc.size() + sizeof(long long) * im.i64.size() +
+                              sizeof(int) * im.i32.size() + sizeof(double) * im.dat.size());
+  return CATN_OK;
+}
+
+catn_status upload(const Image& im, DeviceRun& R, cudaStream_t st) {
+  CUDA_TRY(cudaMemcpyAsync(R.d_desc, im.desc.data(), sizeof(InstDesc) * im.desc.size(), cudaMemcpyHostToDevice, st));
+  if (!im.i64.empty())
+    CUDA_TRY(cudaMemcpyAsync(R.d_i64, im.i64.data(), sizeof(long long) * im.i64.size(), cudaMemcpyHostToDevice, st));
+  if (!im.i32.empty())
+    CUDA_TRY(cudaMemcpyAsync(R.d_i32, im.i32.data(), sizeof(int) * im.i32.size(), cudaMemcpyHostToDevice, st));
+  if (!im.dat.empty())
+    CUDA_TRY(cudaMemcpyAsync(R.d_dat, im.dat.data(), sizeof(double) * im.dat.size(), cudaMemcpyHostToDevice, st));
+  return CATN_OK;
+}
+
+catn_status launch(DeviceRun& R, cudaStream_t st) {
+  CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, sizeof(int), st));
+  catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.ninst, R.d_i64, R.d_i32, R.d_dat,
+                                                                R.d_slots, R.L, R.d_res, R.d_trace, R.d_queue);
+  CUDA_TRY(cudaGetLastError());
+  return CATN_OK;
+}
+
+}  // namespace
+
+struct catn_net {
+  Image im;
+  DeviceRun R;
+  bool contracted = false;
+};
+
+struct catn_batch {
+  Image im;
+  DeviceRun R;
+};
+
+extern "C" {
+
+void catn_params_default(catn_params* p) {
+  if (!p) return;
+  p->Dmax = 32;
+  p->chi = 32;
+  p->cutoff = 1e-15;
+  p->norm_method = 1;
+  p->select = 1;
+  p->reverse = 1;
+  p->svdopt = 1;
+  p->swapopt = 1;
+  p->compress = 0;
+  p->cut_bond = 0;
+  p->seed = 1;
+  p->trace = 0;
+}
+
+static catn_status check_params(const catn_params* p) {
+  if (!p) return fail(CATN_EINVAL, "params is NULL");
+  if (p->chi < 1) return fail(CATN_EINVAL, "chi must be >= 1");
+  if (p->Dmax == 0) return fail(CATN_EINVAL, "Dmax must be nonzero (negative = exact mode)");
+  if (p->norm_method < 0 || p->norm_method > 2) return fail(CATN_EINVAL, "norm_method must be 0, 1 or 2");
+  if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
+  if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
+  return CATN_OK;
+}
+
+static long long default_arena(long long a) { return a > 0 ? a : (1LL << 30); }
+
+static catn_status net_finish(catn_net* net, long long arena_bytes, catn_net** out) {
+  catn_status s = prepare(net->im, default_arena(arena_bytes), 1, net->R);
+  if (s != CATN_OK) {
+    net->R.release();
+    delete net;
+    return s;
+  }
+  *out = net;
+  return CATN_OK;
+}
+
+catn_status catn_net_create_mps(const catn_params* p, int32_t n_nodes, const int32_t* site_counts,
+                                const int32_t* nbr_counts, const int32_t* canos, const int64_t* site_dims,
+                                const double* site_data, const int32_t* neighbors, int64_t arena_bytes,
+                                catn_net** out) {
+  if (catn_status s = check_params(p)) return s;
+  if (!out || !site_counts || !nbr_counts || !canos) return fail(CATN_EINVAL, "NULL argument");
+  catn_net* net = new catn_net();
+  int tc = p->trace ? 4 * 1024 * 64 : 0;
+  long long nsite = 0;
+  for (int k = 0; k < n_nodes; ++k) nsite += site_counts[k];
+  if (p->trace) tc = (int)(nsite + 16);
+  std::string e = net->im.add_mps(*p, n_nodes, site_counts, nbr_counts, canos, (const long long*)site_dims,
+                                  site_data, neighbors, tc);
+  if (!e.empty()) { delete net; return fail(CATN_EINVAL, e); }
+  return net_finish(net, arena_bytes, out);
+}
+
+catn_status catn_net_create_dense(const catn_params* p, int32_t n_nodes, const int32_t* ndims, const int64_t* dims,
+                                  const double* data, const int32_t* neighbors, int64_t arena_bytes,
+                                  catn_net** out) {
+  if (catn_status s = check_params(p)) return s;
+  if (!out || !ndims) return fail(CATN_EINVAL, "NULL argument");
+  catn_net* net = new catn_net();
+  long long legs = 0;
+  for (int k = 0; k < n_nodes; ++k) legs += ndims[k];
+  int tc = p->trace ? (int)(legs + 16) : 0;
+  std::string e = net->im.add_dense(*p, n_nodes, ndims, (const long long*)dims, data, neighbors, tc);
+  if (!e.empty()) { delete net; return fail(CATN_EINVAL, e); }
+  return net_finish(net, arena_bytes, out);
+}
+
+catn_status catn_ising_create(const catn_params* p, int32_t n, int32_t n_edges, const int32_t* edges,
+                              const double* weights, const double* fields, double beta, int32_t pos1,
+                              int32_t val1, int32_t pos2, int32_t val2, int64_t arena_bytes, catn_net** out) {
+  if (catn_status s = check_params(p)) return s;
+  if (!out || (n_edges > 0 && (!edges || !weights)) || !fields) return fail(CATN_EINVAL, "NULL argument");
+  catn_net* net = new catn_net();
+  int tc = p->trace ? 2 * n_edges + 16 : 0;
+  std::string e = net->im.add_ising(*p, n, n_edges, edges, weights, fields, beta, pos1, val1, pos2, val2, tc);
+  if (!e.empty()) { delete net; return fail(CATN_EINVAL, e); }
+  return net_finish(net, arena_bytes, out);
+}
+
+catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32_t trace_cap) {
+  if (!net || !res) return fail(CATN_EINVAL, "NULL argument");
+  if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
+  cudaStream_t st = 0;
+  if (catn_status s = upload(net->im, net->R, st)) return s;
+  if (catn_status s = launch(net->R, st)) return s;
+  CUDA_TRY(cudaMemcpyAsync(res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  net->contracted = true;
+  if (trace && trace_cap > 0 && net->im.desc[0].trace_cap > 0) {
+    int cnt = res->nsteps < trace_cap ? res->nsteps : trace_cap;
+    if (cnt > net->im.desc[0].trace_cap) cnt = net->im.desc[0].trace_cap;
+    if (cnt > 0) CUDA_TRY(cudaMemcpy(trace, net->R.d_trace, sizeof(int) * 8 * cnt, cudaMemcpyDeviceToHost));
+  }
+  if (res->status != CATN_OK) return fail((catn_status)res->status, std::string("contraction failed: ") + status_text(res->status));
+  return CATN_OK;
+}
+
+catn_status catn_result_tensor(catn_net* net, double* out, int64_t cap, int64_t* numel, int32_t* ndim, int64_t* dims) {
+  if (!net || !numel || !ndim) return fail(CATN_EINVAL, "NULL argument");
+  if (!net->contracted) return fail(CATN_ESTATE, "result_tensor before contraction!");
+  long long total_cap = cap > 0 ? cap : 0;
+  double* d_out = nullptr;
+  long long* d_meta = nullptr;
+  CUDA_TRY(cudaMalloc(&d_meta, sizeof(long long) * 80));
+  if (total_cap > 0) CUDA_TRY(cudaMalloc(&d_out, sizeof(double) * total_cap));
+  cudaFuncSetAttribute(catn_result_tensor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+  catn_result_tensor_kernel<<<1, kThreads, kSmemBytes>>>(net->R.d_slots, net->R.L, net->im.desc[0].P,
+                                                        net->im.desc[0].n, d_out, total_cap, d_meta);
+  cudaError_t e = cudaGetLastError();
+  long long meta[80];
+  if (e == cudaSuccess) e = cudaMemcpy(meta, d_meta, sizeof(meta), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && out && meta[0] > 0 && meta[0] <= total_cap)
+    e = cudaMemcpy(out, d_out, sizeof(double) * meta[0], cudaMemcpyDeviceToHost);
+  cudaFree(d_out);
+  cudaFree(d_meta);
+  if (e != cudaSuccess) return cuda_fail(e, "result_tensor");
+  if (meta[0] < 0 || meta[2] != 0)
+    return fail(CATN_ESTATE, "result_tensor: expected one surviving open-leg node");
+  *numel = meta[0] == 0 ? 1 : meta[0];
+  *ndim = (int)meta[1];
+  for (int q = 0; q < meta[1] && q < 64; ++q)
+    if (dims) dims[q] = meta[3 + q];
+  if (meta[0] == 0 && out && cap >= 1) out[0] = 1.0;   // closed network: 0-d one()
+  return CATN_OK;
+}
+
+catn_status catn_net_destroy(catn_net* net) {
+  if (!net) return CATN_OK;
+  net->R.release();
+  delete net;
+  return CATN_OK;
+}
+
+catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const int32_t* n_nodes,
+                                    const int64_t* node_off, const int64_t* edge_off, const int32_t* edges,
+                                    const double* weights, const double* fields, const double* betas,
+                                    const int32_t* pins, int64_t slot_arena_bytes, int32_t max_slots,
+                                    catn_batch** out) {
+  if (catn_status s = check_params(p)) return s;
+  if (!out || n_inst < 1 || !n_nodes || !node_off || !edge_off || !fields || !betas)
+    return fail(CATN_EINVAL, "bad batch arguments");
+  catn_batch* b = new catn_batch();
+  for (int q = 0; q < n_inst; ++q) {
+    long long e0 = edge_off[q], e1 = edge_off[q + 1];
+    int ne = (int)(e1 - e0);
+    int pos1 = 0, val1 = 0, pos2 = 0, val2 = 0;
+    if (pins) { pos1 = pins[4 * q]; val1 = pins[4 * q + 1]; pos2 = pins[4 * q + 2]; val2 = pins[4 * q + 3]; }
+    int tc = p->trace ? 2 * ne + 16 : 0;
+    std::string e = b->im.add_ising(*p, n_nodes[q], ne, edges + 2 * e0, weights + e0, fields + node_off[q],
+                                    betas[q], pos1, val1, pos2, val2, tc);
+    if (!e.empty()) { delete b; return fail(CATN_EINVAL, "instance " + std::to_string(q) + ": " + e); }
+  }
+  long long arena = slot_arena_bytes > 0 ? slot_arena_bytes : (128LL << 20);
+  if (catn_status s = prepare(b->im, arena, max_slots, b->R)) {
+    b->R.release();
+    delete b;
+    return s;
+  }
+  *out = b;
+  return CATN_OK;
+}
+
+catn_status catn_batch_upload(catn_batch* b, void* stream) {
+  if (!b) return fail(CATN_EINVAL, "NULL batch");
+  return upload(b->im, b->R, (cudaStream_t)stream);
+}
+
+catn_status catn_batch_launch(catn_batch* b, void* stream) {
+  if (!b) return fail(CATN_EINVAL, "NULL batch");
+  return launch(b->R, (cudaStream_t)stream);
+}
+
+catn_status catn_batch_results(catn_batch* b, catn_result* results, void* stream) {
+  if (!b || !results) return fail(CATN_EINVAL, "NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  CUDA_TRY(cudaMemcpyAsync(results, b->R.d_res, sizeof(catn_result) * b->R.ninst, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  for (int q = 0; q < b->R.ninst; ++q)
+    if (results[q].status != CATN_OK)
+      return fail((catn_status)results[q].status,
+                  "instance " + std::to_string(q) + " failed: " + status_text(results[q].status));
+  return CATN_OK;
+}
+
+catn_status catn_batch_run(catn_batch* b, catn_result* results) {
+  if (catn_status s = catn_batch_upload(b, nullptr)) return s;
+  if (catn_status s = catn_batch_launch(b, nullptr)) return s;
+  return catn_batch_results(b, results, nullptr);
+}
+
+int32_t catn_batch_slots(const catn_batch* b) { return b ? b->R.nslots : 0; }
+int64_t catn_batch_input_bytes(const catn_batch* b) { return b ? b->R.input_bytes : 0; }
+
+catn_status catn_batch_destroy(catn_batch* b) {
+  if (!b) return CATN_OK;
+  b->R.release();
+  delete b;
+  return CATN_OK;
+}
+
+size_t catn_last_error(char* buf, size_t cap) {
+  if (!buf || cap == 0) return g_err.size();
+  size_t n = g_err.size() < cap - 1 ? g_err.size() : cap - 1;
+  std::memcpy(buf, g_err.data(), n);
+  buf[n] = '\0';
+  return n;
+}
+
+const char* catn_version(void) { return "catn_b200 0.1 (sm_100a, fp64 engine)"; }
+
+}  // extern "C"

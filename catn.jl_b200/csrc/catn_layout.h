@@ -1,0 +1,99 @@
+// Internal data layout shared by the host side of libcatn_b200 and the
+// device engine: per-instance input images, per-CTA slot layout, and the
+// control words of one running instance.
+#pragma once
+#include <stdint.h>
+#include "catn_b200.h"
+
+namespace catn {
+
+constexpr int CATN_NCLS = 40;      // arena size classes: 64 B << c
+constexpr int CATN_CMAX = 8192;    // edge-cost buckets (log2 sizes)
+
+struct NodeHdr {
+  int nsites;
+  int nnbr;
+  int cano;
+  int pad;
+};
+
+struct SiteRef {
+  int dl, d, dr, pad;
+  long long off;   // byte offset of the (dl, d, dr) column-major tensor in the arena
+};
+
+struct EdgeEnt {
+  int cost, i, j, next, prev, alive;
+};
+
+// Control words of a running instance.
+enum {
+  CTL_STATUS = 0,   // catn_status
+  CTL_MINC = 1,     // lowest possibly non-empty cost bucket
+  CTL_FREEENT = 2,  // head of the free entry list
+  CTL_JACMAX = 3,   // max Jacobi sweeps seen
+  CTL_NSTEPS = 4,
+  CTL_ANOMALY = 5,  // bucket bookkeeping anomaly counter (diagnostic)
+  CTL_WORDS = 8
+};
+
+// One instance of the input image.
+struct InstDesc {
+  catn_params P;
+  int n;            // nodes
+  int kind;         // 0 = MPS form, 1 = dense tensors (raw2mps on device)
+  long long hdr_off;   // int64 image: per node 4 words
+                       //   MPS:   nsites, nnbr, cano, 0
+                       //   dense: ndims, nnbr(=ndims), 0, 0
+  long long dim_off;   // int64 image: MPS: 3 per site; dense: ndims per node
+  long long nbr_off;   // int32 image: neighbours, nodes in order
+  long long data_off;  // double image: tensors in order
+  long long data_len;
+  int trace_cap;       // records of 8 int32 (0 = no trace)
+  int pad;
+  long long trace_off; // int32 offset into the trace buffer
+};
+
+// Byte layout of one CTA slot (control state + arena).
+struct SlotLayout {
+  int nmax, maxs, ecap, pcap;
+  long long off_node, off_site, off_nbr, off_ent, off_bhead, off_btail, off_bcnt, off_emap;
+  long long off_ctl, off_pairs, off_list, off_tmp, off_ameta, off_arena;
+  int lcap, pad;
+  long long arena_bytes, slot_bytes;
+};
+
+inline long long align256(long long x) { return (x + 255) & ~255LL; }
+
+inline SlotLayout make_layout(int nmax, int maxs, int ecap, long long arena_bytes) {
+  SlotLayout L;
+  L.nmax = nmax;
+  L.maxs = maxs;
+  L.ecap = ecap;
+  long long pc = (long long)maxs * (maxs + 1);
+  if (pc < 2LL * ecap) pc = 2LL * ecap;
+  L.pcap = (int)(pc + 64);
+  L.lcap = (nmax + 1 > 2 * maxs + 2 ? nmax + 1 : 2 * maxs + 2) + 16;
+  L.pad = 0;
+  long long o = 0;
+  long long nn = (long long)nmax + 1;
+  L.off_node = o;  o = align256(o + nn * (long long)sizeof(NodeHdr));
+  L.off_site = o;  o = align256(o + nn * maxs * (long long)sizeof(SiteRef));
+  L.off_nbr = o;   o = align256(o + nn * maxs * 4LL);
+  L.off_ent = o;   o = align256(o + (long long)ecap * (long long)sizeof(EdgeEnt));
+  L.off_bhead = o; o = align256(o + CATN_CMAX * 4LL);
+  L.off_btail = o; o = align256(o + CATN_CMAX * 4LL);
+  L.off_bcnt = o;  o = align256(o + CATN_CMAX * 4LL);
+  L.off_emap = o;  o = align256(o + nn * nn * 4LL);
+  L.off_ctl = o;   o = align256(o + CTL_WORDS * 4LL);
+  L.off_pairs = o; o = align256(o + (long long)L.pcap * 8LL);
+  L.off_list = o;  o = align256(o + (long long)L.lcap * 4LL);
+  L.off_tmp = o;   o = align256(o + (2LL * maxs + 8) * 4LL);
+  L.off_ameta = o; o = align256(o + (CATN_NCLS + 2) * 8LL);
+  L.off_arena = o;
+  L.arena_bytes = arena_bytes;
+  L.slot_bytes = align256(o + arena_bytes);
+  return L;
+}
+
+}  // namespace catn

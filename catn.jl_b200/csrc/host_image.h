@@ -1,0 +1,228 @@
+// Host-side construction of the packed input image that the device engine
+// loads: networks in MPS form, dense-tensor networks (raw2mps on device) and
+// the Ising / spin-glass builder of the reference (src/ising.jl:20-227).
+#pragma once
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "catn_layout.h"
+
+namespace catn {
+
+struct Image {
+  std::vector<long long> i64;
+  std::vector<int> i32;
+  std::vector<double> dat;
+  std::vector<InstDesc> desc;
+  int nmax = 0;       // largest node count
+  int emax = 0;       // largest real-edge count
+  int smax = 0;       // largest per-node site / neighbour count at load
+  long long trace_total = 0;
+
+  // Network in MPS form.  Returns an error message or "".
+  std::string add_mps(const catn_params& P, int n, const int* site_counts, const int* nbr_counts,
+                      const int* canos, const long long* site_dims, const double* site_data,
+                      const int* neighbors, int trace_cap) {
+    if (n < 1) return "network has no nodes";
+    InstDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.P = P;
+    D.n = n;
+    D.kind = 0;
+    D.hdr_off = (long long)i64.size();
+    long long nsites = 0, nnb = 0;
+    for (int k = 0; k < n; ++k) {
+      if (site_counts[k] < 0 || nbr_counts[k] < 0) return "negative site/neighbour count";
+      i64.push_back(site_counts[k]);
+      i64.push_back(nbr_counts[k]);
+      i64.push_back(canos[k]);
+      i64.push_back(0);
+      nsites += site_counts[k];
+      nnb += nbr_counts[k];
+      if (site_counts[k] > smax) smax = site_counts[k];
+      if (nbr_counts[k] > smax) smax = nbr_counts[k];
+    }
+    D.dim_off = (long long)i64.size();
+    long long ndata = 0;
+    for (long long s = 0; s < nsites; ++s) {
+      long long dl = site_dims[3 * s], d = site_dims[3 * s + 1], dr = site_dims[3 * s + 2];
+      if (dl < 1 || d < 1 || dr < 1) return "site dimensions must be >= 1";
+      i64.push_back(dl);
+      i64.push_back(d);
+      i64.push_back(dr);
+      ndata += dl * d * dr;
+    }
+    D.nbr_off = (long long)i32.size();
+    int edges2 = 0;
+    for (long long q = 0; q < nnb; ++q) {
+      int v = neighbors[q];
+      if (v > n) return "neighbour id out of range";
+      if (v > 0) ++edges2;
+      i32.push_back(v);
+    }
+    D.data_off = (long long)dat.size();
+    D.data_len = ndata;
+    dat.insert(dat.end(), site_data, site_data + ndata);
+    finish(D, n, edges2 / 2 + 1, trace_cap);
+    return "";
+  }
+
+  // Network of dense tensors; raw2mps runs on the device.
+  std::string add_dense(const catn_params& P, int n, const int* ndims, const long long* dims,
+                        const double* data, const int* neighbors, int trace_cap) {
+    if (n < 1) return "network has no nodes";
+    InstDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.P = P;
+    D.n = n;
+    D.kind = 1;
+    D.hdr_off = (long long)i64.size();
+    long long nd_tot = 0;
+    for (int k = 0; k < n; ++k) {
+      i64.push_back(ndims[k]);
+      i64.push_back(ndims[k]);
+      i64.push_back(0);
+      i64.push_back(0);
+      nd_tot += ndims[k];
+      if (ndims[k] > smax) smax = ndims[k];
+    }
+    D.dim_off = (long long)i64.size();
+    long long pos = 0, ndata = 0;
+    for (int k = 0; k < n; ++k) {
+      long long tot = 1;
+      for (int q = 0; q < ndims[k]; ++q) {
+        if (dims[pos + q] < 1) return "tensor dimensions must be >= 1";
+        i64.push_back(dims[pos + q]);
+        tot *= dims[pos + q];
+      }
+      pos += ndims[k];
+      ndata += tot;   // a 0-d tensor holds one value
+    }
+    D.nbr_off = (long long)i32.size();
+    int edges2 = 0;
+    for (long long q = 0; q < nd_tot; ++q) {
+      int v = neighbors[q];
+      if (v > n) return "neighbour id out of range";
+      if (v > 0) ++edges2;
+      i32.push_back(v);
+    }
+    D.data_off = (long long)dat.size();
+    D.data_len = ndata;
+    dat.insert(dat.end(), data, data + ndata);
+    finish(D, n, edges2 / 2 + 1, trace_cap);
+    return "";
+  }
+
+  // ising_network (src/ising.jl:20-227): one site per incident edge, B =
+  // exp(beta w s_i s_j) on the first endpoint, identity on the second, field
+  // folded into the first (or leaf) site, degree-0 spins as 2cosh(beta h).
+  std::string add_ising(const catn_params& P, int n, int n_edges, const int* edges, const double* w,
+                        const double* h, double beta, int pos1, int val1, int pos2, int val2,
+                        int trace_cap) {
+    if (n < 1) return "ising_network: n must be >= 1";
+    std::vector<int> degree(n + 1, 0);
+    for (int e = 0; e < n_edges; ++e) {
+      int i = edges[2 * e], j = edges[2 * e + 1];
+      if (i < 1 || i > n || j < 1 || j > n) return "ising_network: edge endpoint out of range";
+      degree[i] += 1;
+      degree[j] += 1;
+    }
+    if ((pos1 != 0 && (val1 < 1 || val1 > 2)) || (pos2 != 0 && (val2 < 1 || val2 > 2)))
+      return "ising_network: pinned value must be 1 or 2";
+    struct Site { int dl, d, dr; double v[8]; };
+    std::vector<std::vector<Site>> mps(n + 1);
+    std::vector<std::vector<int>> nbr(n + 1);
+    auto build_site = [&](int node, double field_diag[2], const double Q[2][2]) -> Site {
+      Site s;
+      std::memset(&s, 0, sizeof(s));
+      int deg = degree[node];
+      // F*Q with F = diag(field)
+      double FQ[2][2] = {{field_diag[0] * Q[0][0], field_diag[0] * Q[0][1]},
+                         {field_diag[1] * Q[1][0], field_diag[1] * Q[1][1]}};
+      if (deg == 1) {
+        // leaf: sum over spin_i -> (1, 2, 1)
+        s.dl = 1; s.d = 2; s.dr = 1;
+        s.v[0] = FQ[0][0] + FQ[1][0];
+        s.v[1] = FQ[0][1] + FQ[1][1];
+      } else if (nbr[node].empty()) {
+        // first: reshape((F*Q)', 1, 2, 2): site[0, a, b] = (F Q)[b, a]
+        s.dl = 1; s.d = 2; s.dr = 2;
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) s.v[a + 2 * b] = FQ[b][a];
+      } else if ((int)nbr[node].size() == deg - 1) {
+        // last: reshape(Q, 2, 2, 1): site[a, s, 0] = Q[a, s]
+        s.dl = 2; s.d = 2; s.dr = 1;
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) s.v[a + 2 * b] = Q[a][b];
+      } else {
+        // interior: t3[a, s, b] = delta_ab Q[a, s]
+        s.dl = 2; s.d = 2; s.dr = 2;
+        for (int a = 0; a < 2; ++a)
+          for (int sp = 0; sp < 2; ++sp) s.v[a + 2 * sp + 4 * a] = Q[a][sp];
+      }
+      return s;
+    };
+    for (int e = 0; e < n_edges; ++e) {
+      int i = edges[2 * e], j = edges[2 * e + 1];
+      double si[2] = {1.0, -1.0}, sj[2] = {1.0, -1.0};
+      if (i == pos1) si[val1 - 1] = 0.0;
+      else if (i == pos2) si[val2 - 1] = 0.0;
+      if (j == pos1) sj[val1 - 1] = 0.0;
+      else if (j == pos2) sj[val2 - 1] = 0.0;
+      double B[2][2], I2[2][2] = {{1.0, 0.0}, {0.0, 1.0}};
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) B[a][b] = std::exp(beta * w[e] * (si[a] * sj[b]));
+      double fi[2] = {std::exp(beta * h[i - 1] * si[0]), std::exp(beta * h[i - 1] * si[1])};
+      mps[i].push_back(build_site(i, fi, B));
+      nbr[i].push_back(j);
+      double fj[2] = {std::exp(beta * h[j - 1] * sj[0]), std::exp(beta * h[j - 1] * sj[1])};
+      mps[j].push_back(build_site(j, fj, I2));
+      nbr[j].push_back(i);
+    }
+    std::vector<int> sc(n), nc(n), cn(n);
+    std::vector<long long> dims;
+    std::vector<double> data;
+    std::vector<int> nb;
+    for (int k = 1; k <= n; ++k) {
+      if (degree[k] == 0) {
+        Site s;
+        std::memset(&s, 0, sizeof(s));
+        s.dl = s.d = s.dr = 1;
+        s.v[0] = std::exp(beta * h[k - 1]) + std::exp(-beta * h[k - 1]);
+        mps[k].push_back(s);
+      }
+      sc[k - 1] = (int)mps[k].size();
+      nc[k - 1] = (int)nbr[k].size();
+      cn[k - 1] = (int)mps[k].size();
+      for (const Site& s : mps[k]) {
+        dims.push_back(s.dl);
+        dims.push_back(s.d);
+        dims.push_back(s.dr);
+        for (int q = 0; q < s.dl * s.d * s.dr; ++q) data.push_back(s.v[q]);
+      }
+      for (int v : nbr[k]) nb.push_back(v);
+    }
+    return add_mps(P, n, sc.data(), nc.data(), cn.data(), dims.data(), data.data(), nb.data(), trace_cap);
+  }
+
+ private:
+  void finish(InstDesc& D, int n, int edges, int trace_cap) {
+    D.trace_cap = trace_cap;
+    D.trace_off = trace_total;
+    trace_total += 8LL * trace_cap;
+    desc.push_back(D);
+    if (n > nmax) nmax = n;
+    if (edges > emax) emax = edges;
+  }
+};
+
+// Site / neighbour capacity per node: the largest order a node can reach
+// is bounded by its initial order plus everything it can absorb.
+inline int default_maxs(const Image& im) {
+  int m = 128;
+  if (im.smax + 8 > m) m = im.smax + 8;
+  return m;
+}
+
+}  // namespace catn

@@ -1,0 +1,418 @@
+// Team-cooperative dense linear algebra for the CATN engine (FP64).
+//
+//  * gemm      C = A * B over general two-level strided operands, so every
+//              einsum of the reference (mps_node.jl:63,85,99,150,367,504,539,
+//              613) is one call with its index permutation folded into the
+//              operand maps (no separate permute pass).
+//  * qr_*      Householder QR (LAPACK geqrf semantics, R in the upper
+//              triangle, reflectors below) and application of the thin Q to
+//              a padded matrix -- the reference's `qr` + `_thin_q`
+//              (linalg_utils.jl:32-37).
+//  * svd       thin SVD A = U diag(S) V^T with S sorted descending, by QR
+//              pre-reduction (tall inputs) and one-sided Hestenes Jacobi with
+//              a round-robin pair order; the reference's `svd` (gesdd) in
+//              `tsvd` (linalg_utils.jl:15-28).
+#pragma once
+#include "team.cuh"
+
+namespace catn {
+
+// Two-level index map: x -> (x % n1) * s1 + (x / n1) * s2.
+struct IMap {
+  int n1;
+  long long s1, s2;
+  CATN_HD long long at(long long x) const {
+    if (n1 == 1) return x * s2;
+    long long q = x / n1;
+    return (x - q * n1) * s1 + q * s2;
+  }
+};
+CATN_HD IMap imap(int n1, long long s1, long long s2) { IMap m; m.n1 = n1; m.s1 = s1; m.s2 = s2; return m; }
+// Plain column-major index: row r -> r, col c -> c*ld.
+CATN_HD IMap rows_plain() { return imap(1, 0, 1); }
+CATN_HD IMap cols_plain(long long ld) { return imap(1, 0, ld); }
+
+// Matrix operand X(r, c) = p[R.at(r) + C.at(c)] * rs[r] * cs[c] (scales optional).
+struct MOp {
+  double* p;
+  IMap R, C;
+  const double* rs;
+  const double* cs;
+  CATN_HD double ld(long long r, long long c) const {
+    double v = p[R.at(r) + C.at(c)];
+    if (rs) v *= rs[r];
+    if (cs) v *= cs[c];
+    return v;
+  }
+  CATN_HD double& ref(long long r, long long c) const { return p[R.at(r) + C.at(c)]; }
+};
+CATN_HD MOp mop(double* p, IMap R, IMap C, const double* rs = nullptr, const double* cs = nullptr) {
+  MOp o; o.p = p; o.R = R; o.C = C; o.rs = rs; o.cs = cs; return o;
+}
+// Plain column-major matrix with leading dimension ld.
+CATN_HD MOp colmajor(double* p, long long ld) { return mop(p, rows_plain(), cols_plain(ld)); }
+// Transposed view of a column-major matrix: X(r, c) = p[c + r*ld].
+CATN_HD MOp transposed(double* p, long long ld) { return mop(p, cols_plain(ld), rows_plain()); }
+
+// ---------------------------------------------------------------------------
+// GEMM: C(M x N) = A(M x K) * B(K x N), overwrite.
+// ---------------------------------------------------------------------------
+constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
+constexpr int GEMM_STAGE_BYTES = (GEMM_BM + GEMM_BN) * GEMM_BK * 8;
+
+CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, const MOp& A,
+                          const MOp& B, const MOp& C) {
+  if (M <= 0 || N <= 0) return;
+#if CATN_DEVICE_PASS
+  if (T.size() == 256 && T.stage_bytes >= GEMM_STAGE_BYTES && M * N >= 256) {
+    double* sA = (double*)T.stage;            // [BK][BM]
+    double* sB = sA + GEMM_BK * GEMM_BM;      // [BK][BN]
+    const int tid = T.rank();
+    const int tx = tid & 15, ty = tid >> 4;   // 16 x 16 threads, 4 x 4 outputs each
+    for (long long m0 = 0; m0 < M; m0 += GEMM_BM) {
+      for (long long n0 = 0; n0 < N; n0 += GEMM_BN) {
+        double acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+        for (long long k0 = 0; k0 < K; k0 += GEMM_BK) {
+          for (int e = tid; e < GEMM_BK * GEMM_BM; e += 256) {
+            int kk = e / GEMM_BM, mm = e - kk * GEMM_BM;
+            long long r = m0 + mm, k = k0 + kk;
+            sA[e] = (r < M && k < K) ? A.ld(r, k) : 0.0;
+          }
+          for (int e = tid; e < GEMM_BK * GEMM_BN; e += 256) {
+            int kk = e / GEMM_BN, nn = e - kk * GEMM_BN;
+            long long c = n0 + nn, k = k0 + kk;
+            sB[e] = (c < N && k < K) ? B.ld(k, c) : 0.0;
+          }
+          __syncthreads();
+#pragma unroll 4
+          for (int kk = 0; kk < GEMM_BK; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] = sA[kk * GEMM_BM + ty * 4 + q];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) b[q] = sB[kk * GEMM_BN + tx * 4 + q];
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+#pragma unroll
+              for (int y = 0; y < 4; ++y) acc[x][y] = fma(a[x], b[y], acc[x][y]);
+          }
+          __syncthreads();
+        }
+#pragma unroll
+        for (int x = 0; x < 4; ++x) {
+          long long r = m0 + ty * 4 + x;
+          if (r >= M) continue;
+#pragma unroll
+          for (int y = 0; y < 4; ++y) {
+            long long c = n0 + tx * 4 + y;
+            if (c < N) C.ref(r, c) = acc[x][y];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    return;
+  }
+#endif
+  // Small problems (and the host build): one output element per thread.
+  for (long long e = T.rank(); e < M * N; e += T.size()) {
+    long long r = e % M, c = e / M;
+    double s = 0.0;
+    for (long long k = 0; k < K; ++k) s = fma(A.ld(r, k), B.ld(k, c), s);
+    C.ref(r, c) = s;
+  }
+  T.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise helpers
+// ---------------------------------------------------------------------------
+CATN_HDI inline void copy(const Team& T, double* dst, const double* src, long long n) {
+  for (long long e = T.rank(); e < n; e += T.size()) dst[e] = src[e];
+  T.sync();
+}
+CATN_HDI inline void fill(const Team& T, double* dst, double v, long long n) {
+  for (long long e = T.rank(); e < n; e += T.size()) dst[e] = v;
+  T.sync();
+}
+CATN_HDI inline void scale(const Team& T, double* dst, double v, long long n) {
+  for (long long e = T.rank(); e < n; e += T.size()) dst[e] *= v;
+  T.sync();
+}
+// dst(rows x cols, col-major ld_d) = op(r, c)
+CATN_HDI inline void materialize(const Team& T, double* dst, long long rows, long long cols,
+                                 long long ldd, const MOp& op) {
+  for (long long e = T.rank(); e < rows * cols; e += T.size()) {
+    long long r = e % rows, c = e / rows;
+    dst[r + c * ldd] = op.ld(r, c);
+  }
+  T.sync();
+}
+CATN_HDI inline double sumsq(const Team& T, const double* x, long long n) {
+  double s = 0.0;
+  for (long long e = T.rank(); e < n; e += T.size()) s = fma(x[e], x[e], s);
+  return T.sum(s);
+}
+CATN_HDI inline double sumv(const Team& T, const double* x, long long n) {
+  double s = 0.0;
+  for (long long e = T.rank(); e < n; e += T.size()) s += x[e];
+  return T.sum(s);
+}
+CATN_HDI inline double maxabs(const Team& T, const double* x, long long n) {
+  double s = 0.0;
+  for (long long e = T.rank(); e < n; e += T.size()) s = fmax(s, fabs(x[e]));
+  return T.maxv(s);
+}
+
+// ---------------------------------------------------------------------------
+// Householder QR, m >= n, in place (LAPACK dgeqr2 semantics).
+// ---------------------------------------------------------------------------
+CATN_HDI inline void qr_inplace(const Team& T, double* A, long long m, long long n, long long lda,
+                                double* tau) {
+  for (long long k = 0; k < n; ++k) {
+    double* ak = A + k * lda;
+    double loc = 0.0;
+    for (long long i = k + 1 + T.rank(); i < m; i += T.size()) loc = fma(ak[i], ak[i], loc);
+    double xnorm2 = T.sum(loc);
+    double alpha = ak[k];
+    double tk = 0.0;
+    if (xnorm2 > 0.0) {
+      double beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+      tk = (beta - alpha) / beta;
+      double sc = 1.0 / (alpha - beta);
+      for (long long i = k + 1 + T.rank(); i < m; i += T.size()) ak[i] *= sc;
+      T.sync();
+      if (T.leader()) ak[k] = beta;
+    }
+    if (T.leader()) tau[k] = tk;
+    T.sync();
+    if (tk != 0.0) {
+      // A[k:m, j] -= tk * v * (v^T A[k:m, j]),  v = [1; A[k+1:m, k]]
+      for (long long j = k + 1 + T.warp(); j < n; j += T.nwarps()) {
+        double* aj = A + j * lda;
+        double w = 0.0;
+        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], aj[i], w);
+        w = T.wsum(w) + aj[k];
+        w *= tk;
+        T.wsync();
+        if (T.lane() == 0) aj[k] -= w;
+        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) aj[i] -= w * ak[i];
+        T.wsync();
+      }
+      T.sync();
+    }
+  }
+}
+
+// Householder QR with column pivoting, m >= n, in place: A P = Q R
+// (LAPACK dgeqp3 semantics; partial column norms are recomputed exactly
+// while each reflector is applied).  piv[k] = original index of column k.
+CATN_HDI inline void qrcp_inplace(const Team& T, double* A, long long m, long long n, long long lda,
+                                  double* tau, int* piv, double* nrm) {
+  for (long long j = T.warp(); j < n; j += T.nwarps()) {
+    const double* aj = A + j * lda;
+    double s = 0.0;
+    for (long long i = T.lane(); i < m; i += T.wsize()) s = fma(aj[i], aj[i], s);
+    s = T.wsum(s);
+    if (T.lane() == 0) { nrm[j] = s; piv[j] = (int)j; }
+  }
+  T.sync();
+  for (long long k = 0; k < n; ++k) {
+    // pivot: largest remaining partial norm
+    double bv = -1.0;
+    long long bi = -1;
+    for (long long j = k + T.rank(); j < n; j += T.size()) {
+      double v = nrm[j];
+      if (bi < 0 || v > bv) { bv = v; bi = j; }
+    }
+    long long p = T.argmax(bv, bi);
+    if (p != k && p >= 0) {
+      double* ak = A + k * lda;
+      double* ap = A + p * lda;
+      for (long long i = T.rank(); i < m; i += T.size()) {
+        double t = ak[i]; ak[i] = ap[i]; ap[i] = t;
+      }
+      T.sync();
+      if (T.leader()) {
+        double t = nrm[k]; nrm[k] = nrm[p]; nrm[p] = t;
+        int q = piv[k]; piv[k] = piv[p]; piv[p] = q;
+      }
+      T.sync();
+    }
+    double* ak = A + k * lda;
+    double loc = 0.0;
+    for (long long i = k + 1 + T.rank(); i < m; i += T.size()) loc = fma(ak[i], ak[i], loc);
+    double xnorm2 = T.sum(loc);
+    double alpha = ak[k];
+    double tk = 0.0;
+    if (xnorm2 > 0.0) {
+      double beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+      tk = (beta - alpha) / beta;
+      double sc = 1.0 / (alpha - beta);
+      for (long long i = k + 1 + T.rank(); i < m; i += T.size()) ak[i] *= sc;
+      T.sync();
+      if (T.leader()) ak[k] = beta;
+    }
+    if (T.leader()) tau[k] = tk;
+    T.sync();
+    for (long long j = k + 1 + T.warp(); j < n; j += T.nwarps()) {
+      double* aj = A + j * lda;
+      if (tk != 0.0) {
+        double w = 0.0;
+        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], aj[i], w);
+        w = T.wsum(w) + aj[k];
+        w *= tk;
+        T.wsync();
+        if (T.lane() == 0) aj[k] -= w;
+        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) aj[i] -= w * ak[i];
+        T.wsync();
+      }
+      double s = 0.0;
+      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) s = fma(aj[i], aj[i], s);
+      s = T.wsum(s);
+      if (T.lane() == 0) nrm[j] = s;
+      T.wsync();
+    }
+    T.sync();
+  }
+}
+
+// C(m x ncols, ld ldc) <- Q * C with Q = H_0 ... H_{n-1} from qr_inplace.
+CATN_HDI inline void qr_apply_q(const Team& T, const double* A, long long m, long long n,
+                                long long lda, const double* tau, double* C, long long ncols,
+                                long long ldc) {
+  for (long long k = n - 1; k >= 0; --k) {
+    double tk = tau[k];
+    if (tk == 0.0) continue;
+    const double* ak = A + k * lda;
+    for (long long j = T.warp(); j < ncols; j += T.nwarps()) {
+      double* cj = C + j * ldc;
+      double w = 0.0;
+      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], cj[i], w);
+      w = T.wsum(w) + cj[k];
+      w *= tk;
+      T.wsync();
+      if (T.lane() == 0) cj[k] -= w;
+      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) cj[i] -= w * ak[i];
+      T.wsync();
+    }
+    T.sync();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-sided Jacobi on B (m x n, m >= n, col-major ld ldb), accumulating V
+// (n x n, ld n).  Columns of B converge to U * diag(S).  Returns the number
+// of sweeps, or -1 when the sweep cap was reached.
+// ---------------------------------------------------------------------------
+CATN_HD void rr_pair(long long np, long long r, long long i, long long* a, long long* b) {
+  // circle method over np (even) players; player 0 fixed.
+  auto pos = [&](long long k) -> long long { return k == 0 ? 0 : ((k - 1 + r) % (np - 1)) + 1; };
+  *a = pos(i);
+  *b = pos(np - 1 - i);
+}
+
+CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long long n, long long ldb,
+                                  double* V, int max_sweeps) {
+  for (long long e = T.rank(); e < n * n; e += T.size()) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  T.sync();
+  if (n < 2) return 0;
+  // Work at unit max-abs scale so that numerically-zero columns are
+  // recognised by an absolute threshold and never reach denormal range.
+  double mx = 0.0;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) mx = fmax(mx, fabs(B[i + c * ldb]));
+  mx = T.maxv(mx);
+  const double sc = mx > 0.0 ? 1.0 / mx : 1.0;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] *= sc;
+  T.sync();
+  const long long np = (n % 2) ? n + 1 : n;
+  const double tol = 2.220446049250313e-16 * (double)(m > 16 ? m : 16);
+  int result = -1;
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    int rotated = 0;
+    for (long long r = 0; r < np - 1; ++r) {
+      for (long long pi = T.warp(); pi < np / 2; pi += T.nwarps()) {
+        long long p, q;
+        rr_pair(np, r, pi, &p, &q);
+        if (p >= n || q >= n) continue;
+        double* bp = B + p * ldb;
+        double* bq = B + q * ldb;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (long long i = T.lane(); i < m; i += T.wsize()) {
+          double x = bp[i], y = bq[i];
+          al = fma(x, x, al);
+          be = fma(y, y, be);
+          ga = fma(x, y, ga);
+        }
+        al = T.wsum(al);
+        be = T.wsum(be);
+        ga = T.wsum(ga);
+        if (al < 1e-250 || be < 1e-250) continue;   // numerically zero column
+        if (!(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
+        rotated = 1;
+        double zeta = (be - al) / (2.0 * ga);
+        double t = fabs(zeta) > 1e150 ? 0.5 / zeta
+                                      : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double c = 1.0 / sqrt(1.0 + t * t);
+        double s = c * t;
+        T.wsync();
+        for (long long i = T.lane(); i < m; i += T.wsize()) {
+          double x = bp[i], y = bq[i];
+          bp[i] = c * x - s * y;
+          bq[i] = s * x + c * y;
+        }
+        double* vp = V + p * n;
+        double* vq = V + q * n;
+        for (long long i = T.lane(); i < n; i += T.wsize()) {
+          double x = vp[i], y = vq[i];
+          vp[i] = c * x - s * y;
+          vq[i] = s * x + c * y;
+        }
+        T.wsync();
+      }
+      T.sync();
+    }
+    if (!T.any(rotated)) {
+      result = sweep + 1;
+      break;
+    }
+  }
+  const double inv = 1.0 / sc;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] *= inv;
+  T.sync();
+  return result;
+}
+
+// Column norms of B (n columns), then stable descending order.
+// S_out[r] = sigma of the r-th largest column, perm[r] = its column index.
+CATN_HDI inline void sort_columns(const Team& T, const double* B, long long m, long long n,
+                                  long long ldb, double* sig, double* S_out, int* perm) {
+  for (long long j = T.warp(); j < n; j += T.nwarps()) {
+    const double* bj = B + j * ldb;
+    double s = 0.0;
+    for (long long i = T.lane(); i < m; i += T.wsize()) s = fma(bj[i], bj[i], s);
+    s = T.wsum(s);
+    if (T.lane() == 0) sig[j] = sqrt(s);
+  }
+  T.sync();
+  for (long long j = T.rank(); j < n; j += T.size()) {
+    double sj = sig[j];
+    long long rk = 0;
+    for (long long l = 0; l < n; ++l) {
+      double sl = sig[l];
+      rk += (sl > sj || (sl == sj && l < j)) ? 1 : 0;
+    }
+    perm[rk] = (int)j;
+    S_out[rk] = sj;
+  }
+  T.sync();
+}
+
+}  // namespace catn

@@ -1,0 +1,162 @@
+/* catn_b200.h -- C ABI of libcatn_b200.so, the B200 (sm_100a) implementation
+ * of the CATN.jl `contraction!` hot path.
+ *
+ * The reference (xuanzhaogao/CATN.jl v0.1.0) has no FFI: its backend seam is
+ * Julia dispatch on the array type `AT` of `TensorNetwork{T,AT}` /
+ * `MPSNode{T,AT}` (src/tensor_network.jl:1, src/mps_node.jl:1) entered
+ * through `Adapt.adapt_structure` (src/adapt.jl:6-24).  Each entry point
+ * below replaces the reference function named beside it; a Julia `ccall`
+ * binding for each is given in INTEGRATION.md.
+ *
+ * Conventions
+ *   - Node ids are 1-based, neighbour ids of open legs are negative
+ *     sentinels, exactly as in the reference.
+ *   - Site tensors are (left, phys, right) in column-major order (Julia
+ *     layout); dense tensors are column-major over their legs.
+ *   - All buffers passed in are host memory owned by the caller for the
+ *     duration of the call; the library copies what it needs to HBM.
+ *   - Every function returns a catn_status; on failure a thread-local message
+ *     is available from catn_last_error().
+ */
+#ifndef CATN_B200_H
+#define CATN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CATN_OK = 0,
+  CATN_EINVAL = 1,    /* bad argument (reference: error()/@assert)          */
+  CATN_ENOMEM = 2,    /* device arena or control capacity exhausted         */
+  CATN_ENOCONV = 3,   /* Jacobi SVD hit its sweep cap                       */
+  CATN_ETIMEOUT = 4,  /* a bounded device wait ran out                      */
+  CATN_ECUDA = 5,     /* CUDA runtime error                                 */
+  CATN_ESTATE = 6     /* reference error path (e.g. open-leg cut, merge!)   */
+} catn_status;
+
+/* Keyword arguments of TensorNetwork / ising_network
+ * (src/tensor_network.jl:41-54, src/ising.jl:20-40). */
+typedef struct {
+  int32_t Dmax;        /* <0: exact mode                                   */
+  int32_t chi;
+  double cutoff;
+  int32_t norm_method; /* 0 none, 1 Frobenius, 2 max-abs                     */
+  int32_t select;      /* 0 min_dim, 1 min_dim_triangle, 2 sequential        */
+  int32_t reverse;
+  int32_t svdopt;
+  int32_t swapopt;
+  int32_t compress;
+  int32_t cut_bond;
+  int32_t seed;        /* kept for API parity; the reference never reads it */
+  int32_t trace;       /* record the per-step integer trace                 */
+} catn_params;
+
+/* Default values of the reference's keyword arguments. */
+void catn_params_default(catn_params* p);
+
+/* Results of one contraction (`contraction!` return value plus state). */
+typedef struct {
+  double lnZ;          /* tn.lnZ                                            */
+  double err;          /* accumulated discarded singular values             */
+  double psi;          /* tn.psi (phase; +-1 for real networks)             */
+  double sign;         /* tn.sign from network_lognorm                      */
+  int32_t maxdim;      /* tn.maxdim_intermediate                            */
+  int32_t status;      /* catn_status of this instance                      */
+  int32_t nsteps;      /* contraction steps taken                           */
+  int32_t jacobi_max;  /* largest Jacobi sweep count seen                   */
+  int64_t arena_peak;  /* device bytes high-water mark                      */
+} catn_result;
+
+typedef struct catn_net catn_net;       /* one network, device resident    */
+typedef struct catn_batch catn_batch;   /* many networks, one launch       */
+
+/* Network in MPS form (what ising_network and MPSNode carry).
+ *   site_counts[k]        number of sites of node k+1
+ *   nbr_counts[k]         number of neighbour entries of node k+1
+ *   canos[k]              node.cano
+ *   site_dims[3*s..]      (dl, d, dr) of every site, nodes in order
+ *   site_data             all site tensors concatenated (float64)
+ *   neighbors             all neighbour lists concatenated
+ * Replaces TensorNetwork{T,AT}(nodes...) construction on the device side
+ * (src/tensor_network.jl:118-139, src/ising.jl:205-226). */
+catn_status catn_net_create_mps(const catn_params* p, int32_t n_nodes, const int32_t* site_counts,
+                                const int32_t* nbr_counts, const int32_t* canos,
+                                const int64_t* site_dims, const double* site_data,
+                                const int32_t* neighbors, int64_t arena_bytes, catn_net** out);
+
+/* Network from dense tensors (`TensorNetwork(tensors, ixs)`,
+ * src/tensor_network.jl:41-140): node k has ndims[k] legs with the given
+ * dims; the neighbour list gives, per leg, the node sharing it (negative
+ * sentinel for open legs).  raw2mps (src/mps_node.jl:31-50) runs on the
+ * device. */
+catn_status catn_net_create_dense(const catn_params* p, int32_t n_nodes, const int32_t* ndims,
+                                  const int64_t* dims, const double* data,
+                                  const int32_t* neighbors, int64_t arena_bytes, catn_net** out);
+
+/* contraction!(tn) -> (lnZ, error, psi)  (src/tensor_network.jl:556-717).
+ * `trace` (optional, may be NULL) receives 8 int32 per step:
+ *   i, j, rev_i | rev_j<<1, n_duplicates, fnv(duplicates), nsites_i,
+ *   fnv(phys dims of i), maxdim_intermediate. */
+catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32_t trace_cap);
+
+/* Shapes of the surviving nodes after contraction (result_tensor support,
+ * src/tensor_network.jl:517-523): dense tensor of the single surviving
+ * open-leg node, legs in its final MPS order.  `out` may be NULL to query
+ * `numel`/`ndim`; `dims` receives up to 64 leg sizes. */
+catn_status catn_result_tensor(catn_net* net, double* out, int64_t cap, int64_t* numel,
+                               int32_t* ndim, int64_t* dims);
+
+catn_status catn_net_destroy(catn_net* net);
+
+/* Ising / spin-glass network in MPS form (src/ising.jl:20-227), built on the
+ * host exactly as the reference's builder does, contracted on the device.
+ * edges: 2*n_edges 1-based endpoints.  pos/val pin spins as in the
+ * reference (0 = none). */
+catn_status catn_ising_create(const catn_params* p, int32_t n, int32_t n_edges,
+                              const int32_t* edges, const double* weights, const double* fields,
+                              double beta, int32_t pos1, int32_t val1, int32_t pos2, int32_t val2,
+                              int64_t arena_bytes, catn_net** out);
+
+/* Batched Ising instances contracted in ONE persistent kernel launch with a
+ * device work queue (no reference counterpart: the reference loops on the
+ * host, e.g. magnetization/correlation at src/ising.jl:263-339).
+ * Instance b uses edges[edge_off[b] .. edge_off[b+1]) (pairs), fields
+ * [node_off[b] .. node_off[b+1]), betas[b], pins[4*b .. 4*b+3]
+ * (pos1, val1, pos2, val2; NULL = none). */
+catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const int32_t* n_nodes,
+                                    const int64_t* node_off, const int64_t* edge_off,
+                                    const int32_t* edges, const double* weights,
+                                    const double* fields, const double* betas,
+                                    const int32_t* pins, int64_t slot_arena_bytes,
+                                    int32_t max_slots, catn_batch** out);
+
+/* Upload the inputs of the batch (host -> HBM), run the persistent kernel,
+ * read back the per-instance results.  Timing-friendly split below. */
+catn_status catn_batch_run(catn_batch* b, catn_result* results);
+
+/* Device-only run: inputs already resident; `stream` is a cudaStream_t
+ * (NULL = default stream).  Results stay on the device until
+ * catn_batch_results(). */
+catn_status catn_batch_launch(catn_batch* b, void* stream);
+catn_status catn_batch_upload(catn_batch* b, void* stream);
+catn_status catn_batch_results(catn_batch* b, catn_result* results, void* stream);
+/* Number of CTA slots (resident blocks) the batch launches with. */
+int32_t catn_batch_slots(const catn_batch* b);
+/* Bytes of per-batch input copied host->device by catn_batch_upload. */
+int64_t catn_batch_input_bytes(const catn_batch* b);
+catn_status catn_batch_destroy(catn_batch* b);
+
+/* Thread-local message of the last failure (always NUL-terminated). */
+size_t catn_last_error(char* buf, size_t cap);
+
+/* Library build string (arch, version). */
+const char* catn_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CATN_B200_H */

@@ -1,0 +1,50 @@
+// Test-only host build of the device engine (team of one thread), used by the
+// CPU test-suite to check the engine's integer bookkeeping and memory safety
+// (under AddressSanitizer) against the oracle.  It is not part of
+// libcatn_b200 and is never loaded by the product path.
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "../../catn.jl_b200/csrc/engine.cuh"
+#include "../../catn.jl_b200/csrc/host_image.h"
+
+using namespace catn;
+
+static int run_image(Image& im, long long arena_bytes, catn_result* res, int* trace) {
+  if (im.desc.empty()) return CATN_EINVAL;
+  SlotLayout L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
+  std::vector<char> slot((size_t)L.slot_bytes + 256);
+  char* sp = (char*)(((uintptr_t)slot.data() + 255) & ~(uintptr_t)255);
+  std::vector<double> red(64);
+  Team T;
+  T.red = red.data();
+  T.stage = nullptr;
+  T.stage_bytes = 0;
+  std::vector<int> tr((size_t)im.trace_total + 8);
+  run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data());
+  if (trace && im.desc[0].trace_cap > 0)
+    std::memcpy(trace, tr.data(), sizeof(int) * 8 * (size_t)im.desc[0].trace_cap);
+  return res->status;
+}
+
+extern "C" {
+
+int catn_hostcheck_ising(const catn_params* p, int n, int n_edges, const int* edges, const double* w,
+                         const double* h, double beta, int pos1, int val1, int pos2, int val2,
+                         long long arena_bytes, catn_result* res, int* trace, int trace_cap) {
+  Image im;
+  std::string e = im.add_ising(*p, n, n_edges, edges, w, h, beta, pos1, val1, pos2, val2, trace_cap);
+  if (!e.empty()) return CATN_EINVAL;
+  return run_image(im, arena_bytes, res, trace);
+}
+
+int catn_hostcheck_dense(const catn_params* p, int n, const int* ndims, const long long* dims,
+                         const double* data, const int* neighbors, long long arena_bytes,
+                         catn_result* res, int* trace, int trace_cap) {
+  Image im;
+  std::string e = im.add_dense(*p, n, ndims, dims, data, neighbors, trace_cap);
+  if (!e.empty()) return CATN_EINVAL;
+  return run_image(im, arena_bytes, res, trace);
+}
+
+}
