@@ -1,0 +1,347 @@
+"""Benchmark: batched spin-glass lnZ instances/s on B200 (libcatn_b200).
+
+Workload (one "step" = one persistent-kernel pass over one batch):
+  512 independent 2D spin-glass instances, open L x L square lattices with L
+  drawn uniformly from {8,10,12,14,16} (64-256 spins), couplings J ~ N(0,1),
+  fields h ~ N(0, 0.1^2), beta ~ U[0.5, 2.0], Dmax=32, chi=128, cutoff 1e-15,
+  select=1, norm_method=1 -- seeded synthetic inputs (numpy PCG64).
+
+  value  instances/s with the inputs already in HBM (CUDA events around the
+         kernel launch; L2 flushed by a 256 MiB write between steps)
+  e2e    instances/s through the public batch API per step: pinned
+         host->device copy of the packed inputs, the launch, device->host
+         read of every instance's result (CUDA events on the same stream)
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank contracts its own
+512-instance batch (weak scaling, no data-path collective); the time is the
+max over ranks.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = ("Ising lnZ instances/s and ∇lnZ time vs pinning, at |ΔlnZ|/n≤1e-6 vs FP64")
+PARAMS = dict(Dmax=32, chi=128, cutoff=1e-15, select=1, norm_method=1)
+WORKLOAD = ("512 2D spin-glass instances, L~U{8,10,12,14,16}, J~N(0,1), h~N(0,0.1^2), "
+            "beta~U[0.5,2], Dmax=32, chi=128, one persistent launch")
+
+
+def make_instances(count, seed):
+    import __graft_entry__
+    catn = __graft_entry__.load_package()
+    from catn_b200 import graphs
+    return graphs.spinglass_batch(count, seed)
+
+
+# ----------------------------------------------------------------------------
+# CPU legs (oracle port) -- run in spawned worker processes
+# ----------------------------------------------------------------------------
+def _oracle_one(d):
+    from oracle import ising as OI, network as ON
+    tn = OI.ising_network(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **PARAMS)
+    lnZ, _, _ = ON.contraction(tn)
+    return lnZ
+
+
+def _cpu_pool(nproc):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    return mp.get_context("spawn").Pool(nproc)
+
+
+def cpu_sample_rate(instances, seconds, nproc, pool=None):
+    """Contract instances in order on `nproc` single-threaded processes until
+    about `seconds` have passed; return (instances/s, count, lnZ list)."""
+    own = pool is None
+    pool = pool or _cpu_pool(nproc)
+    t0 = time.perf_counter()
+    done, lz = 0, []
+    it = pool.imap(_oracle_one, instances, chunksize=1)
+    for v in it:
+        lz.append(v)
+        done += 1
+        if time.perf_counter() - t0 > seconds or done == len(instances):
+            break
+    dt = time.perf_counter() - t0
+    if own:
+        pool.terminate()
+    return done / dt, done, lz
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------------------
+# clocks
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_traffic():
+    """DRAM bytes per launch of the persistent kernel from the committed ncu
+    summary (profiles/catn_persistent_kernel_spinglass_batch.txt), if any."""
+    p = os.path.join(ROOT, "profiles", "catn_persistent_kernel_spinglass_batch.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_full_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+def run_reference(args):
+    """--impl reference: the oracle port (CPU restatement of the reference
+    algorithm; Julia is unavailable) on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = host_cores()
+    insts = make_instances(args.instances, args.seed)
+    pool = _cpu_pool(cores)
+    per_step = max(cores, 8)
+    rates = []
+    pos = 0
+    for s in range(args.warmup + args.steps):
+        chunk = [insts[(pos + q) % len(insts)] for q in range(per_step)]
+        pos += per_step
+        t0 = time.perf_counter()
+        pool.map(_oracle_one, chunk, chunksize=1)
+        dt = time.perf_counter() - t0
+        if s >= args.warmup:
+            rates.append((per_step, dt))
+    pool.terminate()
+    n = sum(r[0] for r in rates)
+    t = sum(r[1] for r in rates)
+    v = n / t
+    out = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "instances/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(1000 * t / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "instances_per_step": per_step, "l2": "n/a (CPU)"},
+           "cpu_baseline": {"value": round(v, 3), "unit": "instances/s", "cores": cores, "kind": "port",
+                            "sample": f"{per_step} instances per step (instances in workload order, "
+                                      f"one single-threaded process per core)"},
+           "e2e": {"value": round(v, 3), "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
+    ap.add_argument("--arena-mb", type=int, default=64, help="device arena per slot, MiB")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    # CPU baseline first (spawned pool, before any CUDA call), rank 0 at N=1 only
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = host_cores()
+        sample = make_instances(args.instances, args.seed)
+        rate, cnt, _ = cpu_sample_rate(sample, args.cpu_seconds, cores)
+        cpu = {"value": round(rate, 3), "unit": "instances/s", "cores": cores, "kind": "port",
+               "sample": f"first {cnt} of the {args.instances} workload instances in order, "
+                         f"oracle port (numpy/OpenBLAS FP64), {cores} single-threaded processes, "
+                         f"~{args.cpu_seconds:.0f} s"}
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import __graft_entry__
+    catn = __graft_entry__.load_package()
+    insts = make_instances(args.instances, args.seed + 7919 * rank)
+    batch = catn.IsingBatch(insts, slot_arena_bytes=args.arena_mb << 20, max_slots=args.max_slots, **PARAMS)
+    stream = torch.cuda.current_stream()
+    sh = ct_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def device_step():
+        batch.launch(sh)
+
+    # warm-up (full API path, checks every instance)
+    batch.upload(sh)
+    for _ in range(args.warmup):
+        batch.launch(sh)
+        batch.fetch(sh)
+    res = batch.fetch(sh)
+    flops = sum(r.flops for r in res)
+    nbytes = sum(r.bytes for r in res)
+    steps_per_inst = [r.nsteps for r in res]
+    # --- device-resident timing ---
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            device_step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b) / 1000.0)
+        batch.fetch(sh)
+        # --- end-to-end timing through the public API ---
+        e2e_times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            batch.upload(sh)
+            batch.launch(sh)
+            batch.fetch(sh)
+            b.record(stream)
+            torch.cuda.synchronize()
+            e2e_times.append(a.elapsed_time(b) / 1000.0)
+    total = sum(times)
+    total_e2e = sum(e2e_times)
+    if dist:
+        t = torch.tensor([total, total_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total, total_e2e = float(t[0]), float(t[1])
+    units = args.instances * world * args.steps
+    value = units / total
+    e2e_value = units / total_e2e
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    peak, peak_kind = load_peaks()
+    avg = total / args.steps
+    achieved_gbs = nbytes / avg / 1e9
+    traffic = read_traffic()
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": "instances/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * avg, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "instances_per_gpu": args.instances, "seed": args.seed,
+                   "Dmax": 32, "chi": 128, "parallelism": f"replicas x{world} (independent instances)",
+                   "l2": "flushed (256 MiB write) between timed steps", "slots": batch.slots,
+                   "contraction_steps_total": int(sum(steps_per_inst))},
+        "e2e": {"value": round(e2e_value, 3), "unit": "instances/s",
+                "h2d_bytes_per_step": int(batch.input_bytes),
+                "d2h_bytes_per_step": int(args.instances * 64)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 3), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved_gbs / peak, 6), "traffic": traffic,
+                     "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
+                     "algorithmic_bytes_per_launch": nbytes,
+                     "algorithmic_fp64_flops_per_launch": flops,
+                     "achieved_fp64_tflops": round(flops / avg / 1e12, 4)},
+        "clocks": clk.summary(),
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ct_stream(stream):
+    import ctypes
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+if __name__ == "__main__":
+    main()

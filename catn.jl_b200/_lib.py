@@ -35,7 +35,8 @@ class Result(ct.Structure):
     """``catn_result``."""
     _fields_ = [("lnZ", ct.c_double), ("err", ct.c_double), ("psi", ct.c_double),
                 ("sign", ct.c_double), ("maxdim", ct.c_int32), ("status", ct.c_int32),
-                ("nsteps", ct.c_int32), ("jacobi_max", ct.c_int32), ("arena_peak", ct.c_int64)]
+                ("nsteps", ct.c_int32), ("jacobi_max", ct.c_int32), ("arena_peak", ct.c_int64),
+                ("flops", ct.c_double), ("bytes", ct.c_double)]
 
 
 # Every exported symbol with its ctypes signature (argtypes, restype).

@@ -47,7 +47,10 @@ const char* status_text(int s) {
 }
 
 constexpr int kThreads = 256;
-constexpr int kSmemBytes = 64 * 8 + GEMM_STAGE_BYTES;
+// Dynamic shared memory per CTA: reduction area, GEMM tile staging, and the
+// small-SVD workspace (two CTAs fit on one SM).
+constexpr int kSmemBytes = 100 * 1024;
+constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - GEMM_STAGE_BYTES) / 8;
 
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     const InstDesc* __restrict__ descs, int ninst, const long long* i64, const int* i32, const double* dat,
@@ -57,13 +60,14 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
   for (;;) {
     long long inst = 0;
     if (threadIdx.x == 0) inst = atomicAdd(queue, 1);
     inst = T.bcast(inst);
     if (inst >= ninst) break;
-    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace);
+    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles);
   }
 }
 
@@ -74,7 +78,7 @@ __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
-  Ctx C = make_ctx(T, slot, L, P, n);
+  Ctx C = make_ctx(T, slot, L, P, n, (double*)(T.stage + GEMM_STAGE_BYTES), kSwsDoubles);
   int nd = 0;
   long long dims[64];
   long long tot = result_tensor_dev(C, out, cap, dims, &nd);
@@ -86,8 +90,12 @@ __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
   }
 }
 
-// Device copy of an Image plus slots and results.
+// Device copy of an Image plus slots and results.  The input image is packed
+// into one pinned host buffer and one device buffer, so an upload is a single
+// host-to-device copy.
 struct DeviceRun {
+  char* h_input = nullptr;   // pinned
+  char* d_input = nullptr;
   InstDesc* d_desc = nullptr;
   long long* d_i64 = nullptr;
   int* d_i32 = nullptr;
@@ -102,10 +110,10 @@ struct DeviceRun {
   long long input_bytes = 0;
 
   void release() {
-    cudaFree(d_desc); cudaFree(d_i64); cudaFree(d_i32); cudaFree(d_dat);
-    cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
+    cudaFreeHost(h_input);
+    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
+    h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
     d_desc = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
-    d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
   }
 };
 
@@ -128,27 +136,31 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   if (ns * R.L.slot_bytes > budget) ns = budget / R.L.slot_bytes;
   if (ns < 1) return fail(CATN_ENOMEM, "not enough device memory for one slot");
   R.nslots = (int)ns;
-  CUDA_TRY(cudaMalloc(&R.d_desc, sizeof(InstDesc) * im.desc.size()));
-  CUDA_TRY(cudaMalloc(&R.d_i64, sizeof(long long) * (im.i64.size() + 1)));
-  CUDA_TRY(cudaMalloc(&R.d_i32, sizeof(int) * (im.i32.size() + 1)));
-  CUDA_TRY(cudaMalloc(&R.d_dat, sizeof(double) * (im.dat.size() + 1)));
+  const long long b_desc = align256((long long)(sizeof(InstDesc) * im.desc.size()));
+  const long long b_i64 = align256((long long)(sizeof(long long) * (im.i64.size() + 1)));
+  const long long b_i32 = align256((long long)(sizeof(int) * (im.i32.size() + 1)));
+  const long long b_dat = align256((long long)(sizeof(double) * (im.dat.size() + 1)));
+  R.input_bytes = b_desc + b_i64 + b_i32 + b_dat;
+  CUDA_TRY(cudaMallocHost(&R.h_input, (size_t)R.input_bytes));
+  CUDA_TRY(cudaMalloc(&R.d_input, (size_t)R.input_bytes));
+  std::memset(R.h_input, 0, (size_t)R.input_bytes);
+  std::memcpy(R.h_input, im.desc.data(), sizeof(InstDesc) * im.desc.size());
+  if (!im.i64.empty()) std::memcpy(R.h_input + b_desc, im.i64.data(), sizeof(long long) * im.i64.size());
+  if (!im.i32.empty()) std::memcpy(R.h_input + b_desc + b_i64, im.i32.data(), sizeof(int) * im.i32.size());
+  if (!im.dat.empty()) std::memcpy(R.h_input + b_desc + b_i64 + b_i32, im.dat.data(), sizeof(double) * im.dat.size());
+  R.d_desc = (InstDesc*)R.d_input;
+  R.d_i64 = (long long*)(R.d_input + b_desc);
+  R.d_i32 = (int*)(R.d_input + b_desc + b_i64);
+  R.d_dat = (double*)(R.d_input + b_desc + b_i64 + b_i32);
   CUDA_TRY(cudaMalloc(&R.d_slots, (size_t)(R.L.slot_bytes * ns)));
   CUDA_TRY(cudaMalloc(&R.d_res, sizeof(catn_result) * im.desc.size()));
   CUDA_TRY(cudaMalloc(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
   CUDA_TRY(cudaMalloc(&R.d_queue, sizeof(int)));
-  R.input_bytes = (long long)(sizeof(InstDesc) * im.desc.size() + sizeof(long long) * im.i64.size() +
-                              sizeof(int) * im.i32.size() + sizeof(double) * im.dat.size());
   return CATN_OK;
 }
 
-catn_status upload(const Image& im, DeviceRun& R, cudaStream_t st) {
-  CUDA_TRY(cudaMemcpyAsync(R.d_desc, im.desc.data(), sizeof(InstDesc) * im.desc.size(), cudaMemcpyHostToDevice, st));
-  if (!im.i64.empty())
-    CUDA_TRY(cudaMemcpyAsync(R.d_i64, im.i64.data(), sizeof(long long) * im.i64.size(), cudaMemcpyHostToDevice, st));
-  if (!im.i32.empty())
-    CUDA_TRY(cudaMemcpyAsync(R.d_i32, im.i32.data(), sizeof(int) * im.i32.size(), cudaMemcpyHostToDevice, st));
-  if (!im.dat.empty())
-    CUDA_TRY(cudaMemcpyAsync(R.d_dat, im.dat.data(), sizeof(double) * im.dat.size(), cudaMemcpyHostToDevice, st));
+catn_status upload(const Image&, DeviceRun& R, cudaStream_t st) {
+  CUDA_TRY(cudaMemcpyAsync(R.d_input, R.h_input, (size_t)R.input_bytes, cudaMemcpyHostToDevice, st));
   return CATN_OK;
 }
 

@@ -89,7 +89,7 @@ inline SlotLayout make_layout(int nmax, int maxs, int ecap, long long arena_byte
   L.off_pairs = o; o = align256(o + (long long)L.pcap * 8LL);
   L.off_list = o;  o = align256(o + (long long)L.lcap * 4LL);
   L.off_tmp = o;   o = align256(o + (2LL * maxs + 8) * 4LL);
-  L.off_ameta = o; o = align256(o + (CATN_NCLS + 2) * 8LL);
+  L.off_ameta = o; o = align256(o + (CATN_NCLS + 4) * 8LL);
   L.off_arena = o;
   L.arena_bytes = arena_bytes;
   L.slot_bytes = align256(o + arena_bytes);

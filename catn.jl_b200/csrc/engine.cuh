@@ -9,7 +9,7 @@
 // split over the team (linalg.cuh).
 //
 // Reference map (CATN.jl v0.1.0):
-//   tsvd ...................... linalg_utils.jl:15-28       -> svd_full + keep_rule
+//   tsvd ...................... linalg_utils.jl:15-28       -> svd_begin/svd_finish + keep_rule
 //   raw2mps ................... mps_node.jl:31-50           -> raw2mps
 //   cano_to!/left_canonical! .. mps_node.jl:72-106          -> cano_to
 //   swap!/move!/move2tail!/move2head! mps_node.jl:126-229  -> swap, move, ...
@@ -44,87 +44,67 @@ struct Ctx {
   int* bcnt;
   int* emap;
   int* ctl;
-  int* pairs;   // 2 * pcap ints of scratch (pair lists, reverse offsets)
+  int* pairs;   // 2 * pcap ints of scratch (pair lists)
   int pcap;
   int* list;    // lcap ints: node-id lists for the bucket updates
   int* tmp;     // 2 * maxs + 8 ints: neighbour snapshot and duplicates
-  char* base;
-  long long cap;
-  long long* ameta;  // [0] bump, [1..NCLS] free heads, [NCLS+1] peak
+  char* base;   // arena
+  // Scratch stack for per-operation temporaries [sp_lo, sp_hi).  Every
+  // thread keeps an identical copy of the stack pointer, so pushing and
+  // popping needs no barrier.
+  long long sp, sp_lo, sp_hi, sp_peak;
+  // Site heap: two halves of hsize bytes; allocation bumps hb inside the
+  // current half, and a full half is compacted into the other one.
+  long long h_lo0, h_lo1, hsize, hb, he;
+  int half;
+  int compactions;
+  long long h_peak;
+  // Shared-memory workspace for small SVDs.
+  double* sws;
+  long long sws_doubles;
+  double* acct;   // [flops, bytes] (global, leader-updated)
+  int status;     // uniform copy of the instance status
   int* trace;
   int trace_cap;
 };
 
 // ---------------------------------------------------------------------------
-// status
+// status: C.status is identical in every thread (uniform control flow);
+// ctl[CTL_STATUS] is the global copy reported to the host.
 // ---------------------------------------------------------------------------
-CATN_HD void set_status_leader(Ctx& C, int code) {
+CATN_HD void fail_all(Ctx& C, int code) {   // called by every thread alike
+  if (C.status == 0) C.status = code;
+  if (C.T.leader() && C.ctl[CTL_STATUS] == 0) C.ctl[CTL_STATUS] = code;
+}
+CATN_HD void fail_leader(Ctx& C, int code) {   // inside leader-only blocks
   if (C.ctl[CTL_STATUS] == 0) C.ctl[CTL_STATUS] = code;
 }
-CATN_HDI inline void set_status(Ctx& C, int code) {
+// After a leader-only block that may have failed: make the status uniform.
+CATN_HDI inline void refresh_status(Ctx& C) {
   C.T.sync();
-  if (C.T.leader()) set_status_leader(C, code);
+  C.status = C.ctl[CTL_STATUS];
   C.T.sync();
 }
-CATN_HD int failed(const Ctx& C) { return C.ctl[CTL_STATUS] != 0; }
+CATN_HD int failed(const Ctx& C) { return C.status != 0; }
 
 // ---------------------------------------------------------------------------
-// arena: power-of-two classes, per-class free lists, bump allocation
+// memory
 // ---------------------------------------------------------------------------
-CATN_HD int size_class(long long bytes) {
-  int c = 0;
-  long long s = 64;
-  while (s < bytes) { s <<= 1; ++c; }
-  return c;
-}
+CATN_HD long long al256(long long b) { return (b + 255) & ~255LL; }
 
-// Leader-only allocation (no barrier).  Returns -1 and sets the status on failure.
-CATN_HD long long aalloc_leader(Ctx& C, long long bytes) {
-  if (bytes <= 0) bytes = 8;
-  int c = size_class(bytes);
-  long long off = -1;
-  if (c < CATN_NCLS) {
-    if (C.ameta[1 + c] >= 0) {
-      off = C.ameta[1 + c];
-      C.ameta[1 + c] = *(long long*)(C.base + off);
-    } else {
-      long long sz = 64LL << c;
-      if (C.ameta[0] + sz <= C.cap) {
-        off = C.ameta[0];
-        C.ameta[0] += sz;
-        if (C.ameta[0] > C.ameta[CATN_NCLS + 1]) C.ameta[CATN_NCLS + 1] = C.ameta[0];
-      }
-    }
+CATN_HD double* spush(Ctx& C, long long ndoubles) {
+  long long bytes = al256(8 * (ndoubles > 0 ? ndoubles : 1));
+  if (C.sp + bytes > C.sp_hi) {
+    fail_all(C, CATN_ENOMEM);
+    return nullptr;
   }
-  if (off < 0) set_status_leader(C, CATN_ENOMEM);
-  return off;
+  double* p = (double*)(C.base + C.sp);
+  C.sp += bytes;
+  if (C.sp > C.sp_peak) C.sp_peak = C.sp;
+  return p;
 }
-CATN_HD void afree_leader(Ctx& C, long long off, long long bytes) {
-  if (off < 0) return;
-  if (bytes <= 0) bytes = 8;
-  int c = size_class(bytes);
-  *(long long*)(C.base + off) = C.ameta[1 + c];
-  C.ameta[1 + c] = off;
-}
-// Team allocation: every thread receives the offset.
-CATN_HDI inline long long aalloc(Ctx& C, long long bytes) {
-  long long off = 0;
-  C.T.sync();
-  if (C.T.leader()) off = aalloc_leader(C, bytes);
-  return C.T.bcast(off);
-}
-// Team free: the block must no longer be in use by any thread.
-CATN_HDI inline void afree(Ctx& C, long long off, long long bytes) {
-  C.T.sync();
-  if (C.T.leader()) afree_leader(C, off, bytes);
-  C.T.sync();
-}
-CATN_HD double* dptr(const Ctx& C, long long off) { return (double*)(C.base + off); }
-CATN_HD int* iptr(const Ctx& C, long long off) { return (int*)(C.base + off); }
 
-// ---------------------------------------------------------------------------
-// node / site / neighbour accessors (positions are 1-based)
-// ---------------------------------------------------------------------------
+CATN_HD double* dptr(const Ctx& C, long long off) { return (double*)(C.base + off); }
 CATN_HD SiteRef& sref(const Ctx& C, int k, int pos) {
   return C.site[(long long)k * C.maxs + (pos - 1)];
 }
@@ -133,7 +113,71 @@ CATN_HD long long sbytes(const SiteRef& s) { return 8LL * s.dl * s.d * s.dr; }
 CATN_HD SiteRef mksite(int dl, int d, int dr, long long off) {
   SiteRef s; s.dl = dl; s.d = d; s.dr = dr; s.pad = 0; s.off = off; return s;
 }
+CATN_HD double* sdata(const Ctx& C, const SiteRef& s) { return (double*)(C.base + s.off); }
 
+// Move every live site into the other heap half, contiguously.
+CATN_HDI inline void heap_compact(Ctx& C) {
+  const Team& T = C.T;
+  T.sync();
+  const long long lo = C.half ? C.h_lo0 : C.h_lo1;
+  long long cur = lo;
+  for (int k = 1; k <= C.n; ++k) {
+    const int ns = C.node[k].nsites;
+    for (int p = 1; p <= ns; ++p) {
+      SiteRef s = sref(C, k, p);
+      const long long sz = (long long)s.dl * s.d * s.dr;
+      const double* src = dptr(C, s.off);
+      double* dst = dptr(C, cur);
+      for (long long e = T.rank(); e < sz; e += T.size()) dst[e] = src[e];
+      cur += al256(8 * sz);
+    }
+  }
+  T.sync();
+  if (T.leader()) {
+    long long c2 = lo;
+    for (int k = 1; k <= C.n; ++k) {
+      const int ns = C.node[k].nsites;
+      for (int p = 1; p <= ns; ++p) {
+        SiteRef& s = sref(C, k, p);
+        s.off = c2;
+        c2 += al256(sbytes(s));
+      }
+    }
+  }
+  T.sync();
+  C.half ^= 1;
+  C.hb = cur;
+  C.he = lo + C.hsize;
+  C.compactions += 1;
+}
+
+// Make room for `bytes` of new sites (may compact: re-read site refs after).
+CATN_HDI inline bool heap_reserve(Ctx& C, long long bytes) {
+  if (C.hb + bytes <= C.he) return true;
+  heap_compact(C);
+  if (C.hb + bytes <= C.he) return true;
+  fail_all(C, CATN_ENOMEM);
+  return false;
+}
+CATN_HD long long heap_take(Ctx& C, long long bytes) {
+  long long off = C.hb;
+  C.hb += al256(bytes);
+  long long used = C.hb - (C.half ? C.h_lo1 : C.h_lo0);
+  if (used > C.h_peak) C.h_peak = used;
+  return off;
+}
+
+// Algorithmic work counters.
+CATN_HD void account(Ctx& C, double flops, double bytes) {
+  if (C.T.leader()) {
+    C.acct[0] += flops;
+    C.acct[1] += bytes;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// neighbour accessors (positions are 1-based)
+// ---------------------------------------------------------------------------
 // find_neighbor (mps_node.jl:257-260): first match, 1-based, 0 = absent.
 CATN_HD int nb_find(const Ctx& C, int k, int j) {
   int nn = C.node[k].nnbr;
@@ -149,7 +193,7 @@ CATN_HD void nb_delete_at_leader(Ctx& C, int k, int pos) {
 }
 CATN_HD void nb_insert_at_leader(Ctx& C, int k, int pos, int v) {
   int nn = C.node[k].nnbr;
-  if (nn >= C.maxs) { set_status_leader(C, CATN_ENOMEM); return; }
+  if (nn >= C.maxs) { fail_leader(C, CATN_ENOMEM); return; }
   for (int p = nn; p >= pos; --p) nbref(C, k, p + 1) = nbref(C, k, p);
   nbref(C, k, pos) = v;
   C.node[k].nnbr = nn + 1;
@@ -172,116 +216,127 @@ CATN_HD double logdim_all(const Ctx& C, int k) {
 }
 CATN_HD double logdim_at(const Ctx& C, int k, int p) { return log2((double)sref(C, k, p).d); }
 
+
 // ---------------------------------------------------------------------------
-// thin SVD with ownership of the input buffer
+// thin SVD (workspace in shared memory when it fits, else scratch)
 // ---------------------------------------------------------------------------
 struct Svd {
-  long long U, S, V;   // arena offsets: U (m x p), S (p), V (n x p), column-major
+  double* U;   // m x p, column-major
+  double* S;   // p, descending
+  double* V;   // n x p
   long long m, n, p;
 };
 
-CATN_HDI inline void svd_free(Ctx& C, const Svd& R) {
-  afree(C, R.U, 8 * R.m * R.p);
-  afree(C, R.S, 8 * R.p);
-  afree(C, R.V, 8 * R.n * R.p);
+// Oriented input: W (mm x nn, mm >= nn) holds A (m x n) or A^T when m < n.
+struct SvdIn {
+  double* W;
+  long long m, n, mm, nn;
+  bool wide, smem;
+};
+
+CATN_HD long long svd_ws_doubles(long long mm, long long nn) {
+  return 2 * mm * nn + 3 * nn * nn + 8 * nn + 64;
 }
 
-// SVD of the m x n column-major matrix in arena buffer `a` (allocated with
-// `a_bytes`), which is consumed.  S is sorted descending.
-//
-// Method (Drmac-Veselic preconditioned one-sided Jacobi): pivoted
-// Householder QR  W P = Q R  of the tall orientation W (A or A^T), then
-// one-sided Jacobi on X = R^T, X V' = U' Sigma, giving R = V' Sigma U'^T and
+CATN_HDI inline SvdIn svd_begin(Ctx& C, long long m, long long n) {
+  SvdIn s;
+  s.m = m;
+  s.n = n;
+  s.wide = m < n;
+  s.mm = s.wide ? n : m;
+  s.nn = s.wide ? m : n;
+  s.smem = svd_ws_doubles(s.mm, s.nn) <= C.sws_doubles;
+  s.W = s.smem ? C.sws : spush(C, s.mm * s.nn);
+  return s;
+}
+// Operand map that writes A(r, c) into the oriented W.
+CATN_HD MOp svd_target(const SvdIn& s) {
+  return s.wide ? mop(s.W, cols_plain(s.mm), rows_plain()) : colmajor(s.W, s.mm);
+}
+CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
+  const Team& T = C.T;
+  for (long long e = T.rank(); e < s.mm * s.nn; e += T.size()) {
+    long long r = e % s.mm, c = e / s.mm;
+    s.W[e] = s.wide ? A.ld(c, r) : A.ld(r, c);
+  }
+  T.sync();
+}
+
+// Drmac-Veselic preconditioned one-sided Jacobi: pivoted Householder QR
+// W P = Q R, one-sided Jacobi on X = R^T (X V' = U' Sigma), so that
 // W = (Q V') Sigma (P U')^T.  The pivoted, transposed triangle converges in
 // a handful of sweeps even for strongly graded spectra.
-CATN_HDI inline Svd svd_full(Ctx& C, long long a, long long a_bytes, long long m, long long n) {
+CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   const Team& T = C.T;
   Svd R;
-  R.m = m; R.n = n; R.p = 0; R.U = R.S = R.V = -1;
-  const bool wide = m < n;
-  const long long mm = wide ? n : m, nn = wide ? m : n;
-  long long work = a, work_bytes = a_bytes;
-  if (wide) {
-    work = aalloc(C, 8 * mm * nn);
-    if (work < 0) { afree(C, a, a_bytes); return R; }
-    materialize(T, dptr(C, work), mm, nn, mm, transposed(dptr(C, a), m));
-    afree(C, a, a_bytes);
-    work_bytes = 8 * mm * nn;
+  R.m = s.m; R.n = s.n; R.p = 0; R.U = R.S = R.V = nullptr;
+  if (failed(C) || !s.W) return R;
+  const long long mm = s.mm, nn = s.nn;
+  double *X, *Vb, *Ut, *Vt, *tau, *nrm, *sig, *Sout;
+  int *piv, *perm;
+  if (s.smem) {
+    double* q = s.W + mm * nn;
+    X = q; q += nn * nn;
+    Vb = q; q += nn * nn;
+    Vt = q; q += nn * nn;
+    Ut = q; q += mm * nn;
+    tau = q; q += nn;
+    nrm = q; q += nn;
+    sig = q; q += nn;
+    Sout = q; q += nn;
+    piv = (int*)q; q += (nn + 1) / 2 + 1;
+    perm = (int*)q;
+  } else {
+    X = spush(C, nn * nn);
+    Vb = spush(C, nn * nn);
+    Vt = spush(C, nn * nn);
+    Ut = spush(C, mm * nn);
+    tau = spush(C, nn);
+    nrm = spush(C, nn);
+    sig = spush(C, nn);
+    Sout = spush(C, nn);
+    piv = (int*)spush(C, (nn + 1) / 2 + 1);
+    perm = (int*)spush(C, (nn + 1) / 2 + 1);
+    if (failed(C)) return R;
   }
-  long long tau = aalloc(C, 8 * nn);
-  long long piv = aalloc(C, 4 * nn);
-  long long nrm = aalloc(C, 8 * nn);
-  long long X = aalloc(C, 8 * nn * nn);
-  long long Vb = aalloc(C, 8 * nn * nn);
-  long long sig = aalloc(C, 8 * nn);
-  long long Sout = aalloc(C, 8 * nn);
-  long long perm = aalloc(C, 4 * nn);
-  if (tau < 0 || piv < 0 || nrm < 0 || X < 0 || Vb < 0 || sig < 0 || Sout < 0 || perm < 0) return R;
-  qrcp_inplace(T, dptr(C, work), mm, nn, mm, dptr(C, tau), iptr(C, piv), dptr(C, nrm));
-  {
-    const double* W = dptr(C, work);
-    double* Xp = dptr(C, X);
-    for (long long e = T.rank(); e < nn * nn; e += T.size()) {
-      long long i = e % nn, j = e / nn;
-      Xp[e] = (j <= i) ? W[j + i * mm] : 0.0;   // X = R^T
-    }
-    T.sync();
+  qrcp_inplace(T, s.W, mm, nn, mm, tau, piv, nrm);
+  for (long long e = T.rank(); e < nn * nn; e += T.size()) {
+    long long i = e % nn, j = e / nn;
+    X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
   }
-  int sweeps = jacobi_sweeps(T, dptr(C, X), nn, nn, nn, dptr(C, Vb), 60);
-  if (T.leader()) {
-    if (sweeps < 0) set_status_leader(C, CATN_ENOCONV);
-    else if (sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
+  T.sync();
+  int sweeps = jacobi_sweeps(T, X, nn, nn, nn, Vb, 60);
+  if (sweeps < 0) fail_all(C, CATN_ENOCONV);
+  if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
+  sort_columns(T, X, nn, nn, nn, sig, Sout, perm);
+  for (long long e = T.rank(); e < mm * nn; e += T.size()) {
+    long long r = e % mm, c = e / mm;
+    Ut[e] = (r < nn) ? Vb[r + (long long)perm[c] * nn] : 0.0;
   }
-  sort_columns(T, dptr(C, X), nn, nn, nn, dptr(C, sig), dptr(C, Sout), iptr(C, perm));
-  long long Ut = aalloc(C, 8 * mm * nn);   // left vectors of W: Q V'[:, perm]
-  long long Vt = aalloc(C, 8 * nn * nn);   // right vectors of W: P U'[:, perm]
-  if (Ut < 0 || Vt < 0) return R;
-  {
-    const double* Xp = dptr(C, X);
-    const double* Sp = dptr(C, Sout);
-    const int* pp = iptr(C, perm);
-    const int* pv = iptr(C, piv);
-    const double* Vp = dptr(C, Vb);
-    double* Up = dptr(C, Ut);
-    double* Wp = dptr(C, Vt);
-    for (long long e = T.rank(); e < mm * nn; e += T.size()) {
-      long long r = e % mm, c = e / mm;
-      Up[e] = (r < nn) ? Vp[r + (long long)pp[c] * nn] : 0.0;
-    }
-    for (long long e = T.rank(); e < nn * nn; e += T.size()) {
-      long long i = e % nn, c = e / nn;
-      double s = Sp[c];
-      double v = (s > 0.0) ? Xp[i + (long long)pp[c] * nn] / s : 0.0;
-      Wp[(long long)pv[i] + c * nn] = v;
-    }
-    T.sync();
+  for (long long e = T.rank(); e < nn * nn; e += T.size()) {
+    long long i = e % nn, c = e / nn;
+    double sv = Sout[c];
+    Vt[(long long)piv[i] + c * nn] = (sv > 0.0) ? X[i + (long long)perm[c] * nn] / sv : 0.0;
   }
-  qr_apply_q(T, dptr(C, work), mm, nn, mm, dptr(C, tau), dptr(C, Ut), nn, mm);
-  afree(C, tau, 8 * nn);
-  afree(C, piv, 4 * nn);
-  afree(C, nrm, 8 * nn);
-  afree(C, X, 8 * nn * nn);
-  afree(C, Vb, 8 * nn * nn);
-  afree(C, sig, 8 * nn);
-  afree(C, perm, 4 * nn);
-  afree(C, work, work_bytes);
+  T.sync();
+  qr_apply_q(T, s.W, mm, nn, mm, tau, Ut, nn, mm);
   R.p = nn;
   R.S = Sout;
-  if (!wide) {
-    R.U = Ut;   // m x p
-    R.V = Vt;   // n x p
+  if (!s.wide) {
+    R.U = Ut;
+    R.V = Vt;
   } else {
-    R.U = Vt;   // m x m
-    R.V = Ut;   // n x m
+    R.U = Vt;
+    R.V = Ut;
   }
   return R;
 }
 
 // tsvd keep rule (linalg_utils.jl:22-26): nkeep = count(S > cutoff), 0 -> 1,
-// capped by maxdim; returns the discarded sum of singular values.
+// capped by maxdim; *disc = sum of the discarded singular values.
 CATN_HDI inline int keep_rule(Ctx& C, const Svd& R, double cutoff, long long maxdim, double* disc) {
   const Team& T = C.T;
-  const double* S = dptr(C, R.S);
+  const double* S = R.S;
   double cnt = 0.0;
   for (long long e = T.rank(); e < R.p; e += T.size()) cnt += (S[e] > cutoff) ? 1.0 : 0.0;
   long long count = (long long)(T.sum(cnt) + 0.5);
@@ -296,9 +351,8 @@ CATN_HDI inline int keep_rule(Ctx& C, const Svd& R, double cutoff, long long max
 // cano_to! keep rule (mps_node.jl:80-81): count(S > cutoff), all when none pass.
 CATN_HDI inline int keep_all_if_none(Ctx& C, const Svd& R, double cutoff) {
   const Team& T = C.T;
-  const double* S = dptr(C, R.S);
   double cnt = 0.0;
-  for (long long e = T.rank(); e < R.p; e += T.size()) cnt += (S[e] > cutoff) ? 1.0 : 0.0;
+  for (long long e = T.rank(); e < R.p; e += T.size()) cnt += (R.S[e] > cutoff) ? 1.0 : 0.0;
   long long count = (long long)(T.sum(cnt) + 0.5);
   return (int)(count == 0 ? R.p : count);
 }
@@ -314,58 +368,66 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
   if (h.cano < idx) {
     for (int i = h.cano; i < idx; ++i) {
       if (failed(C)) return;
-      SiteRef s = sref(C, k, i), nx = sref(C, k, i + 1);
-      long long m = (long long)s.dl * s.d, n = s.dr;
-      Svd R = svd_full(C, s.off, sbytes(s), m, n);
-      if (R.p == 0) return;
-      int nkeep = keep_all_if_none(C, R, C.P.cutoff);
-      long long ni = aalloc(C, 8 * m * nkeep);
-      long long nn2 = aalloc(C, 8LL * nkeep * nx.d * nx.dr);
-      if (ni < 0 || nn2 < 0) return;
-      copy(T, dptr(C, ni), dptr(C, R.U), m * nkeep);
+      const long long mark = C.sp;
+      SiteRef s = sref(C, k, i);
+      const long long m = (long long)s.dl * s.d, n = s.dr;
+      SvdIn in = svd_begin(C, m, n);
+      if (failed(C)) return;
+      svd_fill(C, in, colmajor(sdata(C, s), m));
+      Svd R = svd_finish(C, in);
+      if (failed(C)) return;
+      const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
+      SiteRef nx = sref(C, k, i + 1);
+      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * nkeep * nx.d * nx.dr))) return;
+      nx = sref(C, k, i + 1);
+      const long long ni = heap_take(C, 8 * m * nkeep);
+      const long long nn2 = heap_take(C, 8LL * nkeep * nx.d * nx.dr);
+      copy(T, dptr(C, ni), R.U, m * nkeep);
       // next <- (S V^H)[1:nkeep, :] * next
-      gemm(T, nkeep, (long long)nx.d * nx.dr, n,
-           mop(dptr(C, R.V), imap(1, 0, n), rows_plain(), dptr(C, R.S), nullptr),
-           colmajor(dptr(C, nx.off), n), colmajor(dptr(C, nn2), nkeep));
-      svd_free(C, R);
-      afree(C, nx.off, sbytes(nx));
+      gemm(T, nkeep, (long long)nx.d * nx.dr, n, mop(R.V, imap(1, 0, n), rows_plain(), R.S, nullptr),
+           colmajor(sdata(C, nx), n), colmajor(dptr(C, nn2), nkeep));
+      account(C, 2.0 * m * n * n + 2.0 * n * n * nx.d * nx.dr,
+              8.0 * (m * n + (double)n * nx.d * nx.dr + m * nkeep + (double)nkeep * nx.d * nx.dr));
       if (T.leader()) {
         sref(C, k, i) = mksite(s.dl, s.d, nkeep, ni);
         sref(C, k, i + 1) = mksite(nkeep, nx.d, nx.dr, nn2);
         C.node[k].cano = i + 1;
       }
       T.sync();
+      C.sp = mark;
     }
   } else {
     for (int i = h.cano; i > idx; --i) {
       if (failed(C)) return;
-      SiteRef s = sref(C, k, i), pv = sref(C, k, i - 1);
+      const long long mark = C.sp;
+      SiteRef s = sref(C, k, i);
       const long long dl = s.dl, m = (long long)s.d * s.dr;
-      long long w = aalloc(C, 8 * m * dl);
-      if (w < 0) return;
       // Mt = permutedims(site, (2,3,1)) as (d*dr) x dl = transpose of the dl x (d*dr) view
-      materialize(T, dptr(C, w), m, dl, m, transposed(dptr(C, s.off), dl));
-      afree(C, s.off, sbytes(s));
-      Svd R = svd_full(C, w, 8 * m * dl, m, dl);
-      if (R.p == 0) return;
-      int nkeep = keep_all_if_none(C, R, C.P.cutoff);
-      long long ni = aalloc(C, 8 * m * nkeep);
-      long long np = aalloc(C, 8LL * pv.dl * pv.d * nkeep);
-      if (ni < 0 || np < 0) return;
+      SvdIn in = svd_begin(C, m, dl);
+      if (failed(C)) return;
+      svd_fill(C, in, transposed(sdata(C, s), dl));
+      Svd R = svd_finish(C, in);
+      if (failed(C)) return;
+      const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
+      SiteRef pv = sref(C, k, i - 1);
+      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * pv.dl * pv.d * nkeep))) return;
+      pv = sref(C, k, i - 1);
+      const long long ni = heap_take(C, 8 * m * nkeep);
+      const long long np = heap_take(C, 8LL * pv.dl * pv.d * nkeep);
       // new site = permutedims(reshape(U[:, 1:nkeep], d, dr, nkeep), (3,1,2)) = U^T
-      materialize(T, dptr(C, ni), nkeep, m, nkeep, transposed(dptr(C, R.U), m));
+      materialize(T, dptr(C, ni), nkeep, m, nkeep, transposed(R.U, m));
       // prev <- prev * (S V^H)^T
-      gemm(T, (long long)pv.dl * pv.d, nkeep, dl, colmajor(dptr(C, pv.off), (long long)pv.dl * pv.d),
-           mop(dptr(C, R.V), rows_plain(), cols_plain(dl), nullptr, dptr(C, R.S)),
-           colmajor(dptr(C, np), (long long)pv.dl * pv.d));
-      svd_free(C, R);
-      afree(C, pv.off, sbytes(pv));
+      gemm(T, (long long)pv.dl * pv.d, nkeep, dl, colmajor(sdata(C, pv), (long long)pv.dl * pv.d),
+           mop(R.V, rows_plain(), cols_plain(dl), nullptr, R.S), colmajor(dptr(C, np), (long long)pv.dl * pv.d));
+      account(C, 2.0 * m * dl * dl + 2.0 * dl * dl * pv.dl * pv.d,
+              8.0 * (m * dl + (double)pv.dl * pv.d * dl + m * nkeep + (double)pv.dl * pv.d * nkeep));
       if (T.leader()) {
         sref(C, k, i) = mksite(nkeep, s.d, s.dr, ni);
         sref(C, k, i - 1) = mksite(pv.dl, pv.d, nkeep, np);
         C.node[k].cano = i - 1;
       }
       T.sync();
+      C.sp = mark;
     }
   }
 }
@@ -378,7 +440,7 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   NodeHdr h = C.node[k];
   int dij = i - j;
   if ((dij != 1 && dij != -1) || i < 1 || j < 1 || i > h.nsites || j > h.nsites) {
-    set_status(C, CATN_ESTATE);
+    fail_all(C, CATN_ESTATE);
     return 0.0;
   }
   if (h.cano != i && h.cano != j) {
@@ -388,20 +450,23 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
     cano_to(C, k, ai < aj ? i : j);
     if (failed(C)) return 0.0;
   }
+  const long long mark = C.sp;
   const int lo = i < j ? i : j, hi = i < j ? j : i;
   SiteRef tl = sref(C, k, lo), tr = sref(C, k, hi);
   const long long d0 = tl.dl, d1 = tr.d, d2 = tl.d, d3 = tr.dr, kk = tl.dr;
   const long long m = d0 * d1, n = d2 * d3;
-  long long Mb = aalloc(C, 8 * m * n);
-  if (Mb < 0) return 0.0;
-  // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3)
-  gemm(T, d0 * d2, d1 * d3, kk, colmajor(dptr(C, tl.off), d0 * d2), colmajor(dptr(C, tr.off), kk),
-       mop(dptr(C, Mb), imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2)));
-  afree(C, tl.off, sbytes(tl));
-  afree(C, tr.off, sbytes(tr));
+  SvdIn in = svd_begin(C, m, n);
+  if (failed(C)) return 0.0;
+  // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
+  // straight into the SVD's oriented input.
+  {
+    MOp out = in.wide ? mop(in.W, imap((int)d0, n, 1), imap((int)d1, n * d0, d2))
+                      : mop(in.W, imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2));
+    gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
+  }
   const bool rsvd_route = C.P.swapopt && ((m > 7000 && n > 7000) || m > 20000 || n > 20000);
-  Svd R = svd_full(C, Mb, 8 * m * n, m, n);
-  if (R.p == 0) return 0.0;
+  Svd R = svd_finish(C, in);
+  if (failed(C)) return 0.0;
   double err = 0.0;
   int myd;
   if (rsvd_route) {
@@ -412,19 +477,18 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   } else {
     myd = keep_rule(C, R, C.P.cutoff, C.P.chi, &err);
   }
-  long long nl = aalloc(C, 8 * m * myd);
-  long long nr = aalloc(C, 8 * n * myd);
-  if (nl < 0 || nr < 0) return err;
+  if (!heap_reserve(C, al256(8 * m * myd) + al256(8 * n * myd))) return err;
+  const long long nl = heap_take(C, 8 * m * myd);
+  const long long nr = heap_take(C, 8 * n * myd);
   if (i < j) {
-    copy(T, dptr(C, nl), dptr(C, R.U), m * myd);
-    materialize(T, dptr(C, nr), myd, n, myd,
-                mop(dptr(C, R.V), imap(1, 0, n), rows_plain(), dptr(C, R.S), nullptr));
+    copy(T, dptr(C, nl), R.U, m * myd);
+    materialize(T, dptr(C, nr), myd, n, myd, mop(R.V, imap(1, 0, n), rows_plain(), R.S, nullptr));
   } else {
-    materialize(T, dptr(C, nl), m, myd, m,
-                mop(dptr(C, R.U), rows_plain(), cols_plain(m), nullptr, dptr(C, R.S)));
-    materialize(T, dptr(C, nr), myd, n, myd, mop(dptr(C, R.V), imap(1, 0, n), rows_plain()));
+    materialize(T, dptr(C, nl), m, myd, m, mop(R.U, rows_plain(), cols_plain(m), nullptr, R.S));
+    materialize(T, dptr(C, nr), myd, n, myd, mop(R.V, imap(1, 0, n), rows_plain()));
   }
-  svd_free(C, R);
+  account(C, 2.0 * m * n * kk + 4.0 * m * n * myd,
+          8.0 * ((double)d0 * d2 * kk + (double)kk * d1 * d3 + (double)m * myd + (double)myd * n));
   if (T.leader()) {
     sref(C, k, lo) = mksite((int)d0, (int)d1, myd, nl);
     sref(C, k, hi) = mksite(myd, (int)d2, (int)d3, nr);
@@ -434,6 +498,7 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
     nbref(C, k, j) = t;
   }
   T.sync();
+  C.sp = mark;
   return err;
 }
 
@@ -471,34 +536,38 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
   NodeHdr h = C.node[k];
   if (h.nsites <= 1) return;
   const int ns = h.nsites;
-  long long* offs = (long long*)(C.pairs);   // scratch: new offsets per site
-  T.sync();
-  if (T.leader()) {
-    for (int p = 1; p <= ns; ++p) offs[p - 1] = aalloc_leader(C, sbytes(sref(C, k, p)));
+  long long total = 0;
+  for (int p = 1; p <= ns; ++p) total += al256(sbytes(sref(C, k, p)));
+  if (!heap_reserve(C, total)) return;
+  const long long first = C.hb;
+  C.hb += total;
+  {
+    long long used = C.hb - (C.half ? C.h_lo1 : C.h_lo0);
+    if (used > C.h_peak) C.h_peak = used;
   }
-  T.sync();
-  if (failed(C)) return;
+  long long cur = first;
   for (int p = 1; p <= ns; ++p) {
     SiteRef s = sref(C, k, p);
-    const double* src = dptr(C, s.off);
-    double* dst = dptr(C, offs[p - 1]);
+    const double* src = sdata(C, s);
+    double* dst = dptr(C, cur);
     const long long dl = s.dl, d = s.d, dr = s.dr, tot = dl * d * dr;
     for (long long e = T.rank(); e < tot; e += T.size()) {
       long long a = e % dl, rest = e / dl, b = rest % d, c = rest / d;
       dst[c + dr * (b + d * a)] = src[e];
     }
+    cur += al256(8 * tot);
   }
   T.sync();
   if (T.leader()) {
-    for (int p = 1; p <= ns; ++p) afree_leader(C, sref(C, k, p).off, sbytes(sref(C, k, p)));
-    for (int p = 1; p <= ns / 2; ++p) {
-      SiteRef a = sref(C, k, p), b = sref(C, k, ns + 1 - p);
-      sref(C, k, p) = b;
-      sref(C, k, ns + 1 - p) = a;
-    }
+    // old site p was copied (transposed) to `first + sum of earlier sizes`;
+    // it becomes position ns + 1 - p
+    SiteRef* old = (SiteRef*)C.pairs;
+    for (int p = 1; p <= ns; ++p) old[p - 1] = sref(C, k, p);
+    long long c2 = first;
     for (int p = 1; p <= ns; ++p) {
-      SiteRef s = sref(C, k, p);
-      sref(C, k, p) = mksite(s.dr, s.d, s.dl, offs[ns - p]);
+      const SiteRef s = old[p - 1];
+      sref(C, k, ns + 1 - p) = mksite(s.dr, s.d, s.dl, c2);
+      c2 += al256(sbytes(s));
     }
     int nn = C.node[k].nnbr;
     for (int p = 1; p <= nn / 2; ++p) {
@@ -511,12 +580,10 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
   T.sync();
 }
 
-// Free every site of node k and empty its lists (clear!, mps_node.jl:335-339).
+// clear! (mps_node.jl:335-339)
 CATN_HDI inline void clear_node(Ctx& C, int k) {
   C.T.sync();
   if (C.T.leader()) {
-    int ns = C.node[k].nsites;
-    for (int p = 1; p <= ns; ++p) afree_leader(C, sref(C, k, p).off, sbytes(sref(C, k, p)));
     C.node[k].nsites = 0;
     C.node[k].nnbr = 0;
   }
@@ -546,7 +613,7 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
     }
   }
   if (found != 2) {
-    set_status(C, CATN_ESTATE);
+    fail_all(C, CATN_ESTATE);
     return 0.0;
   }
   int target = cross ? idx1 : idx1 + 1;
@@ -558,13 +625,13 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
   cano_to(C, k, idx1);
   if (failed(C)) return err;
   SiteRef a = sref(C, k, idx1), b = sref(C, k, idx1 + 1);
-  long long rows = (long long)a.dl * a.d, cols = (long long)b.d * b.dr;
-  long long f = aalloc(C, 8 * rows * cols);
-  if (f < 0) return err;
-  gemm(T, rows, cols, a.dr, colmajor(dptr(C, a.off), rows), colmajor(dptr(C, b.off), a.dr),
-       colmajor(dptr(C, f), rows));
-  afree(C, a.off, sbytes(a));
-  afree(C, b.off, sbytes(b));
+  const long long rows = (long long)a.dl * a.d, cols = (long long)b.d * b.dr;
+  if (!heap_reserve(C, al256(8 * rows * cols))) return err;
+  a = sref(C, k, idx1);
+  b = sref(C, k, idx1 + 1);
+  const long long f = heap_take(C, 8 * rows * cols);
+  gemm(T, rows, cols, a.dr, colmajor(sdata(C, a), rows), colmajor(sdata(C, b), a.dr), colmajor(dptr(C, f), rows));
+  account(C, 2.0 * rows * a.dr * cols, 8.0 * ((double)rows * a.dr + (double)a.dr * cols + (double)rows * cols));
   if (T.leader()) {
     sref(C, k, idx1) = mksite(a.dl, a.d * b.d, b.dr, f);
     site_delete_at_leader(C, k, idx1 + 1);
@@ -584,18 +651,17 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   NodeHdr hi = C.node[ki];
   if (hi.nsites == 1) {
     // (a) both leaves: non-conjugating dot product
-    if (C.node[kj].nsites != 1) { set_status(C, CATN_ESTATE); return 0.0; }
+    if (C.node[kj].nsites != 1) { fail_all(C, CATN_ESTATE); return 0.0; }
     SiteRef si = sref(C, ki, 1), sj = sref(C, kj, 1);
     long long d = si.d;
     double loc = 0.0;
-    const double* vi = dptr(C, si.off);
-    const double* vj = dptr(C, sj.off);
+    const double* vi = sdata(C, si);
+    const double* vj = sdata(C, sj);
     for (long long e = T.rank(); e < d; e += T.size()) loc = fma(vi[e], vj[e], loc);
     double r = T.sum(loc);
     double absr = fabs(r);
     T.sync();
     if (T.leader()) {
-      afree_leader(C, si.off, sbytes(si));
       C.node[ki].nsites = 0;
       nb_delete_at_leader(C, ki, idx);
     }
@@ -607,23 +673,22 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   *err += move2tail(C, ki, idx);
   if (failed(C)) return 0.0;
   hi = C.node[ki];
-  SiteRef last = sref(C, ki, hi.nsites);   // (dl, d, 1)
-  SiteRef prev = sref(C, ki, hi.nsites - 1);
+  const long long mark = C.sp;
   if (C.node[kj].nsites == 1) {
-    // (b) j is a leaf
-    SiteRef tj = sref(C, kj, 1);
-    long long vbuf = aalloc(C, 8LL * last.dl);
-    long long nt = aalloc(C, 8LL * prev.dl * prev.d);
-    if (vbuf < 0 || nt < 0) return 0.0;
-    gemm(T, last.dl, 1, last.d, colmajor(dptr(C, last.off), last.dl), colmajor(dptr(C, tj.off), last.d),
-         colmajor(dptr(C, vbuf), last.dl));
-    gemm(T, (long long)prev.dl * prev.d, 1, prev.dr, colmajor(dptr(C, prev.off), (long long)prev.dl * prev.d),
-         colmajor(dptr(C, vbuf), prev.dr), colmajor(dptr(C, nt), (long long)prev.dl * prev.d));
-    afree(C, vbuf, 8LL * last.dl);
+    // (b) j is a leaf: mat = mati * matj, folded into mps[end-1]
+    SiteRef last = sref(C, ki, hi.nsites), tj = sref(C, kj, 1);
+    double* vbuf = spush(C, last.dl);
+    if (failed(C)) return 0.0;
+    gemm(T, last.dl, 1, last.d, colmajor(sdata(C, last), last.dl), colmajor(sdata(C, tj), last.d),
+         colmajor(vbuf, last.dl));
+    SiteRef prev = sref(C, ki, hi.nsites - 1);
     const long long ne = (long long)prev.dl * prev.d;
-    double nrm = norm_of(C, dptr(C, nt), ne);
-    afree(C, last.off, sbytes(last));
-    afree(C, prev.off, sbytes(prev));
+    if (!heap_reserve(C, al256(8 * ne))) return 0.0;
+    prev = sref(C, ki, hi.nsites - 1);
+    const long long nt = heap_take(C, 8 * ne);
+    gemm(T, ne, 1, prev.dr, colmajor(sdata(C, prev), ne), colmajor(vbuf, prev.dr), colmajor(dptr(C, nt), ne));
+    account(C, 2.0 * last.dl * last.d + 2.0 * ne * prev.dr, 8.0 * ((double)last.dl * last.d + ne * prev.dr + ne));
+    const double nrm = norm_of(C, dptr(C, nt), ne);
     if (T.leader()) {
       sref(C, ki, hi.nsites - 1) = mksite(prev.dl, prev.d, 1, nt);
       C.node[ki].cano = C.node[ki].cano - 1;
@@ -631,6 +696,7 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
       C.node[ki].nnbr = C.node[ki].nnbr - 1;
     }
     T.sync();
+    C.sp = mark;
     if (nrm <= cutoff) return 0.0;
     scale(T, dptr(C, nt), 1.0 / nrm, ne);
     return log(nrm);
@@ -638,108 +704,95 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   // (c) general
   *err += move2head(C, kj, idxi);
   if (failed(C)) return 0.0;
-  SiteRef hj = sref(C, kj, 1);   // (1, d, drj)
+  SiteRef last = sref(C, ki, hi.nsites);   // (Dl, dd, 1)
+  SiteRef hj = sref(C, kj, 1);              // (1, dd, Dr)
   const long long Dl = last.dl, dd = last.d, Dr = hj.dr;
-  long long mat = aalloc(C, 8 * Dl * Dr);
-  long long nt = aalloc(C, 8LL * prev.dl * prev.d * Dr);
-  if (mat < 0 || nt < 0) return 0.0;
-  gemm(T, Dl, Dr, dd, colmajor(dptr(C, last.off), Dl), colmajor(dptr(C, hj.off), dd),
-       colmajor(dptr(C, mat), Dl));
-  gemm(T, (long long)prev.dl * prev.d, Dr, prev.dr, colmajor(dptr(C, prev.off), (long long)prev.dl * prev.d),
-       colmajor(dptr(C, mat), Dl), colmajor(dptr(C, nt), (long long)prev.dl * prev.d));
-  afree(C, mat, 8 * Dl * Dr);
-  afree(C, last.off, sbytes(last));
-  afree(C, prev.off, sbytes(prev));
-  afree(C, hj.off, sbytes(hj));
+  double* mat = spush(C, Dl * Dr);
+  if (failed(C)) return 0.0;
+  gemm(T, Dl, Dr, dd, colmajor(sdata(C, last), Dl), colmajor(sdata(C, hj), dd), colmajor(mat, Dl));
+  SiteRef prev = sref(C, ki, hi.nsites - 1);
+  const long long pr = (long long)prev.dl * prev.d;
+  if (!heap_reserve(C, al256(8 * pr * Dr))) return 0.0;
+  prev = sref(C, ki, hi.nsites - 1);
+  const long long nt = heap_take(C, 8 * pr * Dr);
+  gemm(T, pr, Dr, prev.dr, colmajor(sdata(C, prev), pr), colmajor(mat, Dl), colmajor(dptr(C, nt), pr));
+  account(C, 2.0 * Dl * dd * Dr + 2.0 * pr * prev.dr * Dr,
+          8.0 * ((double)Dl * dd + (double)dd * Dr + (double)pr * prev.dr + (double)pr * Dr));
   T.sync();
   if (T.leader()) {
     const int nsi = hi.nsites - 1;
     sref(C, ki, nsi) = mksite(prev.dl, prev.d, (int)Dr, nt);
     const int nsj = C.node[kj].nsites;
     if (nsi + nsj - 1 > C.maxs || C.node[ki].nnbr - 1 + C.node[kj].nnbr > C.maxs) {
-      set_status_leader(C, CATN_ENOMEM);
+      fail_leader(C, CATN_ENOMEM);
     } else {
       for (int p = 2; p <= nsj; ++p) sref(C, ki, nsi + p - 1) = sref(C, kj, p);
       C.node[ki].nsites = nsi + nsj - 1;
       C.node[ki].cano = nsi;
-      C.node[kj].nsites = 0;   // ownership of j's sites 2:end moved to i
+      C.node[kj].nsites = 0;   // j's sites 2:end now belong to i
       int nni = C.node[ki].nnbr - 1;
       const int nnj = C.node[kj].nnbr;
       for (int p = 2; p <= nnj; ++p) nbref(C, ki, nni + p - 1) = nbref(C, kj, p);
       C.node[ki].nnbr = nni + (nnj > 1 ? nnj - 1 : 0);
     }
   }
-  T.sync();
+  refresh_status(C);
+  C.sp = mark;
   if (failed(C)) return 0.0;
   cano_to(C, ki, C.node[ki].nsites);
   if (failed(C)) return 0.0;
   SiteRef ctr = sref(C, ki, C.node[ki].cano);
-  double nrm = norm_of(C, dptr(C, ctr.off), (long long)ctr.dl * ctr.d * ctr.dr);
+  const long long ce = (long long)ctr.dl * ctr.d * ctr.dr;
+  const double nrm = norm_of(C, sdata(C, ctr), ce);
   if (nrm <= cutoff) return 0.0;
-  scale(T, dptr(C, ctr.off), 1.0 / nrm, (long long)ctr.dl * ctr.d * ctr.dr);
+  scale(T, sdata(C, ctr), 1.0 / nrm, ce);
   return log(nrm);
 }
 
 // ---------------------------------------------------------------------------
-// QR pre-reduction helper: matrix X (rows x cols) in buffer `buf` (consumed
-// into Householder form when rows > cols).  Produces R (cols x cols or the
-// original rows x cols) in a new buffer.
+// QR pre-reduction (compress_opt!, cut_bondim_opt!): X (rows x cols) in a
+// scratch buffer, consumed into Householder form when rows > cols.
 // ---------------------------------------------------------------------------
 struct QRed {
   bool flag;
-  long long house, house_bytes, tau;   // Householder storage (rows x cols) and tau (cols)
-  long long Rb;                         // R (or the matrix itself), column-major
+  double* house;   // rows x cols (Householder form when flag)
+  double* tau;
+  double* Rb;      // R (cols x cols) or the matrix itself (rows x cols)
   long long rrows, cols, rows;
 };
 
-CATN_HDI inline QRed qr_reduce(Ctx& C, long long buf, long long buf_bytes, long long rows, long long cols) {
+CATN_HDI inline QRed qr_reduce(Ctx& C, double* X, long long rows, long long cols) {
   const Team& T = C.T;
   QRed q;
   q.rows = rows;
   q.cols = cols;
-  q.house = buf;
-  q.house_bytes = buf_bytes;
-  q.tau = -1;
+  q.house = X;
+  q.tau = nullptr;
   q.flag = rows > cols;
-  if (!q.flag) {
-    q.Rb = buf;
-    q.rrows = rows;
-    return q;
-  }
-  q.tau = aalloc(C, 8 * cols);
-  q.Rb = aalloc(C, 8 * cols * cols);
+  q.Rb = X;
+  q.rrows = rows;
+  if (!q.flag) return q;
+  q.tau = spush(C, cols);
+  q.Rb = spush(C, cols * cols);
   q.rrows = cols;
-  if (q.tau < 0 || q.Rb < 0) return q;
-  qr_inplace(T, dptr(C, buf), rows, cols, rows, dptr(C, q.tau));
-  const double* W = dptr(C, buf);
-  double* Rp = dptr(C, q.Rb);
+  if (failed(C)) return q;
+  qr_inplace(T, X, rows, cols, rows, q.tau);
   for (long long e = T.rank(); e < cols * cols; e += T.size()) {
     long long r = e % cols, c = e / cols;
-    Rp[e] = (r <= c) ? W[r + c * rows] : 0.0;
+    q.Rb[e] = (r <= c) ? X[r + c * rows] : 0.0;
   }
   T.sync();
   return q;
 }
-// Y (rrows x ncols) -> Q [Y; 0] (rows x ncols) in a new buffer (or a copy when !flag).
-CATN_HDI inline long long qr_expand(Ctx& C, const QRed& q, const double* Y, long long ncols) {
+// Y (rrows x ncols) -> Q [Y; 0] (rows x ncols) into `out`.
+CATN_HDI inline void qr_expand(Ctx& C, const QRed& q, const double* Y, long long ncols, double* out) {
   const Team& T = C.T;
-  long long out = aalloc(C, 8 * q.rows * ncols);
-  if (out < 0) return out;
-  double* O = dptr(C, out);
   for (long long e = T.rank(); e < q.rows * ncols; e += T.size()) {
     long long r = e % q.rows, c = e / q.rows;
-    O[e] = (r < q.rrows) ? Y[r + c * q.rrows] : 0.0;
+    out[e] = (r < q.rrows) ? Y[r + c * q.rrows] : 0.0;
   }
   T.sync();
-  if (q.flag) qr_apply_q(T, dptr(C, q.house), q.rows, q.cols, q.rows, dptr(C, q.tau), O, ncols, q.rows);
-  return out;
-}
-CATN_HDI inline void qr_release(Ctx& C, const QRed& q) {
-  if (q.flag) {
-    afree(C, q.tau, 8 * q.cols);
-    afree(C, q.Rb, 8 * q.cols * q.cols);
-  }
-  afree(C, q.house, q.house_bytes);
+  if (q.flag) qr_apply_q(T, q.house, q.rows, q.cols, q.rows, q.tau, out, ncols, q.rows);
 }
 
 // ---------------------------------------------------------------------------
@@ -756,69 +809,65 @@ CATN_HDI inline double compress_node(Ctx& C, int k, bool opt) {
   const int ns = C.node[k].nsites;
   for (int jj = ns; jj >= 2 && !failed(C); --jj) {
     const int i = jj - 1;
+    const long long mark = C.sp;
     SiteRef tl = sref(C, k, i), tr = sref(C, k, jj);
     const long long d0 = tl.dl, d1 = tl.d, dd = tl.dr, d2 = tr.d, d3 = tr.dr;
     const long long ml = d0 * d1, nr = d2 * d3;
-    long long Uo, Vo;
+    double* Uo = nullptr;   // ml x myd  (U * S, through Ql)
+    double* Vo = nullptr;   // nr x myd  (V, through Qr)
     int myd;
     double e;
+    Svd R;
     if (!opt) {
-      long long mat = aalloc(C, 8 * ml * nr);
-      if (mat < 0) return err;
-      gemm(T, ml, nr, dd, colmajor(dptr(C, tl.off), ml), colmajor(dptr(C, tr.off), dd),
-           colmajor(dptr(C, mat), ml));
-      afree(C, tl.off, sbytes(tl));
-      afree(C, tr.off, sbytes(tr));
-      Svd R = svd_full(C, mat, 8 * ml * nr, ml, nr);
-      if (R.p == 0) return err;
+      SvdIn in = svd_begin(C, ml, nr);
+      if (failed(C)) return err;
+      gemm(T, ml, nr, dd, colmajor(sdata(C, tl), ml), colmajor(sdata(C, tr), dd), svd_target(in));
+      R = svd_finish(C, in);
+      if (failed(C)) return err;
       myd = keep_rule(C, R, C.P.cutoff, C.P.chi, &e);
-      Uo = aalloc(C, 8 * ml * myd);
-      Vo = aalloc(C, 8 * nr * myd);
-      if (Uo < 0 || Vo < 0) return err;
-      materialize(T, dptr(C, Uo), ml, myd, ml, mop(dptr(C, R.U), rows_plain(), cols_plain(ml), nullptr, dptr(C, R.S)));
-      materialize(T, dptr(C, Vo), myd, nr, myd, mop(dptr(C, R.V), imap(1, 0, nr), rows_plain()));
-      svd_free(C, R);
     } else {
-      // matl = (d0 d1) x dd, QR when tall; matr^H = (d2 d3) x dd, QR when matr is wide
-      QRed ql = qr_reduce(C, tl.off, sbytes(tl), ml, dd);
-      long long trt = aalloc(C, 8 * nr * dd);
-      if (trt < 0) return err;
-      materialize(T, dptr(C, trt), nr, dd, nr, transposed(dptr(C, tr.off), dd));
-      afree(C, tr.off, sbytes(tr));
-      QRed qr = qr_reduce(C, trt, 8 * nr * dd, nr, dd);
+      double* matl = spush(C, ml * dd);
+      double* matrt = spush(C, nr * dd);
+      if (failed(C)) return err;
+      copy(T, matl, sdata(C, tl), ml * dd);
+      materialize(T, matrt, nr, dd, nr, transposed(sdata(C, tr), dd));
+      QRed ql = qr_reduce(C, matl, ml, dd);
+      QRed qr = qr_reduce(C, matrt, nr, dd);
       if (failed(C)) return err;
       // mat = Rl * Rr^H  (ql.rrows x qr.rrows)
-      long long mat = aalloc(C, 8 * ql.rrows * qr.rrows);
-      if (mat < 0) return err;
-      gemm(T, ql.rrows, qr.rrows, dd, colmajor(dptr(C, ql.Rb), ql.rrows), transposed(dptr(C, qr.Rb), qr.rrows),
-           colmajor(dptr(C, mat), ql.rrows));
-      Svd R = svd_full(C, mat, 8 * ql.rrows * qr.rrows, ql.rrows, qr.rrows);
-      if (R.p == 0) return err;
+      SvdIn in = svd_begin(C, ql.rrows, qr.rrows);
+      if (failed(C)) return err;
+      gemm(T, ql.rrows, qr.rrows, dd, colmajor(ql.Rb, ql.rrows), transposed(qr.Rb, qr.rrows), svd_target(in));
+      R = svd_finish(C, in);
+      if (failed(C)) return err;
       myd = keep_rule(C, R, C.P.cutoff, C.P.chi, &e);
-      // U * S then Ql;  V then Qr
-      long long us = aalloc(C, 8 * ql.rrows * myd);
-      if (us < 0) return err;
-      materialize(T, dptr(C, us), ql.rrows, myd, ql.rrows,
-                  mop(dptr(C, R.U), rows_plain(), cols_plain(ql.rrows), nullptr, dptr(C, R.S)));
-      long long Ufull = qr_expand(C, ql, dptr(C, us), myd);
-      long long Vfull = qr_expand(C, qr, dptr(C, R.V), myd);   // first myd columns of V
-      afree(C, us, 8 * ql.rrows * myd);
-      svd_free(C, R);
-      qr_release(C, ql);
-      qr_release(C, qr);
-      if (Ufull < 0 || Vfull < 0) return err;
-      Uo = Ufull;
-      Vo = aalloc(C, 8 * nr * myd);
-      if (Vo < 0) return err;
-      materialize(T, dptr(C, Vo), myd, nr, myd, transposed(dptr(C, Vfull), nr));
-      afree(C, Vfull, 8 * nr * myd);
+      double* us = spush(C, ql.rrows * myd);
+      Uo = spush(C, ml * myd);
+      Vo = spush(C, nr * myd);
+      if (failed(C)) return err;
+      materialize(T, us, ql.rrows, myd, ql.rrows, mop(R.U, rows_plain(), cols_plain(ql.rrows), nullptr, R.S));
+      qr_expand(C, ql, us, myd, Uo);
+      qr_expand(C, qr, R.V, myd, Vo);
     }
     err += e;
+    if (!heap_reserve(C, al256(8 * ml * myd) + al256(8 * nr * myd))) return err;
+    const long long ou = heap_take(C, 8 * ml * myd);
+    const long long ov = heap_take(C, 8 * nr * myd);
+    if (!opt) {
+      materialize(T, dptr(C, ou), ml, myd, ml, mop(R.U, rows_plain(), cols_plain(ml), nullptr, R.S));
+      materialize(T, dptr(C, ov), myd, nr, myd, mop(R.V, imap(1, 0, nr), rows_plain()));
+    } else {
+      copy(T, dptr(C, ou), Uo, ml * myd);
+      materialize(T, dptr(C, ov), myd, nr, myd, transposed(Vo, nr));
+    }
+    account(C, 2.0 * ml * nr * dd + 4.0 * ml * nr * myd,
+            8.0 * ((double)ml * dd + (double)dd * nr + (double)ml * myd + (double)myd * nr));
     if (T.leader()) {
-      sref(C, k, i) = mksite((int)d0, (int)d1, myd, Uo);
-      sref(C, k, jj) = mksite(myd, (int)d2, (int)d3, Vo);
+      sref(C, k, i) = mksite((int)d0, (int)d1, myd, ou);
+      sref(C, k, jj) = mksite(myd, (int)d2, (int)d3, ov);
     }
     T.sync();
+    C.sp = mark;
   }
   T.sync();
   if (T.leader()) C.node[k].cano = 1;
@@ -833,97 +882,80 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   const Team& T = C.T;
   if (C.P.Dmax < 0) return 0.0;
   int j = nbref(C, i, idx_j_in_i);
-  if (j <= 0) { set_status(C, CATN_ESTATE); return 0.0; }
+  if (j <= 0) { fail_all(C, CATN_ESTATE); return 0.0; }
   int idx_i_in_j = nb_find(C, j, i);
-  if (idx_i_in_j == 0) { set_status(C, CATN_ESTATE); return 0.0; }
+  if (idx_i_in_j == 0) { fail_all(C, CATN_ESTATE); return 0.0; }
   cano_to(C, i, idx_j_in_i);
   cano_to(C, j, idx_i_in_j);
   if (failed(C)) return 0.0;
+  const long long mark = C.sp;
   SiteRef Ai = sref(C, i, idx_j_in_i), Aj = sref(C, j, idx_i_in_j);
   const long long d = Ai.d;
   const long long ri_rows = (long long)Ai.dl * Ai.dr, rj_rows = (long long)Aj.dl * Aj.dr;
   // mati = reshape(permutedims(Ai, (1,3,2)), da_l*da_r, d)
-  long long mi = aalloc(C, 8 * ri_rows * d);
-  long long mj = aalloc(C, 8 * rj_rows * d);
-  if (mi < 0 || mj < 0) return 0.0;
-  materialize(T, dptr(C, mi), ri_rows, d, ri_rows,
-              mop(dptr(C, Ai.off), imap(Ai.dl, 1, (long long)Ai.dl * d), cols_plain(Ai.dl)));
-  materialize(T, dptr(C, mj), rj_rows, d, rj_rows,
-              mop(dptr(C, Aj.off), imap(Aj.dl, 1, (long long)Aj.dl * d), cols_plain(Aj.dl)));
-  afree(C, Ai.off, sbytes(Ai));
-  afree(C, Aj.off, sbytes(Aj));
-  QRed qi = qr_reduce(C, mi, 8 * ri_rows * d, ri_rows, d);
-  QRed qj = qr_reduce(C, mj, 8 * rj_rows * d, rj_rows, d);
+  double* mi = spush(C, ri_rows * d);
+  double* mj = spush(C, rj_rows * d);
   if (failed(C)) return 0.0;
-  long long mg = aalloc(C, 8 * qi.rrows * qj.rrows);
-  if (mg < 0) return 0.0;
-  gemm(T, qi.rrows, qj.rrows, d, colmajor(dptr(C, qi.Rb), qi.rrows), transposed(dptr(C, qj.Rb), qj.rrows),
-       colmajor(dptr(C, mg), qi.rrows));
-  Svd R = svd_full(C, mg, 8 * qi.rrows * qj.rrows, qi.rrows, qj.rrows);
-  if (R.p == 0) return 0.0;
+  materialize(T, mi, ri_rows, d, ri_rows, mop(sdata(C, Ai), imap(Ai.dl, 1, (long long)Ai.dl * d), cols_plain(Ai.dl)));
+  materialize(T, mj, rj_rows, d, rj_rows, mop(sdata(C, Aj), imap(Aj.dl, 1, (long long)Aj.dl * d), cols_plain(Aj.dl)));
+  QRed qi = qr_reduce(C, mi, ri_rows, d);
+  QRed qj = qr_reduce(C, mj, rj_rows, d);
+  if (failed(C)) return 0.0;
+  SvdIn in = svd_begin(C, qi.rrows, qj.rrows);
+  if (failed(C)) return 0.0;
+  gemm(T, qi.rrows, qj.rrows, d, colmajor(qi.Rb, qi.rrows), transposed(qj.Rb, qj.rrows), svd_target(in));
+  Svd R = svd_finish(C, in);
+  if (failed(C)) return 0.0;
   double disc = 0.0;
-  int kept = keep_rule(C, R, C.P.cutoff, 0x7fffffffLL, &disc);
+  const int kept = keep_rule(C, R, C.P.cutoff, 0x7fffffffLL, &disc);
   int myd = kept < C.P.Dmax ? kept : C.P.Dmax;
   if (myd < 1) myd = 1;
   double extra = 0.0;
   {
-    const double* S = dptr(C, R.S);
     double loc = 0.0;
-    for (long long e = myd + T.rank(); e < kept; e += T.size()) loc += S[e];
+    for (long long e = myd + T.rank(); e < kept; e += T.size()) loc += R.S[e];
     extra = T.sum(loc);
   }
-  // sqrt(S) scaled factors
-  long long sq = aalloc(C, 8LL * myd);
-  long long ui = aalloc(C, 8 * qi.rrows * myd);
-  long long vj = aalloc(C, 8 * qj.rrows * myd);
-  if (sq < 0 || ui < 0 || vj < 0) return 0.0;
+  double* sq = spush(C, myd);
+  double* ui = spush(C, qi.rrows * myd);
+  double* vj = spush(C, qj.rrows * myd);
+  double* fi = spush(C, ri_rows * myd);
+  double* fj = spush(C, rj_rows * myd);
+  if (failed(C)) return 0.0;
+  for (long long e = T.rank(); e < myd; e += T.size()) sq[e] = sqrt(R.S[e]);
+  T.sync();
+  materialize(T, ui, qi.rrows, myd, qi.rrows, mop(R.U, rows_plain(), cols_plain(qi.rrows), nullptr, sq));
+  materialize(T, vj, qj.rrows, myd, qj.rrows, mop(R.V, rows_plain(), cols_plain(qj.rrows), nullptr, sq));
+  qr_expand(C, qi, ui, myd, fi);   // (da_l*da_r) x myd
+  qr_expand(C, qj, vj, myd, fj);
+  if (!heap_reserve(C, al256(8LL * Ai.dl * myd * Ai.dr) + al256(8LL * Aj.dl * myd * Aj.dr))) return 0.0;
+  const long long ni = heap_take(C, 8LL * Ai.dl * myd * Ai.dr);
+  const long long nj = heap_take(C, 8LL * Aj.dl * myd * Aj.dr);
   {
-    const double* S = dptr(C, R.S);
-    double* q = dptr(C, sq);
-    for (long long e = T.rank(); e < myd; e += T.size()) q[e] = sqrt(S[e]);
-    T.sync();
-  }
-  materialize(T, dptr(C, ui), qi.rrows, myd, qi.rrows,
-              mop(dptr(C, R.U), rows_plain(), cols_plain(qi.rrows), nullptr, dptr(C, sq)));
-  materialize(T, dptr(C, vj), qj.rrows, myd, qj.rrows,
-              mop(dptr(C, R.V), rows_plain(), cols_plain(qj.rrows), nullptr, dptr(C, sq)));
-  svd_free(C, R);
-  afree(C, sq, 8LL * myd);
-  long long fi = qr_expand(C, qi, dptr(C, ui), myd);   // (da_l*da_r) x myd
-  long long fj = qr_expand(C, qj, dptr(C, vj), myd);
-  afree(C, ui, 8 * qi.rrows * myd);
-  afree(C, vj, 8 * qj.rrows * myd);
-  qr_release(C, qi);
-  qr_release(C, qj);
-  if (fi < 0 || fj < 0) return 0.0;
-  // new site = permutedims(reshape(mat, dl, dr, myd), (1,3,2))
-  long long ni = aalloc(C, 8LL * Ai.dl * myd * Ai.dr);
-  long long nj = aalloc(C, 8LL * Aj.dl * myd * Aj.dr);
-  if (ni < 0 || nj < 0) return 0.0;
-  {
-    const double* F = dptr(C, fi);
+    // new site = permutedims(reshape(mat, dl, dr, myd), (1,3,2))
     double* O = dptr(C, ni);
     const long long dl = Ai.dl, dr = Ai.dr, tot = dl * myd * dr;
     for (long long e = T.rank(); e < tot; e += T.size()) {
       long long a = e % dl, rest = e / dl, r = rest % myd, c = rest / myd;
-      O[e] = F[(a + dl * c) + ri_rows * r];
+      O[e] = fi[(a + dl * c) + ri_rows * r];
     }
-    const double* G = dptr(C, fj);
     double* P2 = dptr(C, nj);
     const long long dl2 = Aj.dl, dr2 = Aj.dr, tot2 = dl2 * myd * dr2;
     for (long long e = T.rank(); e < tot2; e += T.size()) {
       long long a = e % dl2, rest = e / dl2, r = rest % myd, c = rest / myd;
-      P2[e] = G[(a + dl2 * c) + rj_rows * r];
+      P2[e] = fj[(a + dl2 * c) + rj_rows * r];
     }
     T.sync();
   }
-  afree(C, fi, 8 * ri_rows * myd);
-  afree(C, fj, 8 * rj_rows * myd);
+  account(C, 4.0 * (double)ri_rows * d * d + 4.0 * (double)rj_rows * d * d + 2.0 * qi.rrows * qj.rrows * d +
+                 4.0 * qi.rrows * qj.rrows * myd,
+          8.0 * ((double)ri_rows * d + (double)rj_rows * d + (double)ri_rows * myd + (double)rj_rows * myd));
   if (T.leader()) {
     sref(C, i, idx_j_in_i) = mksite(Ai.dl, myd, Ai.dr, ni);
     sref(C, j, idx_i_in_j) = mksite(Aj.dl, myd, Aj.dr, nj);
   }
   T.sync();
+  C.sp = mark;
   return disc + extra;
 }
 
@@ -933,39 +965,47 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
 CATN_HDI inline void raw2mps(Ctx& C, int k, const double* data, const long long* dims, int nd) {
   const Team& T = C.T;
   if (nd == 0) return;   // the reference returns an empty MPS for a 0-d tensor
+  if (nd > C.maxs) { fail_all(C, CATN_ENOMEM); return; }
+  const long long mark = C.sp;
   long long total = 1;
   for (int q = 0; q < nd; ++q) total *= dims[q];
-  if (nd > C.maxs) { set_status(C, CATN_ENOMEM); return; }
-  long long R = aalloc(C, 8 * total);
-  if (R < 0) return;
-  copy(T, dptr(C, R), data, total);
-  long long Rbytes = 8 * total, cur = total;
-  long long dleft = 1;
+  double* R = spush(C, total);
+  if (failed(C)) return;
+  copy(T, R, data, total);
+  long long cur = total, dleft = 1;
   for (int q = 0; q < nd - 1; ++q) {
-    long long m = dleft * dims[q], n = cur / m;
-    Svd S = svd_full(C, R, Rbytes, m, n);
-    if (S.p == 0) return;
+    const long long m = dleft * dims[q], n = cur / m;
+    SvdIn in = svd_begin(C, m, n);
+    if (failed(C)) return;
+    svd_fill(C, in, colmajor(R, m));
+    Svd S = svd_finish(C, in);
+    if (failed(C)) return;
     double disc;
-    int c = keep_rule(C, S, C.P.cutoff, C.P.chi, &disc);
-    long long u = aalloc(C, 8 * m * c);
-    long long r2 = aalloc(C, 8LL * c * n);
-    if (u < 0 || r2 < 0) return;
-    copy(T, dptr(C, u), dptr(C, S.U), m * c);
-    materialize(T, dptr(C, r2), c, n, c, mop(dptr(C, S.V), imap(1, 0, n), rows_plain(), dptr(C, S.S), nullptr));
-    svd_free(C, S);
+    const int c = keep_rule(C, S, C.P.cutoff, C.P.chi, &disc);
+    double* r2 = spush(C, (long long)c * n);
+    if (failed(C) || !heap_reserve(C, al256(8 * m * c))) return;
+    const long long u = heap_take(C, 8 * m * c);
+    copy(T, dptr(C, u), S.U, m * c);
+    materialize(T, r2, c, n, c, mop(S.V, imap(1, 0, n), rows_plain(), S.S, nullptr));
     if (T.leader()) sref(C, k, q + 1) = mksite((int)dleft, (int)dims[q], c, u);
     T.sync();
+    // sites 1..q+1 are live from here on (compaction may move them)
+    if (T.leader()) C.node[k].nsites = q + 1;
+    T.sync();
     R = r2;
-    Rbytes = 8LL * c * n;
     cur = (long long)c * n;
     dleft = c;
   }
+  if (!heap_reserve(C, al256(8 * cur))) return;
+  const long long last = heap_take(C, 8 * cur);
+  copy(T, dptr(C, last), R, cur);
   if (T.leader()) {
-    sref(C, k, nd) = mksite((int)dleft, (int)dims[nd - 1], 1, R);
+    sref(C, k, nd) = mksite((int)dleft, (int)dims[nd - 1], 1, last);
     C.node[k].nsites = nd;
     C.node[k].cano = nd;
   }
   T.sync();
+  C.sp = mark;
 }
 
 // ---------------------------------------------------------------------------
@@ -979,9 +1019,9 @@ CATN_HD int dim_after_merge(const Ctx& C, int i, int j) {
 CATN_HD int& emap_at(const Ctx& C, int i, int j) { return C.emap[(long long)i * (C.n + 1) + j]; }
 
 CATN_HD void bucket_add_leader(Ctx& C, int cost, int i, int j) {
-  if (cost < 0 || cost >= CATN_CMAX) { set_status_leader(C, CATN_ENOMEM); return; }
+  if (cost < 0 || cost >= CATN_CMAX) { fail_leader(C, CATN_ENOMEM); return; }
   int e = C.ctl[CTL_FREEENT];
-  if (e < 0) { set_status_leader(C, CATN_ENOMEM); return; }
+  if (e < 0) { fail_leader(C, CATN_ENOMEM); return; }
   C.ctl[CTL_FREEENT] = C.ent[e].next;
   EdgeEnt& E = C.ent[e];
   E.cost = cost; E.i = i; E.j = j; E.alive = 1; E.next = -1; E.prev = C.btail[cost];
@@ -1062,7 +1102,7 @@ CATN_HD void count_add_nodes_leader(Ctx& C, const int* list, int nl) {
     for (int p = 1; p <= nn; ++p) {
       int j = nbref(C, i, p);
       if (j <= 0) continue;
-      if (np >= C.pcap) { set_status_leader(C, CATN_ENOMEM); return; }
+      if (np >= C.pcap) { fail_leader(C, CATN_ENOMEM); return; }
       pr[2 * np] = i < j ? i : j;
       pr[2 * np + 1] = i < j ? j : i;
       ++np;
@@ -1102,7 +1142,7 @@ CATN_HD long long select_leader(Ctx& C, int* maxdim) {
   int sel = C.P.select;
   if (sel == 0 || sel == 1) {
     int cost = min_cost_leader(C);
-    if (cost >= CATN_CMAX) { set_status_leader(C, CATN_ESTATE); return 0; }
+    if (cost >= CATN_CMAX) { fail_leader(C, CATN_ESTATE); return 0; }
     if (cost > *maxdim) *maxdim = cost;
     int e = C.bhead[cost];
     int bi = C.ent[e].i, bj = C.ent[e].j;
@@ -1137,7 +1177,7 @@ CATN_HD long long select_leader(Ctx& C, int* maxdim) {
       if (i + nb < bs) { bs = i + nb; best = ((long long)i << 32) | (unsigned)nb; }
     }
   }
-  if (best < 0) set_status_leader(C, CATN_ESTATE);
+  if (best < 0) fail_leader(C, CATN_ESTATE);
   return best < 0 ? 0 : best;
 }
 
@@ -1174,7 +1214,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
       for (int k = 1; k <= C.n; ++k) C.list[k - 1] = k;
       count_add_nodes_leader(C, C.list, C.n);
     }
-    T.sync();
+    refresh_status(C);
   }
   int maxdim = -1;
   // Every step clears one node, so a network of n nodes needs fewer than n
@@ -1182,7 +1222,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
   const int step_cap = C.n + 16;
   while (!failed(C) && has_real_edges(C)) {
     if (O.nsteps > step_cap) {
-      set_status(C, CATN_ESTATE);
+      fail_all(C, CATN_ESTATE);
       break;
     }
     // --- select ---
@@ -1192,6 +1232,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
     if (T.leader()) pk = select_leader(C, &md);
     pk = T.bcast(pk);
     maxdim = (int)T.bcast(md);
+    refresh_status(C);
     if (failed(C)) break;
     int i = (int)(pk >> 32), j = (int)(pk & 0xffffffff);
     if (C.node[j].nsites > C.node[i].nsites) { int t = i; i = j; j = t; }
@@ -1207,7 +1248,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
         for (int p = 1; p <= C.node[j].nnbr; ++p) list[nl++] = nbref(C, j, p);
         count_remove_nodes_leader(C, list, nl);
       }
-      T.sync();
+      refresh_status(C);
     }
     int idx_j_in_i = nb_find(C, i, j);
     int idx_i_in_j = nb_find(C, j, i);
@@ -1243,13 +1284,14 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
       int idx_k_in_i = nb_find(C, i, k);
       int idx_i_in_k = nb_find(C, k, i);
       int idx_j_in_k = nb_find(C, k, j);
-      if (idx_j_in_k == 0) { set_status(C, CATN_ESTATE); break; }
+      if (idx_j_in_k == 0) { fail_all(C, CATN_ESTATE); break; }
       T.sync();
       if (T.leader()) {
         nb_delete_at_leader(C, k, idx_j_in_k);
         nb_insert_at_leader(C, k, idx_j_in_k, i);
       }
-      T.sync();
+      refresh_status(C);
+      if (failed(C)) break;
       if (idx_k_in_i > 0) {
         T.sync();
         if (T.leader()) dup[nd] = k;
@@ -1287,7 +1329,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
         for (int p = 1; p <= C.node[i].nnbr; ++p) list[nl++] = nbref(C, i, p);
         count_add_nodes_leader(C, list, nl);
       }
-      T.sync();
+      refresh_status(C);
     }
     const int nsi = C.node[i].nsites;
     unsigned shh = 2166136261u;
@@ -1327,7 +1369,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
   nneg = T.sum(nneg);
   nzero = T.sum(nzero);
   bad = T.sum(bad);
-  if (bad > 0.5) set_status(C, CATN_ESTATE);
+  if (bad > 0.5) fail_all(C, CATN_ESTATE);
   O.lnZ += lsum;
   O.sign = nzero > 0.5 ? 0.0 : (((long long)(nneg + 0.5)) % 2 ? -1.0 : 1.0);
   O.maxdim = maxdim;
@@ -1337,7 +1379,9 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
 // ---------------------------------------------------------------------------
 // Slot initialisation and instance loading
 // ---------------------------------------------------------------------------
-CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, const catn_params& P, int n) {
+// `sws`/`sws_doubles`: shared-memory SVD workspace of the team.
+CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, const catn_params& P, int n,
+                             double* sws, long long sws_doubles) {
   Ctx C;
   C.T = T;
   C.P = P;
@@ -1357,9 +1401,26 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.pcap = L.pcap;
   C.list = (int*)(slot + L.off_list);
   C.tmp = (int*)(slot + L.off_tmp);
-  C.ameta = (long long*)(slot + L.off_ameta);
+  C.acct = (double*)(slot + L.off_ameta);
   C.base = slot + L.off_arena;
-  C.cap = L.arena_bytes;
+  // arena: scratch stack (40%), two heap halves (30% each)
+  const long long cap = L.arena_bytes & ~255LL;
+  const long long sc = (cap * 2 / 5) & ~255LL;
+  C.hsize = ((cap - sc) / 2) & ~255LL;
+  C.sp_lo = 0;
+  C.sp = 0;
+  C.sp_hi = sc;
+  C.sp_peak = 0;
+  C.h_lo0 = sc;
+  C.h_lo1 = sc + C.hsize;
+  C.half = 0;
+  C.hb = C.h_lo0;
+  C.he = C.h_lo0 + C.hsize;
+  C.h_peak = 0;
+  C.compactions = 0;
+  C.sws = sws;
+  C.sws_doubles = sws_doubles;
+  C.status = 0;
   C.trace = nullptr;
   C.trace_cap = 0;
   return C;
@@ -1375,12 +1436,13 @@ CATN_HDI inline void reset_slot(Ctx& C) {
     C.ent[e].next = (e + 1 < C.ecap) ? (int)(e + 1) : -1;
   }
   for (long long e = T.rank(); e < nn; e += T.size()) { C.node[e].nsites = 0; C.node[e].nnbr = 0; C.node[e].cano = 0; C.node[e].pad = 0; }
-  for (long long e = T.rank(); e < CATN_NCLS + 2; e += T.size()) C.ameta[e] = (e >= 1 && e <= CATN_NCLS) ? -1 : 0;
   for (long long e = T.rank(); e < CTL_WORDS; e += T.size()) C.ctl[e] = 0;
   T.sync();
   if (T.leader()) {
     C.ctl[CTL_FREEENT] = C.ecap > 0 ? 0 : -1;
     C.ctl[CTL_MINC] = 0;
+    C.acct[0] = 0.0;
+    C.acct[1] = 0.0;
   }
   T.sync();
 }
@@ -1394,43 +1456,51 @@ CATN_HDI inline void load_instance(Ctx& C, const InstDesc& D, const long long* i
   const int* nbrs = img32 + D.nbr_off;
   const double* data = imgd + D.data_off;
   if (D.kind == 0) {
-    // MPS form: leader allocates every site, then the team copies
-    T.sync();
+    // MPS form: sites laid out contiguously in the heap (every thread
+    // computes the same offsets), leader writes the refs, team copies data.
+    long long total = 0, nsites = 0;
+    for (int k = 1; k <= C.n; ++k) {
+      const int ns = (int)hdr[4 * (k - 1)], nn = (int)hdr[4 * (k - 1) + 1];
+      if (ns > C.maxs || nn > C.maxs) { fail_all(C, CATN_ENOMEM); return; }
+      for (int p = 0; p < ns; ++p, ++nsites)
+        total += al256(8 * dims[3 * nsites] * dims[3 * nsites + 1] * dims[3 * nsites + 2]);
+    }
+    if (!heap_reserve(C, total)) return;
+    const long long first = C.hb;
+    C.hb += total;
+    if (C.hb - C.h_lo0 > C.h_peak) C.h_peak = C.hb - C.h_lo0;
     if (T.leader()) {
-      long long sidx = 0, nidx = 0;
+      long long sidx = 0, nidx = 0, cur = first;
       for (int k = 1; k <= C.n; ++k) {
-        int ns = (int)hdr[4 * (k - 1)], nn = (int)hdr[4 * (k - 1) + 1], cano = (int)hdr[4 * (k - 1) + 2];
-        if (ns > C.maxs || nn > C.maxs) { set_status_leader(C, CATN_ENOMEM); break; }
+        const int ns = (int)hdr[4 * (k - 1)], nn = (int)hdr[4 * (k - 1) + 1], cano = (int)hdr[4 * (k - 1) + 2];
         C.node[k].nsites = ns;
         C.node[k].nnbr = nn;
         C.node[k].cano = cano;
         for (int p = 1; p <= ns; ++p, ++sidx) {
-          int dl = (int)dims[3 * sidx], d = (int)dims[3 * sidx + 1], dr = (int)dims[3 * sidx + 2];
-          long long off = aalloc_leader(C, 8LL * dl * d * dr);
-          sref(C, k, p) = mksite(dl, d, dr, off);
+          const int dl = (int)dims[3 * sidx], d = (int)dims[3 * sidx + 1], dr = (int)dims[3 * sidx + 2];
+          sref(C, k, p) = mksite(dl, d, dr, cur);
+          cur += al256(8LL * dl * d * dr);
         }
         for (int p = 1; p <= nn; ++p, ++nidx) nbref(C, k, p) = nbrs[nidx];
       }
     }
-    T.sync();
-    if (failed(C)) return;
-    long long doff = 0;
+    long long sidx = 0, doff = 0, cur = first;
     for (int k = 1; k <= C.n; ++k) {
-      int ns = C.node[k].nsites;
-      for (int p = 1; p <= ns; ++p) {
-        SiteRef s = sref(C, k, p);
-        long long sz = (long long)s.dl * s.d * s.dr;
-        double* dst = dptr(C, s.off);
+      const int ns = (int)hdr[4 * (k - 1)];
+      for (int p = 1; p <= ns; ++p, ++sidx) {
+        const long long sz = dims[3 * sidx] * dims[3 * sidx + 1] * dims[3 * sidx + 2];
+        double* dst = dptr(C, cur);
         for (long long e = T.rank(); e < sz; e += T.size()) dst[e] = data[doff + e];
         doff += sz;
+        cur += al256(8 * sz);
       }
     }
     T.sync();
   } else {
     long long dpos = 0, doff = 0, nidx = 0;
     for (int k = 1; k <= C.n && !failed(C); ++k) {
-      int nd = (int)hdr[4 * (k - 1)];
-      if (nd > C.maxs) { set_status(C, CATN_ENOMEM); break; }
+      const int nd = (int)hdr[4 * (k - 1)];
+      if (nd > C.maxs) { fail_all(C, CATN_ENOMEM); break; }
       T.sync();
       if (T.leader()) {
         C.node[k].nnbr = nd;
@@ -1447,15 +1517,11 @@ CATN_HDI inline void load_instance(Ctx& C, const InstDesc& D, const long long* i
   }
 }
 
-}  // namespace catn
-
-namespace catn {
-
 // Load, contract and report one instance in the given slot.
 CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L, const InstDesc& D,
                                   const long long* i64, const int* i32, const double* dat,
-                                  catn_result* res, int* trace_base) {
-  Ctx C = make_ctx(T, slot, L, D.P, D.n);
+                                  catn_result* res, int* trace_base, double* sws, long long sws_doubles) {
+  Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {
     C.trace = trace_base + D.trace_off;
@@ -1472,17 +1538,15 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     res->psi = O.psi;
     res->sign = O.sign;
     res->maxdim = O.maxdim;
-    res->status = C.ctl[CTL_STATUS];
+    res->status = C.ctl[CTL_STATUS] ? C.ctl[CTL_STATUS] : C.status;
     res->nsteps = O.nsteps;
     res->jacobi_max = C.ctl[CTL_JACMAX];
-    res->arena_peak = C.ameta[CATN_NCLS + 1];
+    res->arena_peak = C.sp_peak + 2 * C.h_peak;
+    res->flops = C.acct[0];
+    res->bytes = C.acct[1];
   }
   T.sync();
 }
-
-}  // namespace catn
-
-namespace catn {
 
 // mps2raw of the single surviving open-leg node (tensor_network.jl:517-523,
 // mps_node.jl:52-70) into `out` (capacity `cap` doubles).  Returns the number
@@ -1497,34 +1561,35 @@ CATN_HDI inline long long result_tensor_dev(Ctx& C, double* out, long long cap, 
       if (sref(C, k, p).d != 1) { scalar = false; break; }
     if (!scalar) { open = k; ++cnt; }
   }
-  if (cnt == 0) { *ndim = 0; return 0; }
-  if (cnt > 1) { set_status(C, CATN_ESTATE); return -1; }
+  if (cnt == 0) {
+    if (T.leader()) *ndim = 0;
+    T.sync();
+    return 0;
+  }
+  if (cnt > 1) { fail_all(C, CATN_ESTATE); return -1; }
   const int ns = C.node[open].nsites;
   long long total = 1;
   for (int p = 1; p <= ns; ++p) total *= sref(C, open, p).d;
   SiteRef s0 = sref(C, open, 1);
   long long rmax = s0.dr;
   for (int p = 1; p <= ns; ++p) if (sref(C, open, p).dr > rmax) rmax = sref(C, open, p).dr;
-  long long cur = aalloc(C, 8 * total * rmax);
-  long long nxt = aalloc(C, 8 * total * rmax);
-  if (cur < 0 || nxt < 0) return -1;
-  copy(T, dptr(C, cur), dptr(C, s0.off), (long long)s0.d * s0.dr);
+  double* cur = spush(C, total * rmax);
+  double* nxt = spush(C, total * rmax);
+  if (failed(C)) return -1;
+  copy(T, cur, sdata(C, s0), (long long)s0.d * s0.dr);
   long long pdim = s0.d;
   for (int p = 2; p <= ns; ++p) {
     SiteRef b = sref(C, open, p);
-    gemm(T, pdim, (long long)b.d * b.dr, b.dl, colmajor(dptr(C, cur), pdim), colmajor(dptr(C, b.off), b.dl),
-         colmajor(dptr(C, nxt), pdim));
-    long long t = cur; cur = nxt; nxt = t;
+    gemm(T, pdim, (long long)b.d * b.dr, b.dl, colmajor(cur, pdim), colmajor(sdata(C, b), b.dl), colmajor(nxt, pdim));
+    double* t = cur; cur = nxt; nxt = t;
     pdim *= b.d;
   }
-  if (total <= cap && out) copy(T, out, dptr(C, cur), total);
+  if (total <= cap && out) copy(T, out, cur, total);
   if (T.leader()) {
     for (int p = 1; p <= ns && p <= 64; ++p) dims[p - 1] = sref(C, open, p).d;
     *ndim = ns;
   }
   T.sync();
-  afree(C, cur, 8 * total * rmax);
-  afree(C, nxt, 8 * total * rmax);
   return total;
 }
 

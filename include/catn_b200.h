@@ -69,7 +69,17 @@ typedef struct {
   int32_t nsteps;      /* contraction steps taken                           */
   int32_t jacobi_max;  /* largest Jacobi sweep count seen                   */
   int64_t arena_peak;  /* device bytes high-water mark                      */
+  double flops;        /* algorithmic FLOPs of the contraction (see below)  */
+  double bytes;        /* algorithmic bytes: site tensors read + written    */
 } catn_result;
+/* Algorithmic work convention (per step, FP64 elements of 8 bytes):
+ *   swap / compress pair: 2*m*n*k + 4*m*n*r  (m=d0*d1, n=d2*d3, k bond, r kept)
+ *   cano step:            2*(dl*d)*dr^2 + 2*dr^2*(d'*dr')
+ *   eat fold:             2*Dl*d*Dr + 2*dl2*d2*Dl*Dr
+ *   Dmax cut:             2*(dl*dr)*d^2 * 2 + 2*di*dj*d + 4*di*dj*r
+ *   merge fuse:           2*(dl*d1)*k*(d2*dr2)
+ * bytes count the site tensors each step reads and writes; the merged
+ * two-site matrix and SVD workspaces count as on-chip. */
 
 typedef struct catn_net catn_net;       /* one network, device resident    */
 typedef struct catn_batch catn_batch;   /* many networks, one launch       */

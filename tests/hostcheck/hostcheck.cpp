@@ -21,7 +21,11 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   T.stage = nullptr;
   T.stage_bytes = 0;
   std::vector<int> tr((size_t)im.trace_total + 8);
-  run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data());
+  // stand-in for the GPU's shared-memory SVD workspace (same capacity)
+  const long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  std::vector<double> sws((size_t)sws_doubles);
+  run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
+               sws_doubles);
   if (trace && im.desc[0].trace_cap > 0)
     std::memcpy(trace, tr.data(), sizeof(int) * 8 * (size_t)im.desc[0].trace_cap);
   return res->status;
