@@ -36,7 +36,7 @@ class Result(ct.Structure):
     _fields_ = [("lnZ", ct.c_double), ("err", ct.c_double), ("psi", ct.c_double),
                 ("sign", ct.c_double), ("maxdim", ct.c_int32), ("status", ct.c_int32),
                 ("nsteps", ct.c_int32), ("jacobi_max", ct.c_int32), ("arena_peak", ct.c_int64),
-                ("flops", ct.c_double), ("bytes", ct.c_double)]
+                ("flops", ct.c_double), ("bytes", ct.c_double), ("prof", ct.c_double * 8)]
 
 
 # Every exported symbol with its ctypes signature (argtypes, restype).

@@ -7,6 +7,7 @@
 // slot that stays resident afterwards for result_tensor.
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -52,9 +53,11 @@ constexpr int kThreads = 256;
 constexpr int kSmemBytes = 100 * 1024;
 constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - GEMM_STAGE_BYTES) / 8;
 
+// `order` lists instance ids by descending work estimate, so the longest
+// contractions start first (longest-processing-time scheduling).
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
-    const InstDesc* __restrict__ descs, int ninst, const long long* i64, const int* i32, const double* dat,
-    char* slots, SlotLayout L, catn_result* res, int* trace, int* queue) {
+    const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
+    const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -64,7 +67,10 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
   for (;;) {
     long long inst = 0;
-    if (threadIdx.x == 0) inst = atomicAdd(queue, 1);
+    if (threadIdx.x == 0) {
+      const int q = atomicAdd(queue, 1);
+      inst = q < ninst ? order[q] : ninst;
+    }
     inst = T.bcast(inst);
     if (inst >= ninst) break;
     run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles);
@@ -97,6 +103,7 @@ struct DeviceRun {
   char* h_input = nullptr;   // pinned
   char* d_input = nullptr;
   InstDesc* d_desc = nullptr;
+  int* d_order = nullptr;
   long long* d_i64 = nullptr;
   int* d_i32 = nullptr;
   double* d_dat = nullptr;
@@ -113,7 +120,7 @@ struct DeviceRun {
     cudaFreeHost(h_input);
     cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
     h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
-    d_desc = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
+    d_desc = nullptr; d_order = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
   }
 };
 
@@ -136,7 +143,12 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   if (ns * R.L.slot_bytes > budget) ns = budget / R.L.slot_bytes;
   if (ns < 1) return fail(CATN_ENOMEM, "not enough device memory for one slot");
   R.nslots = (int)ns;
-  const long long b_desc = align256((long long)(sizeof(InstDesc) * im.desc.size()));
+  const long long b_desc = align256((long long)(sizeof(InstDesc) * im.desc.size())) +
+                           align256((long long)(sizeof(int) * im.desc.size()));
+  std::vector<int> order(im.desc.size());
+  for (size_t q = 0; q < order.size(); ++q) order[q] = (int)q;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return im.desc[a].cost > im.desc[b].cost; });
   const long long b_i64 = align256((long long)(sizeof(long long) * (im.i64.size() + 1)));
   const long long b_i32 = align256((long long)(sizeof(int) * (im.i32.size() + 1)));
   const long long b_dat = align256((long long)(sizeof(double) * (im.dat.size() + 1)));
@@ -145,10 +157,13 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   CUDA_TRY(cudaMalloc(&R.d_input, (size_t)R.input_bytes));
   std::memset(R.h_input, 0, (size_t)R.input_bytes);
   std::memcpy(R.h_input, im.desc.data(), sizeof(InstDesc) * im.desc.size());
+  const long long off_order = align256((long long)(sizeof(InstDesc) * im.desc.size()));
+  std::memcpy(R.h_input + off_order, order.data(), sizeof(int) * order.size());
   if (!im.i64.empty()) std::memcpy(R.h_input + b_desc, im.i64.data(), sizeof(long long) * im.i64.size());
   if (!im.i32.empty()) std::memcpy(R.h_input + b_desc + b_i64, im.i32.data(), sizeof(int) * im.i32.size());
   if (!im.dat.empty()) std::memcpy(R.h_input + b_desc + b_i64 + b_i32, im.dat.data(), sizeof(double) * im.dat.size());
   R.d_desc = (InstDesc*)R.d_input;
+  R.d_order = (int*)(R.d_input + off_order);
   R.d_i64 = (long long*)(R.d_input + b_desc);
   R.d_i32 = (int*)(R.d_input + b_desc + b_i64);
   R.d_dat = (double*)(R.d_input + b_desc + b_i64 + b_i32);
@@ -166,8 +181,9 @@ catn_status upload(const Image&, DeviceRun& R, cudaStream_t st) {
 
 catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, sizeof(int), st));
-  catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.ninst, R.d_i64, R.d_i32, R.d_dat,
-                                                                R.d_slots, R.L, R.d_res, R.d_trace, R.d_queue);
+  catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
+                                                                R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
+                                                                R.d_queue);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

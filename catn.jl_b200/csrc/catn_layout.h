@@ -24,6 +24,8 @@ struct SiteRef {
 
 struct EdgeEnt {
   int cost, i, j, next, prev, alive;
+  int seq;   // insertion sequence number (bucket order = ascending seq)
+  int pad;
 };
 
 // Control words of a running instance.
@@ -34,6 +36,7 @@ enum {
   CTL_JACMAX = 3,   // max Jacobi sweeps seen
   CTL_NSTEPS = 4,
   CTL_ANOMALY = 5,  // bucket bookkeeping anomaly counter (diagnostic)
+  CTL_SEQ = 6,      // next insertion sequence number
   CTL_WORDS = 8
 };
 
@@ -50,7 +53,7 @@ struct InstDesc {
   long long data_off;  // double image: tensors in order
   long long data_len;
   int trace_cap;       // records of 8 int32 (0 = no trace)
-  int pad;
+  int cost;            // work estimate (real edges) used to order the queue
   long long trace_off; // int32 offset into the trace buffer
 };
 
@@ -58,7 +61,7 @@ struct InstDesc {
 struct SlotLayout {
   int nmax, maxs, ecap, pcap;
   long long off_node, off_site, off_nbr, off_ent, off_bhead, off_btail, off_bcnt, off_emap;
-  long long off_ctl, off_pairs, off_list, off_tmp, off_ameta, off_arena;
+  long long off_ctl, off_pairs, off_list, off_tmp, off_ameta, off_ldc, off_arena;
   int lcap, pad;
   long long arena_bytes, slot_bytes;
 };
@@ -90,6 +93,7 @@ inline SlotLayout make_layout(int nmax, int maxs, int ecap, long long arena_byte
   L.off_list = o;  o = align256(o + (long long)L.lcap * 4LL);
   L.off_tmp = o;   o = align256(o + (2LL * maxs + 8) * 4LL);
   L.off_ameta = o; o = align256(o + (CATN_NCLS + 4) * 8LL);
+  L.off_ldc = o;   o = align256(o + nn * 16LL);   // per-node logdim cache: value + valid flag
   L.off_arena = o;
   L.arena_bytes = arena_bytes;
   L.slot_bytes = align256(o + arena_bytes);

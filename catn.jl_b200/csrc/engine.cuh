@@ -63,6 +63,8 @@ struct Ctx {
   double* sws;
   long long sws_doubles;
   double* acct;   // [flops, bytes] (global, leader-updated)
+  double* ldc;    // per-node logdim cache [n+1] (leader-maintained)
+  long long* ldv; // cache validity [n+1]
   int status;     // uniform copy of the instance status
   int* trace;
   int trace_cap;
@@ -92,6 +94,21 @@ CATN_HD int failed(const Ctx& C) { return C.status != 0; }
 // ---------------------------------------------------------------------------
 CATN_HD long long al256(long long b) { return (b + 255) & ~255LL; }
 
+// SM clock for the per-instance cycle breakdown (0 in the host build).
+CATN_HD long long clk() {
+#if CATN_DEVICE_PASS
+  return (long long)clock64();
+#else
+  return 0;
+#endif
+}
+enum { PROF_TOTAL = 0, PROF_SVD_SMALL, PROF_SVD_LARGE, PROF_BOOK, PROF_COMPACT, PROF_N_SMALL, PROF_N_LARGE,
+       PROF_N_COMPACT };
+CATN_HD void prof_add(Ctx& C, int slot, double v) {
+  if (C.T.leader()) C.acct[2 + slot] += v;
+}
+
+
 CATN_HD double* spush(Ctx& C, long long ndoubles) {
   long long bytes = al256(8 * (ndoubles > 0 ? ndoubles : 1));
   if (C.sp + bytes > C.sp_hi) {
@@ -118,6 +135,7 @@ CATN_HD double* sdata(const Ctx& C, const SiteRef& s) { return (double*)(C.base 
 // Move every live site into the other heap half, contiguously.
 CATN_HDI inline void heap_compact(Ctx& C) {
   const Team& T = C.T;
+  const long long t0 = clk();
   T.sync();
   const long long lo = C.half ? C.h_lo0 : C.h_lo1;
   long long cur = lo;
@@ -149,6 +167,8 @@ CATN_HDI inline void heap_compact(Ctx& C) {
   C.hb = cur;
   C.he = lo + C.hsize;
   C.compactions += 1;
+  prof_add(C, PROF_COMPACT, (double)(clk() - t0));
+  prof_add(C, PROF_N_COMPACT, 1.0);
 }
 
 // Make room for `bytes` of new sites (may compact: re-read site refs after).
@@ -232,16 +252,21 @@ struct SvdIn {
   double* W;
   long long m, n, mm, nn;
   bool wide, smem;
+  double tol;   // rank-revealing stop tolerance for large inputs (0 = none)
 };
 
 CATN_HD long long svd_ws_doubles(long long mm, long long nn) {
   return 2 * mm * nn + 3 * nn * nn + 8 * nn + 64;
 }
 
-CATN_HDI inline SvdIn svd_begin(Ctx& C, long long m, long long n) {
+// `cutoff`: the truncation cutoff the caller applies to the singular values;
+// large inputs may drop a trailing block whose singular values are all below
+// a quarter of it (never counted, never kept).
+CATN_HDI inline SvdIn svd_begin(Ctx& C, long long m, long long n, double cutoff = 0.0) {
   SvdIn s;
   s.m = m;
   s.n = n;
+  s.tol = 0.25 * cutoff;
   s.wide = m < n;
   s.mm = s.wide ? n : m;
   s.nn = s.wide ? m : n;
@@ -262,6 +287,74 @@ CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
   T.sync();
 }
 
+// Large input whose pivoted QR W P = Q R stopped at rank r (trailing block
+// dropped): SVD of the r x nn top block T = [R11 R12] P^T through its
+// transpose (pivoted QR + Jacobi again), then U_W = Q1 * V_T, V_W = U_T.
+CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const double* tau, const int* piv,
+                                  long long t0) {
+  const Team& T = C.T;
+  Svd R;
+  R.m = s.m; R.n = s.n; R.p = 0; R.U = R.S = R.V = nullptr;
+  const long long mm = s.mm, nn = s.nn;
+  double* Tt = spush(C, nn * r);
+  double* tau2 = spush(C, r);
+  double* nrm2 = spush(C, r);
+  int* piv2 = (int*)spush(C, r / 2 + 1);
+  double* X2 = spush(C, r * r);
+  double* Vb2 = spush(C, r * r);
+  double* sig2 = spush(C, r);
+  double* S2 = spush(C, r);
+  int* perm2 = (int*)spush(C, r / 2 + 1);
+  double* Uin = spush(C, nn * r);
+  double* Vin = spush(C, r * r);
+  double* Uw = spush(C, mm * r);
+  if (failed(C)) return R;
+  for (long long e = T.rank(); e < nn * r; e += T.size()) {
+    long long j = e % nn, i = e / nn;   // Tt[piv[j], i] = R[i, j]
+    Tt[(long long)piv[j] + nn * i] = (j >= i) ? s.W[i + j * mm] : 0.0;
+  }
+  T.sync();
+  qrcp_inplace(T, Tt, nn, r, nn, tau2, piv2, nrm2, 0.0);
+  for (long long e = T.rank(); e < r * r; e += T.size()) {
+    long long i = e % r, j = e / r;
+    X2[e] = (j <= i) ? Tt[j + i * nn] : 0.0;
+  }
+  T.sync();
+  int sweeps = jacobi_sweeps(T, X2, r, r, r, Vb2, 60);
+  if (sweeps < 0) fail_all(C, CATN_ENOCONV);
+  if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
+  sort_columns(T, X2, r, r, r, sig2, S2, perm2);
+  for (long long e = T.rank(); e < nn * r; e += T.size()) {
+    long long rr = e % nn, c = e / nn;
+    Uin[e] = (rr < r) ? Vb2[rr + (long long)perm2[c] * r] : 0.0;
+  }
+  for (long long e = T.rank(); e < r * r; e += T.size()) {
+    long long i = e % r, c = e / r;
+    double sv = S2[c];
+    Vin[(long long)piv2[i] + c * r] = (sv > 0.0) ? X2[i + (long long)perm2[c] * r] / sv : 0.0;
+  }
+  T.sync();
+  qr_apply_q(T, Tt, nn, r, nn, tau2, Uin, r, nn);
+  for (long long e = T.rank(); e < mm * r; e += T.size()) {
+    long long rr = e % mm, c = e / mm;
+    Uw[e] = (rr < r) ? Vin[rr + c * r] : 0.0;
+  }
+  T.sync();
+  qr_apply_q(T, s.W, mm, r, mm, tau, Uw, r, mm);
+  prof_add(C, PROF_SVD_LARGE, (double)(clk() - t0));
+  prof_add(C, PROF_N_LARGE, 1.0);
+  R.p = r;
+  R.S = S2;
+  if (!s.wide) {
+    R.U = Uw;
+    R.V = Uin;
+  } else {
+    R.U = Uin;
+    R.V = Uw;
+  }
+  return R;
+}
+
 // Drmac-Veselic preconditioned one-sided Jacobi: pivoted Householder QR
 // W P = Q R, one-sided Jacobi on X = R^T (X V' = U' Sigma), so that
 // W = (Q V') Sigma (P U')^T.  The pivoted, transposed triangle converges in
@@ -271,6 +364,7 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   Svd R;
   R.m = s.m; R.n = s.n; R.p = 0; R.U = R.S = R.V = nullptr;
   if (failed(C) || !s.W) return R;
+  const long long t0 = clk();
   const long long mm = s.mm, nn = s.nn;
   double *X, *Vb, *Ut, *Vt, *tau, *nrm, *sig, *Sout;
   int *piv, *perm;
@@ -287,19 +381,35 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     piv = (int*)q; q += (nn + 1) / 2 + 1;
     perm = (int*)q;
   } else {
+    tau = spush(C, nn);
+    nrm = spush(C, nn);
+    piv = (int*)spush(C, (nn + 1) / 2 + 1);
+    X = Vb = Vt = Ut = sig = Sout = nullptr;
+    perm = nullptr;
+    if (failed(C)) return R;
+  }
+  double stop = 0.0;
+  if (!s.smem && s.tol > 0.0) {
+    // truncate only when the matrix is far above the tolerance, so that the
+    // "keep everything when nothing passes the cutoff" rule never meets a
+    // truncated factorisation
+    double f2 = 0.0;
+    for (long long e = T.rank(); e < mm * nn; e += T.size()) f2 = fma(s.W[e], s.W[e], f2);
+    f2 = T.sum(f2);
+    if (sqrt(f2) > 1e6 * s.tol) stop = s.tol;
+  }
+  const long long r = qrcp_inplace(T, s.W, mm, nn, mm, tau, piv, nrm, stop);
+  if (r < nn) return svd_truncated(C, s, r, tau, piv, t0);
+  if (!s.smem) {
     X = spush(C, nn * nn);
     Vb = spush(C, nn * nn);
     Vt = spush(C, nn * nn);
     Ut = spush(C, mm * nn);
-    tau = spush(C, nn);
-    nrm = spush(C, nn);
     sig = spush(C, nn);
     Sout = spush(C, nn);
-    piv = (int*)spush(C, (nn + 1) / 2 + 1);
     perm = (int*)spush(C, (nn + 1) / 2 + 1);
     if (failed(C)) return R;
   }
-  qrcp_inplace(T, s.W, mm, nn, mm, tau, piv, nrm);
   for (long long e = T.rank(); e < nn * nn; e += T.size()) {
     long long i = e % nn, j = e / nn;
     X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
@@ -320,6 +430,8 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   }
   T.sync();
   qr_apply_q(T, s.W, mm, nn, mm, tau, Ut, nn, mm);
+  prof_add(C, s.smem ? PROF_SVD_SMALL : PROF_SVD_LARGE, (double)(clk() - t0));
+  prof_add(C, s.smem ? PROF_N_SMALL : PROF_N_LARGE, 1.0);
   R.p = nn;
   R.S = Sout;
   if (!s.wide) {
@@ -371,7 +483,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       const long long mark = C.sp;
       SiteRef s = sref(C, k, i);
       const long long m = (long long)s.dl * s.d, n = s.dr;
-      SvdIn in = svd_begin(C, m, n);
+      SvdIn in = svd_begin(C, m, n, C.P.cutoff);
       if (failed(C)) return;
       svd_fill(C, in, colmajor(sdata(C, s), m));
       Svd R = svd_finish(C, in);
@@ -403,7 +515,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       SiteRef s = sref(C, k, i);
       const long long dl = s.dl, m = (long long)s.d * s.dr;
       // Mt = permutedims(site, (2,3,1)) as (d*dr) x dl = transpose of the dl x (d*dr) view
-      SvdIn in = svd_begin(C, m, dl);
+      SvdIn in = svd_begin(C, m, dl, C.P.cutoff);
       if (failed(C)) return;
       svd_fill(C, in, transposed(sdata(C, s), dl));
       Svd R = svd_finish(C, in);
@@ -455,7 +567,8 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   SiteRef tl = sref(C, k, lo), tr = sref(C, k, hi);
   const long long d0 = tl.dl, d1 = tr.d, d2 = tl.d, d3 = tr.dr, kk = tl.dr;
   const long long m = d0 * d1, n = d2 * d3;
-  SvdIn in = svd_begin(C, m, n);
+  const bool rsvd_route = C.P.swapopt && ((m > 7000 && n > 7000) || m > 20000 || n > 20000);
+  SvdIn in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);
   if (failed(C)) return 0.0;
   // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
   // straight into the SVD's oriented input.
@@ -464,7 +577,6 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
                       : mop(in.W, imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2));
     gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
   }
-  const bool rsvd_route = C.P.swapopt && ((m > 7000 && n > 7000) || m > 20000 || n > 20000);
   Svd R = svd_finish(C, in);
   if (failed(C)) return 0.0;
   double err = 0.0;
@@ -819,7 +931,7 @@ CATN_HDI inline double compress_node(Ctx& C, int k, bool opt) {
     double e;
     Svd R;
     if (!opt) {
-      SvdIn in = svd_begin(C, ml, nr);
+      SvdIn in = svd_begin(C, ml, nr, C.P.cutoff);
       if (failed(C)) return err;
       gemm(T, ml, nr, dd, colmajor(sdata(C, tl), ml), colmajor(sdata(C, tr), dd), svd_target(in));
       R = svd_finish(C, in);
@@ -835,7 +947,7 @@ CATN_HDI inline double compress_node(Ctx& C, int k, bool opt) {
       QRed qr = qr_reduce(C, matrt, nr, dd);
       if (failed(C)) return err;
       // mat = Rl * Rr^H  (ql.rrows x qr.rrows)
-      SvdIn in = svd_begin(C, ql.rrows, qr.rrows);
+      SvdIn in = svd_begin(C, ql.rrows, qr.rrows, C.P.cutoff);
       if (failed(C)) return err;
       gemm(T, ql.rrows, qr.rrows, dd, colmajor(ql.Rb, ql.rrows), transposed(qr.Rb, qr.rrows), svd_target(in));
       R = svd_finish(C, in);
@@ -901,7 +1013,7 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   QRed qi = qr_reduce(C, mi, ri_rows, d);
   QRed qj = qr_reduce(C, mj, rj_rows, d);
   if (failed(C)) return 0.0;
-  SvdIn in = svd_begin(C, qi.rrows, qj.rrows);
+  SvdIn in = svd_begin(C, qi.rrows, qj.rrows, C.P.cutoff);
   if (failed(C)) return 0.0;
   gemm(T, qi.rrows, qj.rrows, d, colmajor(qi.Rb, qi.rrows), transposed(qj.Rb, qj.rrows), svd_target(in));
   Svd R = svd_finish(C, in);
@@ -975,7 +1087,7 @@ CATN_HDI inline void raw2mps(Ctx& C, int k, const double* data, const long long*
   long long cur = total, dleft = 1;
   for (int q = 0; q < nd - 1; ++q) {
     const long long m = dleft * dims[q], n = cur / m;
-    SvdIn in = svd_begin(C, m, n);
+    SvdIn in = svd_begin(C, m, n, C.P.cutoff);
     if (failed(C)) return;
     svd_fill(C, in, colmajor(R, m));
     Svd S = svd_finish(C, in);
@@ -1011,9 +1123,19 @@ CATN_HDI inline void raw2mps(Ctx& C, int k, const double* data, const long long*
 // ---------------------------------------------------------------------------
 // edge-cost buckets (tensor_network.jl:152-236), leader-only helpers
 // ---------------------------------------------------------------------------
-CATN_HD int dim_after_merge(const Ctx& C, int i, int j) {
+// logdim of node k through the leader's cache.  Entries are invalidated for
+// every node whose sites a contraction step may touch, so the value is always
+// the reference's left fold over the current sites.
+CATN_HD double logdim_cached(Ctx& C, int k) {
+  if (C.ldv[k]) return C.ldc[k];
+  double v = logdim_all(C, k);
+  C.ldc[k] = v;
+  C.ldv[k] = 1;
+  return v;
+}
+CATN_HD int dim_after_merge(Ctx& C, int i, int j) {
   int idx = nb_find(C, i, j);
-  double v = logdim_all(C, i) + logdim_all(C, j) - 2.0 * logdim_at(C, i, idx);
+  double v = logdim_cached(C, i) + logdim_cached(C, j) - 2.0 * logdim_at(C, i, idx);
   return (int)rint(v);
 }
 CATN_HD int& emap_at(const Ctx& C, int i, int j) { return C.emap[(long long)i * (C.n + 1) + j]; }
@@ -1025,6 +1147,7 @@ CATN_HD void bucket_add_leader(Ctx& C, int cost, int i, int j) {
   C.ctl[CTL_FREEENT] = C.ent[e].next;
   EdgeEnt& E = C.ent[e];
   E.cost = cost; E.i = i; E.j = j; E.alive = 1; E.next = -1; E.prev = C.btail[cost];
+  E.seq = C.ctl[CTL_SEQ]++;
   if (C.btail[cost] >= 0) C.ent[C.btail[cost]].next = e;
   else C.bhead[cost] = e;
   C.btail[cost] = e;
@@ -1137,48 +1260,63 @@ CATN_HD int min_cost_leader(Ctx& C) {
   return c;
 }
 
-// select_edge_min_dim (:248-253) / _triangle (:262-288) / _sequentially (:300-316)
-CATN_HD long long select_leader(Ctx& C, int* maxdim) {
-  int sel = C.P.select;
+// select_edge_min_dim (:248-253) / _triangle (:262-288) / _sequentially
+// (:300-316), as team reductions.  Bucket order is insertion order, so the
+// triangle selector's "first candidate with the largest count" is the entry
+// with the largest count and, among those, the smallest insertion sequence.
+CATN_HDI inline long long select_team(Ctx& C, int* maxdim) {
+  const Team& T = C.T;
+  const int sel = C.P.select;
   if (sel == 0 || sel == 1) {
-    int cost = min_cost_leader(C);
-    if (cost >= CATN_CMAX) { fail_leader(C, CATN_ESTATE); return 0; }
-    if (cost > *maxdim) *maxdim = cost;
-    int e = C.bhead[cost];
-    int bi = C.ent[e].i, bj = C.ent[e].j;
-    if (sel == 1) {
-      int best = -1;
-      for (int guard = 0; e >= 0 && guard <= C.ecap; e = C.ent[e].next, ++guard) {
-        int i = C.ent[e].i, j = C.ent[e].j;
-        int nn = C.node[j].nnbr;
-        int both = 0;
-        for (int p = 1; p <= nn; ++p) {
-          int k = nbref(C, j, p);
-          if (k <= 0 || k == i) continue;
-          bool dup = false;
-          for (int q = 1; q < p; ++q)
-            if (nbref(C, j, q) == k) { dup = true; break; }
-          if (dup) continue;
-          if (nb_find(C, k, i) > 0) ++both;
-        }
-        if (both > best) { best = both; bi = i; bj = j; }
+    long long cost = 0;
+    T.sync();
+    if (T.leader()) cost = min_cost_leader(C);
+    cost = T.bcast(cost);
+    if (cost >= CATN_CMAX) { fail_all(C, CATN_ESTATE); return 0; }
+    if (cost > *maxdim) *maxdim = (int)cost;
+    if (sel == 0) {
+      const int e = C.bhead[cost];
+      return ((long long)C.ent[e].i << 32) | (unsigned)C.ent[e].j;
+    }
+    double bv = -1.0;
+    long long be = -1;
+    for (int e = T.rank(); e < C.ecap; e += T.size()) {
+      const EdgeEnt E = C.ent[e];
+      if (!E.alive || E.cost != cost) continue;
+      const int i = E.i, j = E.j, nn = C.node[j].nnbr;
+      int both = 0;
+      for (int p = 1; p <= nn; ++p) {
+        const int k = nbref(C, j, p);
+        if (k <= 0 || k == i) continue;
+        bool dup = false;
+        for (int q = 1; q < p; ++q)
+          if (nbref(C, j, q) == k) { dup = true; break; }
+        if (dup) continue;
+        if (nb_find(C, k, i) > 0) ++both;
       }
+      const double key = (double)both * 2147483648.0 + (double)(0x7fffffff - E.seq);
+      if (be < 0 || key > bv) { bv = key; be = e; }
     }
-    return ((long long)bi << 32) | (unsigned)bj;
+    const long long e = T.argmax(bv, be);
+    if (e < 0) { fail_all(C, CATN_ESTATE); return 0; }
+    return ((long long)C.ent[e].i << 32) | (unsigned)C.ent[e].j;
   }
-  // sequential: minimum i + nb, ascending node ids
-  long long best = -1;
-  int bs = 0x7fffffff;
-  for (int i = 1; i <= C.n; ++i) {
-    int nn = C.node[i].nnbr;
+  // sequential: minimum i + nb, ties by ascending node id
+  double bv = -1.0;
+  long long bi = -1;
+  for (int i = 1 + T.rank(); i <= C.n; i += T.size()) {
+    const int nn = C.node[i].nnbr;
     for (int p = 1; p <= nn; ++p) {
-      int nb = nbref(C, i, p);
+      const int nb = nbref(C, i, p);
       if (nb <= 0 || !(i < nb)) continue;
-      if (i + nb < bs) { bs = i + nb; best = ((long long)i << 32) | (unsigned)nb; }
+      const double key = -((double)(i + nb) * 4194304.0 + (double)i);
+      if (bi < 0 || key > bv) { bv = key; bi = ((long long)i << 32) | (unsigned)nb; }
     }
   }
-  if (best < 0) fail_leader(C, CATN_ESTATE);
-  return best < 0 ? 0 : best;
+  // argmax breaks ties on the packed pair; keys are distinct per (sum, i)
+  const long long best = T.argmax(bv, bi);
+  if (best < 0) { fail_all(C, CATN_ESTATE); return 0; }
+  return best;
 }
 
 CATN_HDI inline int has_real_edges(Ctx& C) {
@@ -1226,13 +1364,8 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
       break;
     }
     // --- select ---
-    long long pk = 0;
-    int md = maxdim;
-    T.sync();
-    if (T.leader()) pk = select_leader(C, &md);
-    pk = T.bcast(pk);
-    maxdim = (int)T.bcast(md);
-    refresh_status(C);
+    const long long tb0 = clk();
+    const long long pk = select_team(C, &maxdim);
     if (failed(C)) break;
     int i = (int)(pk >> 32), j = (int)(pk & 0xffffffff);
     if (C.node[j].nsites > C.node[i].nsites) { int t = i; i = j; j = t; }
@@ -1247,9 +1380,13 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
         for (int p = 1; p <= C.node[i].nnbr; ++p) list[nl++] = nbref(C, i, p);
         for (int p = 1; p <= C.node[j].nnbr; ++p) list[nl++] = nbref(C, j, p);
         count_remove_nodes_leader(C, list, nl);
+        // every node whose sites this step may change: i, j and their neighbours
+        for (int q = 0; q < nl; ++q)
+          if (list[q] > 0) C.ldv[list[q]] = 0;
       }
       refresh_status(C);
     }
+    prof_add(C, PROF_BOOK, (double)(clk() - tb0));
     int idx_j_in_i = nb_find(C, i, j);
     int idx_i_in_j = nb_find(C, j, i);
     int rev = 0;
@@ -1321,6 +1458,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
     if (C.P.compress) compress_node(C, i, C.P.svdopt != 0);   // error discarded (:688-694)
     if (failed(C)) break;
     if (buckets) {
+      const long long tb1 = clk();
       T.sync();
       if (T.leader()) {
         int* list = C.list;
@@ -1330,6 +1468,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
         count_add_nodes_leader(C, list, nl);
       }
       refresh_status(C);
+      prof_add(C, PROF_BOOK, (double)(clk() - tb1));
     }
     const int nsi = C.node[i].nsites;
     unsigned shh = 2166136261u;
@@ -1402,6 +1541,8 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.list = (int*)(slot + L.off_list);
   C.tmp = (int*)(slot + L.off_tmp);
   C.acct = (double*)(slot + L.off_ameta);
+  C.ldc = (double*)(slot + L.off_ldc);
+  C.ldv = (long long*)(slot + L.off_ldc) + (C.n + 1);
   C.base = slot + L.off_arena;
   // arena: scratch stack (40%), two heap halves (30% each)
   const long long cap = L.arena_bytes & ~255LL;
@@ -1435,14 +1576,16 @@ CATN_HDI inline void reset_slot(Ctx& C) {
     C.ent[e].alive = 0;
     C.ent[e].next = (e + 1 < C.ecap) ? (int)(e + 1) : -1;
   }
-  for (long long e = T.rank(); e < nn; e += T.size()) { C.node[e].nsites = 0; C.node[e].nnbr = 0; C.node[e].cano = 0; C.node[e].pad = 0; }
+  for (long long e = T.rank(); e < nn; e += T.size()) {
+    C.node[e].nsites = 0; C.node[e].nnbr = 0; C.node[e].cano = 0; C.node[e].pad = 0;
+    C.ldv[e] = 0;
+  }
   for (long long e = T.rank(); e < CTL_WORDS; e += T.size()) C.ctl[e] = 0;
   T.sync();
   if (T.leader()) {
     C.ctl[CTL_FREEENT] = C.ecap > 0 ? 0 : -1;
     C.ctl[CTL_MINC] = 0;
-    C.acct[0] = 0.0;
-    C.acct[1] = 0.0;
+    for (int q = 0; q < 10; ++q) C.acct[q] = 0.0;
   }
   T.sync();
 }
@@ -1530,7 +1673,9 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
   load_instance(C, D, i64, i32, dat);
   ContractOut O;
   O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
+  const long long t0 = clk();
   if (!failed(C)) O = contract(C);
+  prof_add(C, PROF_TOTAL, (double)(clk() - t0));
   T.sync();
   if (T.leader()) {
     res->lnZ = O.lnZ;
@@ -1544,6 +1689,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     res->arena_peak = C.sp_peak + 2 * C.h_peak;
     res->flops = C.acct[0];
     res->bytes = C.acct[1];
+    for (int q = 0; q < 8; ++q) res->prof[q] = C.acct[2 + q];
   }
   T.sync();
 }

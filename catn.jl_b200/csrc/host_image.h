@@ -209,6 +209,7 @@ struct Image {
  private:
   void finish(InstDesc& D, int n, int edges, int trace_cap) {
     D.trace_cap = trace_cap;
+    D.cost = edges;
     D.trace_off = trace_total;
     trace_total += 8LL * trace_cap;
     desc.push_back(D);

@@ -211,8 +211,12 @@ CATN_HDI inline void qr_inplace(const Team& T, double* A, long long m, long long
 // Householder QR with column pivoting, m >= n, in place: A P = Q R
 // (LAPACK dgeqp3 semantics; partial column norms are recomputed exactly
 // while each reflector is applied).  piv[k] = original index of column k.
-CATN_HDI inline void qrcp_inplace(const Team& T, double* A, long long m, long long n, long long lda,
-                                  double* tau, int* piv, double* nrm) {
+// With stop_tol > 0 the factorisation ends at the first step k >= 1 where
+// the trailing block's Frobenius norm sqrt(sum_j>=k nrm[j]) <= stop_tol and
+// returns that rank k (every singular value of the dropped block is below
+// stop_tol); otherwise it returns n.
+CATN_HDI inline long long qrcp_inplace(const Team& T, double* A, long long m, long long n, long long lda,
+                                       double* tau, int* piv, double* nrm, double stop_tol = 0.0) {
   for (long long j = T.warp(); j < n; j += T.nwarps()) {
     const double* aj = A + j * lda;
     double s = 0.0;
@@ -223,11 +227,16 @@ CATN_HDI inline void qrcp_inplace(const Team& T, double* A, long long m, long lo
   T.sync();
   for (long long k = 0; k < n; ++k) {
     // pivot: largest remaining partial norm
-    double bv = -1.0;
+    double bv = -1.0, rem = 0.0;
     long long bi = -1;
     for (long long j = k + T.rank(); j < n; j += T.size()) {
       double v = nrm[j];
+      rem += v;
       if (bi < 0 || v > bv) { bv = v; bi = j; }
+    }
+    if (stop_tol > 0.0 && k > 0) {
+      rem = T.sum(rem);
+      if (rem <= stop_tol * stop_tol) return k;
     }
     long long p = T.argmax(bv, bi);
     if (p != k && p >= 0) {
@@ -279,6 +288,7 @@ CATN_HDI inline void qrcp_inplace(const Team& T, double* A, long long m, long lo
     }
     T.sync();
   }
+  return n;
 }
 
 // C(m x ncols, ld ldc) <- Q * C with Q = H_0 ... H_{n-1} from qr_inplace.

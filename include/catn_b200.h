@@ -71,6 +71,10 @@ typedef struct {
   int64_t arena_peak;  /* device bytes high-water mark                      */
   double flops;        /* algorithmic FLOPs of the contraction (see below)  */
   double bytes;        /* algorithmic bytes: site tensors read + written    */
+  double prof[8];      /* SM cycles: [0] contraction total, [1] small SVDs,
+                          [2] large SVDs, [3] edge bookkeeping, [4] heap
+                          compaction; counts: [5] small SVDs, [6] large
+                          SVDs, [7] compactions                            */
 } catn_result;
 /* Algorithmic work convention (per step, FP64 elements of 8 bytes):
  *   swap / compress pair: 2*m*n*k + 4*m*n*r  (m=d0*d1, n=d2*d3, k bond, r kept)

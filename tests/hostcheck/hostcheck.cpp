@@ -22,8 +22,11 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   T.stage_bytes = 0;
   std::vector<int> tr((size_t)im.trace_total + 8);
   // stand-in for the GPU's shared-memory SVD workspace (same capacity)
-  const long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
-  std::vector<double> sws((size_t)sws_doubles);
+  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  // CATN_HOSTCHECK_SWS overrides the capacity (0 sends every SVD through the
+  // large-matrix path, including its rank-revealing truncation)
+  if (const char* e = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(e);
+  std::vector<double> sws((size_t)(sws_doubles > 0 ? sws_doubles : 1));
   run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
                sws_doubles);
   if (trace && im.desc[0].trace_cap > 0)
