@@ -36,7 +36,7 @@ class Result(ct.Structure):
     _fields_ = [("lnZ", ct.c_double), ("err", ct.c_double), ("psi", ct.c_double),
                 ("sign", ct.c_double), ("maxdim", ct.c_int32), ("status", ct.c_int32),
                 ("nsteps", ct.c_int32), ("jacobi_max", ct.c_int32), ("arena_peak", ct.c_int64),
-                ("flops", ct.c_double), ("bytes", ct.c_double), ("prof", ct.c_double * 8)]
+                ("flops", ct.c_double), ("bytes", ct.c_double), ("prof", ct.c_double * 16)]
 
 
 # Every exported symbol with its ctypes signature (argtypes, restype).
@@ -75,7 +75,7 @@ def load(path=None):
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("CATN_B200_LIB") or LIB_PATH
     if not os.path.exists(p):
         raise CatnError(CATN_ECUDA, f"libcatn_b200.so not built ({p}); run __graft_entry__.build()")
     lib = ct.CDLL(p)

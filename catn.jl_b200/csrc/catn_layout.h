@@ -8,7 +8,6 @@
 namespace catn {
 
 constexpr int CATN_NCLS = 40;      // arena size classes: 64 B << c
-constexpr int CATN_CMAX = 8192;    // edge-cost buckets (log2 sizes)
 
 struct NodeHdr {
   int nsites;
@@ -22,21 +21,24 @@ struct SiteRef {
   long long off;   // byte offset of the (dl, d, dr) column-major tensor in the arena
 };
 
+// One pair [i, j] in the bucket of its cost (the reference's edge_count).
 struct EdgeEnt {
-  int cost, i, j, next, prev, alive;
-  int seq;   // insertion sequence number (bucket order = ascending seq)
+  int cost, i, j;
+  int alive;   // 1 while in its bucket
+  int seq;     // insertion sequence number (bucket order = ascending seq)
   int pad;
 };
 
 // Control words of a running instance.
 enum {
   CTL_STATUS = 0,   // catn_status
-  CTL_MINC = 1,     // lowest possibly non-empty cost bucket
-  CTL_FREEENT = 2,  // head of the free entry list
+  CTL_FTOP = 1,     // entries on the free stack
+  CTL_SPARE = 2,    // scratch counter for team atomics
   CTL_JACMAX = 3,   // max Jacobi sweeps seen
   CTL_NSTEPS = 4,
   CTL_ANOMALY = 5,  // bucket bookkeeping anomaly counter (diagnostic)
   CTL_SEQ = 6,      // next insertion sequence number
+  CTL_BCAST = 7,    // scratch word for team broadcasts of small results
   CTL_WORDS = 8
 };
 
@@ -54,13 +56,15 @@ struct InstDesc {
   long long data_len;
   int trace_cap;       // records of 8 int32 (0 = no trace)
   int cost;            // work estimate (real edges) used to order the queue
+  int multigraph;      // some node lists the same neighbour twice
+  int pad2;
   long long trace_off; // int32 offset into the trace buffer
 };
 
 // Byte layout of one CTA slot (control state + arena).
 struct SlotLayout {
   int nmax, maxs, ecap, pcap;
-  long long off_node, off_site, off_nbr, off_ent, off_bhead, off_btail, off_bcnt, off_emap;
+  long long off_node, off_site, off_nbr, off_ent, off_fstack, off_emap;
   long long off_ctl, off_pairs, off_list, off_tmp, off_ameta, off_ldc, off_arena;
   int lcap, pad;
   long long arena_bytes, slot_bytes;
@@ -84,15 +88,13 @@ inline SlotLayout make_layout(int nmax, int maxs, int ecap, long long arena_byte
   L.off_site = o;  o = align256(o + nn * maxs * (long long)sizeof(SiteRef));
   L.off_nbr = o;   o = align256(o + nn * maxs * 4LL);
   L.off_ent = o;   o = align256(o + (long long)ecap * (long long)sizeof(EdgeEnt));
-  L.off_bhead = o; o = align256(o + CATN_CMAX * 4LL);
-  L.off_btail = o; o = align256(o + CATN_CMAX * 4LL);
-  L.off_bcnt = o;  o = align256(o + CATN_CMAX * 4LL);
+  L.off_fstack = o; o = align256(o + (long long)ecap * 4LL);   // free stack of entry ids
   L.off_emap = o;  o = align256(o + nn * nn * 4LL);
   L.off_ctl = o;   o = align256(o + CTL_WORDS * 4LL);
-  L.off_pairs = o; o = align256(o + (long long)L.pcap * 8LL);
+  L.off_pairs = o; o = align256(o + (long long)L.pcap * 12LL);
   L.off_list = o;  o = align256(o + (long long)L.lcap * 4LL);
   L.off_tmp = o;   o = align256(o + (2LL * maxs + 8) * 4LL);
-  L.off_ameta = o; o = align256(o + (CATN_NCLS + 4) * 8LL);
+  L.off_ameta = o; o = align256(o + 64 * 8LL);   // work and cycle counters
   L.off_ldc = o;   o = align256(o + nn * 16LL);   // per-node logdim cache: value + valid flag
   L.off_arena = o;
   L.arena_bytes = arena_bytes;

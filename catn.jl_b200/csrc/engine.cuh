@@ -20,7 +20,7 @@
 //   compress!/compress_opt! ... mps_node.jl:356-447         -> compress_node
 //   eat! ...................... mps_node.jl:463-575         -> eat
 //   merge! .................... mps_node.jl:595-622         -> merge_dup
-//   dim_after_merge/count_*/select_* tensor_network.jl:152-316
+//   dim_after_merge/count_*/select_* tensor_network.jl:152-316 -> pair_cost, count_*_team, select_team
 //   cut_bondim_opt! ........... tensor_network.jl:399-477   -> cut_bond
 //   contraction! .............. tensor_network.jl:556-717   -> contract
 #pragma once
@@ -39,12 +39,10 @@ struct Ctx {
   int* nbr;
   EdgeEnt* ent;
   int ecap;
-  int* bhead;
-  int* btail;
-  int* bcnt;
+  int* fstack;   // free stack of entry ids (CTL_FTOP entries)
   int* emap;
   int* ctl;
-  int* pairs;   // 2 * pcap ints of scratch (pair lists)
+  int* pairs;   // 12 * pcap bytes of scratch (sort keys, reverse refs)
   int pcap;
   int* list;    // lcap ints: node-id lists for the bucket updates
   int* tmp;     // 2 * maxs + 8 ints: neighbour snapshot and duplicates
@@ -63,9 +61,10 @@ struct Ctx {
   double* sws;
   long long sws_doubles;
   double* acct;   // [flops, bytes] (global, leader-updated)
-  double* ldc;    // per-node logdim cache [n+1] (leader-maintained)
+  double* ldc;    // per-node logdim cache [n+1]
   long long* ldv; // cache validity [n+1]
   int status;     // uniform copy of the instance status
+  int multigraph; // the input lists some neighbour twice
   int* trace;
   int trace_cap;
 };
@@ -102,8 +101,9 @@ CATN_HD long long clk() {
   return 0;
 #endif
 }
-enum { PROF_TOTAL = 0, PROF_SVD_SMALL, PROF_SVD_LARGE, PROF_BOOK, PROF_COMPACT, PROF_N_SMALL, PROF_N_LARGE,
-       PROF_N_COMPACT };
+enum { PROF_TOTAL = 0, PROF_SVD_TINY, PROF_SVD_SMALL, PROF_SVD_LARGE, PROF_BOOK, PROF_N_TINY, PROF_N_SMALL,
+       PROF_N_LARGE, PROF_SWAP_GEMM, PROF_SWAP_EPI, PROF_CANO_EPI, PROF_EAT, PROF_MERGE, PROF_CUT, PROF_REVERSE,
+       PROF_CONTROL, PROF_SLOTS, PROF_COMPACT = PROF_SLOTS, PROF_N_COMPACT = PROF_SLOTS + 1 };
 CATN_HD void prof_add(Ctx& C, int slot, double v) {
   if (C.T.leader()) C.acct[2 + slot] += v;
 }
@@ -270,6 +270,12 @@ CATN_HDI inline SvdIn svd_begin(Ctx& C, long long m, long long n, double cutoff 
   s.wide = m < n;
   s.mm = s.wide ? n : m;
   s.nn = s.wide ? m : n;
+  if (s.mm * s.nn >= (1LL << 31)) {   // index arithmetic is 32-bit per operation
+    fail_all(C, CATN_ENOMEM);
+    s.smem = false;
+    s.W = nullptr;
+    return s;
+  }
   s.smem = svd_ws_doubles(s.mm, s.nn) <= C.sws_doubles;
   s.W = s.smem ? C.sws : spush(C, s.mm * s.nn);
   return s;
@@ -281,7 +287,8 @@ CATN_HD MOp svd_target(const SvdIn& s) {
 CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
   const Team& T = C.T;
   for (long long e = T.rank(); e < s.mm * s.nn; e += T.size()) {
-    long long r = e % s.mm, c = e / s.mm;
+    long long r, c;
+    divmod(e, s.mm, &r, &c);
     s.W[e] = s.wide ? A.ld(c, r) : A.ld(r, c);
   }
   T.sync();
@@ -310,13 +317,15 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
   double* Uw = spush(C, mm * r);
   if (failed(C)) return R;
   for (long long e = T.rank(); e < nn * r; e += T.size()) {
-    long long j = e % nn, i = e / nn;   // Tt[piv[j], i] = R[i, j]
+    long long j, i;   // Tt[piv[j], i] = R[i, j]
+    divmod(e, nn, &j, &i);
     Tt[(long long)piv[j] + nn * i] = (j >= i) ? s.W[i + j * mm] : 0.0;
   }
   T.sync();
   qrcp_inplace(T, Tt, nn, r, nn, tau2, piv2, nrm2, 0.0);
   for (long long e = T.rank(); e < r * r; e += T.size()) {
-    long long i = e % r, j = e / r;
+    long long i, j;
+    divmod(e, r, &i, &j);
     X2[e] = (j <= i) ? Tt[j + i * nn] : 0.0;
   }
   T.sync();
@@ -325,18 +334,21 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X2, r, r, r, sig2, S2, perm2);
   for (long long e = T.rank(); e < nn * r; e += T.size()) {
-    long long rr = e % nn, c = e / nn;
+    long long rr, c;
+    divmod(e, nn, &rr, &c);
     Uin[e] = (rr < r) ? Vb2[rr + (long long)perm2[c] * r] : 0.0;
   }
   for (long long e = T.rank(); e < r * r; e += T.size()) {
-    long long i = e % r, c = e / r;
+    long long i, c;
+    divmod(e, r, &i, &c);
     double sv = S2[c];
     Vin[(long long)piv2[i] + c * r] = (sv > 0.0) ? X2[i + (long long)perm2[c] * r] / sv : 0.0;
   }
   T.sync();
   qr_apply_q(T, Tt, nn, r, nn, tau2, Uin, r, nn);
   for (long long e = T.rank(); e < mm * r; e += T.size()) {
-    long long rr = e % mm, c = e / mm;
+    long long rr, c;
+    divmod(e, mm, &rr, &c);
     Uw[e] = (rr < r) ? Vin[rr + c * r] : 0.0;
   }
   T.sync();
@@ -388,6 +400,29 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     perm = nullptr;
     if (failed(C)) return R;
   }
+#if CATN_DEVICE_PASS
+  if (s.smem && nn <= 16 && mm <= 64) {
+    // tiny problem: one warp, warp-level synchronisation only
+    int sweeps = 0;
+    if (T.warp() == 0)
+      sweeps = nn <= 8 ? svd_warp_tiny<8>(s.W, (int)mm, (int)nn, tau, piv, Ut, Vt, Sout, 60)
+                       : svd_warp_tiny<16>(s.W, (int)mm, (int)nn, tau, piv, Ut, Vt, Sout, 60);
+    T.sync();
+    if (T.leader()) {
+      if (sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
+      C.ctl[CTL_BCAST] = sweeps;
+    }
+    T.sync();
+    if (C.ctl[CTL_BCAST] < 0) fail_all(C, CATN_ENOCONV);
+    T.sync();
+    prof_add(C, PROF_SVD_TINY, (double)(clk() - t0));
+    prof_add(C, PROF_N_TINY, 1.0);
+    R.p = nn;
+    R.S = Sout;
+    if (!s.wide) { R.U = Ut; R.V = Vt; } else { R.U = Vt; R.V = Ut; }
+    return R;
+  }
+#endif
   double stop = 0.0;
   if (!s.smem && s.tol > 0.0) {
     // truncate only when the matrix is far above the tolerance, so that the
@@ -411,7 +446,8 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     if (failed(C)) return R;
   }
   for (long long e = T.rank(); e < nn * nn; e += T.size()) {
-    long long i = e % nn, j = e / nn;
+    long long i, j;
+    divmod(e, nn, &i, &j);
     X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
   }
   T.sync();
@@ -420,11 +456,13 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X, nn, nn, nn, sig, Sout, perm);
   for (long long e = T.rank(); e < mm * nn; e += T.size()) {
-    long long r = e % mm, c = e / mm;
+    long long r, c;
+    divmod(e, mm, &r, &c);
     Ut[e] = (r < nn) ? Vb[r + (long long)perm[c] * nn] : 0.0;
   }
   for (long long e = T.rank(); e < nn * nn; e += T.size()) {
-    long long i = e % nn, c = e / nn;
+    long long i, c;
+    divmod(e, nn, &i, &c);
     double sv = Sout[c];
     Vt[(long long)piv[i] + c * nn] = (sv > 0.0) ? X[i + (long long)perm[c] * nn] / sv : 0.0;
   }
@@ -488,6 +526,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       svd_fill(C, in, colmajor(sdata(C, s), m));
       Svd R = svd_finish(C, in);
       if (failed(C)) return;
+      const long long te = clk();
       const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
       SiteRef nx = sref(C, k, i + 1);
       if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * nkeep * nx.d * nx.dr))) return;
@@ -507,6 +546,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       }
       T.sync();
       C.sp = mark;
+      prof_add(C, PROF_CANO_EPI, (double)(clk() - te));
     }
   } else {
     for (int i = h.cano; i > idx; --i) {
@@ -520,6 +560,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       svd_fill(C, in, transposed(sdata(C, s), dl));
       Svd R = svd_finish(C, in);
       if (failed(C)) return;
+      const long long te = clk();
       const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
       SiteRef pv = sref(C, k, i - 1);
       if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * pv.dl * pv.d * nkeep))) return;
@@ -540,6 +581,7 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       }
       T.sync();
       C.sp = mark;
+      prof_add(C, PROF_CANO_EPI, (double)(clk() - te));
     }
   }
 }
@@ -573,12 +615,15 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
   // straight into the SVD's oriented input.
   {
+    const long long tg = clk();
     MOp out = in.wide ? mop(in.W, imap((int)d0, n, 1), imap((int)d1, n * d0, d2))
                       : mop(in.W, imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2));
     gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
+    prof_add(C, PROF_SWAP_GEMM, (double)(clk() - tg));
   }
   Svd R = svd_finish(C, in);
   if (failed(C)) return 0.0;
+  const long long te = clk();
   double err = 0.0;
   int myd;
   if (rsvd_route) {
@@ -611,6 +656,7 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   }
   T.sync();
   C.sp = mark;
+  prof_add(C, PROF_SWAP_EPI, (double)(clk() - te));
   return err;
 }
 
@@ -647,6 +693,7 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
   const Team& T = C.T;
   NodeHdr h = C.node[k];
   if (h.nsites <= 1) return;
+  const long long tr0 = clk();
   const int ns = h.nsites;
   long long total = 0;
   for (int p = 1; p <= ns; ++p) total += al256(sbytes(sref(C, k, p)));
@@ -664,7 +711,9 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
     double* dst = dptr(C, cur);
     const long long dl = s.dl, d = s.d, dr = s.dr, tot = dl * d * dr;
     for (long long e = T.rank(); e < tot; e += T.size()) {
-      long long a = e % dl, rest = e / dl, b = rest % d, c = rest / d;
+      long long a, rest, b, c;
+      divmod(e, dl, &a, &rest);
+      divmod(rest, d, &b, &c);
       dst[c + dr * (b + d * a)] = src[e];
     }
     cur += al256(8 * tot);
@@ -690,6 +739,7 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
     C.node[k].cano = ns + 1 - h.cano;
   }
   T.sync();
+  prof_add(C, PROF_REVERSE, (double)(clk() - tr0));
 }
 
 // clear! (mps_node.jl:335-339)
@@ -736,6 +786,7 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
   T.sync();
   cano_to(C, k, idx1);
   if (failed(C)) return err;
+  const long long tf = clk();
   SiteRef a = sref(C, k, idx1), b = sref(C, k, idx1 + 1);
   const long long rows = (long long)a.dl * a.d, cols = (long long)b.d * b.dr;
   if (!heap_reserve(C, al256(8 * rows * cols))) return err;
@@ -749,6 +800,7 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
     site_delete_at_leader(C, k, idx1 + 1);
   }
   T.sync();
+  prof_add(C, PROF_MERGE, (double)(clk() - tf));
   cano_to(C, k, idx1);
   return err;
 }
@@ -816,6 +868,7 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   // (c) general
   *err += move2head(C, kj, idxi);
   if (failed(C)) return 0.0;
+  const long long tf = clk();
   SiteRef last = sref(C, ki, hi.nsites);   // (Dl, dd, 1)
   SiteRef hj = sref(C, kj, 1);              // (1, dd, Dr)
   const long long Dl = last.dl, dd = last.d, Dr = hj.dr;
@@ -850,6 +903,7 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   }
   refresh_status(C);
   C.sp = mark;
+  prof_add(C, PROF_EAT, (double)(clk() - tf));
   if (failed(C)) return 0.0;
   cano_to(C, ki, C.node[ki].nsites);
   if (failed(C)) return 0.0;
@@ -890,7 +944,8 @@ CATN_HDI inline QRed qr_reduce(Ctx& C, double* X, long long rows, long long cols
   if (failed(C)) return q;
   qr_inplace(T, X, rows, cols, rows, q.tau);
   for (long long e = T.rank(); e < cols * cols; e += T.size()) {
-    long long r = e % cols, c = e / cols;
+    long long r, c;
+    divmod(e, cols, &r, &c);
     q.Rb[e] = (r <= c) ? X[r + c * rows] : 0.0;
   }
   T.sync();
@@ -900,7 +955,8 @@ CATN_HDI inline QRed qr_reduce(Ctx& C, double* X, long long rows, long long cols
 CATN_HDI inline void qr_expand(Ctx& C, const QRed& q, const double* Y, long long ncols, double* out) {
   const Team& T = C.T;
   for (long long e = T.rank(); e < q.rows * ncols; e += T.size()) {
-    long long r = e % q.rows, c = e / q.rows;
+    long long r, c;
+    divmod(e, q.rows, &r, &c);
     out[e] = (r < q.rrows) ? Y[r + c * q.rrows] : 0.0;
   }
   T.sync();
@@ -1000,6 +1056,7 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   cano_to(C, i, idx_j_in_i);
   cano_to(C, j, idx_i_in_j);
   if (failed(C)) return 0.0;
+  const long long tcut = clk();
   const long long mark = C.sp;
   SiteRef Ai = sref(C, i, idx_j_in_i), Aj = sref(C, j, idx_i_in_j);
   const long long d = Ai.d;
@@ -1048,13 +1105,17 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
     double* O = dptr(C, ni);
     const long long dl = Ai.dl, dr = Ai.dr, tot = dl * myd * dr;
     for (long long e = T.rank(); e < tot; e += T.size()) {
-      long long a = e % dl, rest = e / dl, r = rest % myd, c = rest / myd;
+      long long a, rest, r, c;
+      divmod(e, dl, &a, &rest);
+      divmod(rest, myd, &r, &c);
       O[e] = fi[(a + dl * c) + ri_rows * r];
     }
     double* P2 = dptr(C, nj);
     const long long dl2 = Aj.dl, dr2 = Aj.dr, tot2 = dl2 * myd * dr2;
     for (long long e = T.rank(); e < tot2; e += T.size()) {
-      long long a = e % dl2, rest = e / dl2, r = rest % myd, c = rest / myd;
+      long long a, rest, r, c;
+      divmod(e, dl2, &a, &rest);
+      divmod(rest, myd, &r, &c);
       P2[e] = fj[(a + dl2 * c) + rj_rows * r];
     }
     T.sync();
@@ -1068,6 +1129,7 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   }
   T.sync();
   C.sp = mark;
+  prof_add(C, PROF_CUT, (double)(clk() - tcut));
   return disc + extra;
 }
 
@@ -1121,179 +1183,229 @@ CATN_HDI inline void raw2mps(Ctx& C, int k, const double* data, const long long*
 }
 
 // ---------------------------------------------------------------------------
-// edge-cost buckets (tensor_network.jl:152-236), leader-only helpers
+// Edge-cost bookkeeping (tensor_network.jl:152-316) as an entry pool.  An
+// alive entry (cost, i, j, seq) stands for pair [i, j] in bucket `cost` of the
+// reference's edge_count; `seq` is its insertion rank, so bucket order is
+// ascending seq and "first pair of the cheapest bucket" is the alive entry of
+// least cost with the least seq.  Removal, insertion and selection are
+// team-parallel.
 // ---------------------------------------------------------------------------
-// logdim of node k through the leader's cache.  Entries are invalidated for
-// every node whose sites a contraction step may touch, so the value is always
-// the reference's left fold over the current sites.
-CATN_HD double logdim_cached(Ctx& C, int k) {
-  if (C.ldv[k]) return C.ldc[k];
-  double v = logdim_all(C, k);
-  C.ldc[k] = v;
-  C.ldv[k] = 1;
-  return v;
-}
-CATN_HD int dim_after_merge(Ctx& C, int i, int j) {
-  int idx = nb_find(C, i, j);
-  double v = logdim_cached(C, i) + logdim_cached(C, j) - 2.0 * logdim_at(C, i, idx);
-  return (int)rint(v);
-}
 CATN_HD int& emap_at(const Ctx& C, int i, int j) { return C.emap[(long long)i * (C.n + 1) + j]; }
 
-CATN_HD void bucket_add_leader(Ctx& C, int cost, int i, int j) {
-  if (cost < 0 || cost >= CATN_CMAX) { fail_leader(C, CATN_ENOMEM); return; }
-  int e = C.ctl[CTL_FREEENT];
-  if (e < 0) { fail_leader(C, CATN_ENOMEM); return; }
-  C.ctl[CTL_FREEENT] = C.ent[e].next;
-  EdgeEnt& E = C.ent[e];
-  E.cost = cost; E.i = i; E.j = j; E.alive = 1; E.next = -1; E.prev = C.btail[cost];
-  E.seq = C.ctl[CTL_SEQ]++;
-  if (C.btail[cost] >= 0) C.ent[C.btail[cost]].next = e;
-  else C.bhead[cost] = e;
-  C.btail[cost] = e;
-  C.bcnt[cost] += 1;
-  if (cost < C.ctl[CTL_MINC]) C.ctl[CTL_MINC] = cost;
-  int& m = emap_at(C, i, j);
-  if (m >= 0 && C.ent[m].alive) C.ctl[CTL_ANOMALY] += 1;
-  m = e;
+// Fill the logdim cache (left fold of log2 phys dims, mps_node.jl:299-311) for
+// `list` nodes and all their neighbours, in a phase of its own so that cost
+// readers never race cache writers.
+CATN_HDI inline void logdim_prefetch(Ctx& C, const int* list, int nl) {
+  const Team& T = C.T;
+  for (int a = T.warp(); a < nl; a += T.nwarps()) {
+    const int x = list[a];
+    if (x <= 0) continue;
+    const int nn = C.node[x].nnbr;
+    for (int p = T.lane(); p <= nn; p += T.wsize()) {
+      const int y = (p == 0) ? x : nbref(C, x, p);
+      if (y <= 0 || C.ldv[y]) continue;
+      C.ldc[y] = logdim_all(C, y);
+    }
+  }
+  T.sync();
+  for (int a = T.warp(); a < nl; a += T.nwarps()) {
+    const int x = list[a];
+    if (x <= 0) continue;
+    const int nn = C.node[x].nnbr;
+    for (int p = T.lane(); p <= nn; p += T.wsize()) {
+      const int y = (p == 0) ? x : nbref(C, x, p);
+      if (y > 0) C.ldv[y] = 1;
+    }
+  }
+  T.sync();
 }
-CATN_HD void bucket_unlink_leader(Ctx& C, int e) {
-  EdgeEnt& E = C.ent[e];
-  if (E.prev >= 0) C.ent[E.prev].next = E.next; else C.bhead[E.cost] = E.next;
-  if (E.next >= 0) C.ent[E.next].prev = E.prev; else C.btail[E.cost] = E.prev;
-  C.bcnt[E.cost] -= 1;
-  E.alive = 0;
-  E.next = C.ctl[CTL_FREEENT];
-  C.ctl[CTL_FREEENT] = e;
+
+// dim_after_merge (tensor_network.jl:152-155) with the shared bond's phys dim
+// d already known (a bond has the same phys dim at both ends):
+// round(logdim(i) + logdim(j) - 2 log2(d)), ties to even.
+CATN_HD int pair_cost(const Ctx& C, int i, int j, int d) {
+  const double v = C.ldc[i] + C.ldc[j] - 2.0 * log2((double)d);
+  return (int)rint(v);
 }
-// filter!(pair -> pair != [i,j], edge_count[cost])
-CATN_HD void bucket_remove_leader(Ctx& C, int cost, int i, int j) {
-  if (cost < 0 || cost >= CATN_CMAX) return;
-  int& m = emap_at(C, i, j);
-  if (m >= 0 && C.ent[m].alive && C.ent[m].cost == cost && C.ent[m].i == i && C.ent[m].j == j) {
-    bucket_unlink_leader(C, m);
-    m = -1;
+
+// count_remove_nodes! (:213-225): every bond of every node in `list` leaves
+// the bucket of its current cost.
+CATN_HDI inline void count_remove_nodes_team(Ctx& C, const int* list, int nl) {
+  const Team& T = C.T;
+  logdim_prefetch(C, list, nl);
+  int* ftop = C.ctl + CTL_FTOP;
+  for (int a = T.warp(); a < nl; a += T.nwarps()) {
+    const int x = list[a];
+    if (x <= 0) continue;
+    const int nn = C.node[x].nnbr;
+    for (int p = 1 + T.lane(); p <= nn; p += T.wsize()) {
+      const int y = nbref(C, x, p);
+      if (y <= 0) continue;
+      const int i = x < y ? x : y, j = x < y ? y : x;
+      const int cost = pair_cost(C, i, j, sref(C, x, p).d);
+      int& m = emap_at(C, i, j);
+      const int e = m;
+      if (e < 0) continue;
+      EdgeEnt& E = C.ent[e];
+      if (E.cost != cost || E.i != i || E.j != j) continue;
+      if (T.atomic_cas(&E.alive, 1, 0) == 1) {   // exactly one remover per entry
+        m = -1;
+        C.fstack[T.atomic_add(ftop, 1)] = e;
+      }
+    }
+  }
+  T.sync();
+}
+
+// Bitonic sort of `pow2` 64-bit keys with one int payload, in place.
+CATN_HDI inline void bitonic_sort(const Team& T, long long* key, int* val, int pow2) {
+  for (int k = 2; k <= pow2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = T.rank(); t < pow2; t += T.size()) {
+        const int u = t ^ j;
+        if (u > t) {
+          const bool up = (t & k) == 0;
+          if ((key[t] > key[u]) == up) {
+            const long long kk = key[t]; key[t] = key[u]; key[u] = kk;
+            const int vv = val[t]; val[t] = val[u]; val[u] = vv;
+          }
+        }
+      }
+      T.sync();
+    }
+  }
+}
+
+// count_add_nodes! (:185-197): the bonds of `list` nodes, deduplicated and
+// inserted in lexicographic order of (i, j) -- the reference's
+// sort(collect(Set(...))).
+CATN_HDI inline void count_add_nodes_team(Ctx& C, const int* list, int nl) {
+  const Team& T = C.T;
+  const long long EMPTY = 0x7fffffffffffffffLL;
+  logdim_prefetch(C, list, nl);
+  int local = 0;
+  for (int a = T.rank(); a < nl; a += T.size())
+    if (list[a] > 0) local += C.node[list[a]].nnbr;
+  const int npairs = (int)(T.sum((double)local) + 0.5);
+  int pow2 = 1;
+  while (pow2 < npairs) pow2 <<= 1;
+  // sort workspace: shared memory when it fits, else the slot's pair scratch
+  long long* key;
+  int* val;
+  if ((long long)pow2 * 12 <= C.sws_doubles * 8) {
+    key = (long long*)C.sws;
+  } else if ((long long)pow2 <= (long long)C.pcap) {
+    key = (long long*)C.pairs;
+  } else {
+    fail_all(C, CATN_ENOMEM);
     return;
   }
-  // Slow path: entries not reachable through the pair map.
-  if (C.bcnt[cost] == 0) return;
-  int e = C.bhead[cost];
-  for (int guard = 0; e >= 0 && guard <= C.ecap; ++guard) {
-    int nx = C.ent[e].next;
-    if (C.ent[e].i == i && C.ent[e].j == j) {
-      bucket_unlink_leader(C, e);
-      if (m == e) m = -1;
-    }
-    e = nx;
-  }
-}
-
-// Sort pairs (lexicographic) in scratch, dedupe; returns count.
-CATN_HD int sort_pairs_leader(int* pr, int np) {
-  // shell sort on packed 64-bit keys
-  for (int gap = np / 2; gap > 0; gap /= 2) {
-    for (int a = gap; a < np; ++a) {
-      int ti = pr[2 * a], tj = pr[2 * a + 1];
-      int b = a;
-      while (b >= gap && (pr[2 * (b - gap)] > ti || (pr[2 * (b - gap)] == ti && pr[2 * (b - gap) + 1] > tj))) {
-        pr[2 * b] = pr[2 * (b - gap)];
-        pr[2 * b + 1] = pr[2 * (b - gap) + 1];
-        b -= gap;
+  val = (int*)(key + pow2);
+  int* cnt = C.ctl + CTL_SPARE;
+  T.sync();
+  if (T.leader()) *cnt = 0;
+  T.sync();
+  for (int a = T.warp(); a < nl; a += T.nwarps()) {
+    const int x = list[a];
+    if (x <= 0) continue;
+    const int nn = C.node[x].nnbr;
+    for (int p = 1 + T.lane(); p <= nn; p += T.wsize()) {
+      const int y = nbref(C, x, p);
+      const int slot = T.atomic_add(cnt, 1);
+      if (y <= 0) {
+        key[slot] = EMPTY;   // open leg: sorts to the end, dropped below
+        val[slot] = 0;
+        continue;
       }
-      pr[2 * b] = ti;
-      pr[2 * b + 1] = tj;
+      const int i = x < y ? x : y, j = x < y ? y : x;
+      key[slot] = ((long long)i << 32) | (long long)j;
+      val[slot] = sref(C, x, p).d;
     }
   }
-  int w = 0;
-  for (int a = 0; a < np; ++a) {
-    if (w > 0 && pr[2 * (w - 1)] == pr[2 * a] && pr[2 * (w - 1) + 1] == pr[2 * a + 1]) continue;
-    pr[2 * w] = pr[2 * a];
-    pr[2 * w + 1] = pr[2 * a + 1];
-    ++w;
+  T.sync();
+  for (int t = npairs + T.rank(); t < pow2; t += T.size()) {
+    key[t] = EMPTY;
+    val[t] = 0;
   }
-  return w;
-}
-
-// count_add_nodes! (:185-197) over `list` (node ids, <=0 skipped).
-CATN_HD void count_add_nodes_leader(Ctx& C, const int* list, int nl) {
-  int* pr = C.pairs;
-  int np = 0;
-  for (int a = 0; a < nl; ++a) {
-    int i = list[a];
-    if (i <= 0) continue;
-    int nn = C.node[i].nnbr;
-    for (int p = 1; p <= nn; ++p) {
-      int j = nbref(C, i, p);
-      if (j <= 0) continue;
-      if (np >= C.pcap) { fail_leader(C, CATN_ENOMEM); return; }
-      pr[2 * np] = i < j ? i : j;
-      pr[2 * np + 1] = i < j ? j : i;
-      ++np;
+  T.sync();
+  bitonic_sort(T, key, val, pow2);
+  // unique real pairs get consecutive ranks in sorted order
+  int* ftop = C.ctl + CTL_FTOP;
+  const int top0 = *ftop;
+  const int seq0 = C.ctl[CTL_SEQ];
+  int base_rank = 0;
+  for (int t0 = 0; t0 < pow2; t0 += T.size()) {
+    const int t = t0 + T.rank();
+    int flag = 0;
+    if (t < pow2 && key[t] != EMPTY && (t == 0 || key[t] != key[t - 1])) flag = 1;
+    int tot = 0;
+    const int r = base_rank + T.scan_excl(flag, &tot);
+    if (flag) {
+      if (r >= top0) {
+        fail_all(C, CATN_ENOMEM);
+      } else {
+        const int i = (int)(key[t] >> 32), j = (int)(key[t] & 0xffffffff);
+        const int e = C.fstack[top0 - 1 - r];
+        EdgeEnt& E = C.ent[e];
+        E.cost = pair_cost(C, i, j, val[t]);
+        E.i = i;
+        E.j = j;
+        E.seq = seq0 + r;
+        E.alive = 1;
+        int& m = emap_at(C, i, j);
+        if (m >= 0 && C.ent[m].alive) T.atomic_add(C.ctl + CTL_ANOMALY, 1);
+        m = e;
+      }
     }
+    base_rank += tot;
   }
-  np = sort_pairs_leader(pr, np);
-  for (int a = 0; a < np; ++a) {
-    int i = pr[2 * a], j = pr[2 * a + 1];
-    bucket_add_leader(C, dim_after_merge(C, i, j), i, j);
+  T.sync();
+  if (T.leader()) {
+    const int used = base_rank < top0 ? base_rank : top0;
+    *ftop = top0 - used;
+    C.ctl[CTL_SEQ] = seq0 + used;
+    if (base_rank > top0) fail_leader(C, CATN_ENOMEM);
   }
-}
-// count_remove_nodes! (:213-225)
-CATN_HD void count_remove_nodes_leader(Ctx& C, const int* list, int nl) {
-  for (int a = 0; a < nl; ++a) {
-    int id = list[a];
-    if (id <= 0) continue;
-    int nn = C.node[id].nnbr;
-    for (int p = 1; p <= nn; ++p) {
-      int nb = nbref(C, id, p);
-      if (nb <= 0) continue;
-      int i = id < nb ? id : nb, j = id < nb ? nb : id;
-      bucket_remove_leader(C, dim_after_merge(C, i, j), i, j);
-    }
-  }
-}
-
-CATN_HD int min_cost_leader(Ctx& C) {
-  int c = C.ctl[CTL_MINC];
-  if (c < 0) c = 0;
-  while (c < CATN_CMAX && C.bcnt[c] == 0) ++c;
-  C.ctl[CTL_MINC] = c;
-  return c;
+  refresh_status(C);
 }
 
 // select_edge_min_dim (:248-253) / _triangle (:262-288) / _sequentially
-// (:300-316), as team reductions.  Bucket order is insertion order, so the
-// triangle selector's "first candidate with the largest count" is the entry
-// with the largest count and, among those, the smallest insertion sequence.
+// (:300-316), as team reductions over the entry pool / the nodes.
 CATN_HDI inline long long select_team(Ctx& C, int* maxdim) {
   const Team& T = C.T;
   const int sel = C.P.select;
   if (sel == 0 || sel == 1) {
-    long long cost = 0;
-    T.sync();
-    if (T.leader()) cost = min_cost_leader(C);
-    cost = T.bcast(cost);
-    if (cost >= CATN_CMAX) { fail_all(C, CATN_ESTATE); return 0; }
-    if (cost > *maxdim) *maxdim = (int)cost;
-    if (sel == 0) {
-      const int e = C.bhead[cost];
-      return ((long long)C.ent[e].i << 32) | (unsigned)C.ent[e].j;
-    }
+    // cheapest non-empty bucket
+    double mc = 1e300;
+    for (int e = T.rank(); e < C.ecap; e += T.size())
+      if (C.ent[e].alive && C.ent[e].cost < mc) mc = C.ent[e].cost;
+    mc = -T.maxv(-mc);
+    if (mc > 1e299) { fail_all(C, CATN_ESTATE); return 0; }
+    const int cost = (int)mc;
+    if (cost > *maxdim) *maxdim = cost;
     double bv = -1.0;
     long long be = -1;
     for (int e = T.rank(); e < C.ecap; e += T.size()) {
       const EdgeEnt E = C.ent[e];
       if (!E.alive || E.cost != cost) continue;
-      const int i = E.i, j = E.j, nn = C.node[j].nnbr;
       int both = 0;
-      for (int p = 1; p <= nn; ++p) {
-        const int k = nbref(C, j, p);
-        if (k <= 0 || k == i) continue;
-        bool dup = false;
-        for (int q = 1; q < p; ++q)
-          if (nbref(C, j, q) == k) { dup = true; break; }
-        if (dup) continue;
-        if (nb_find(C, k, i) > 0) ++both;
+      if (sel == 1) {
+        const int i = E.i, j = E.j, nn = C.node[j].nnbr;
+        for (int p = 1; p <= nn; ++p) {
+          const int k = nbref(C, j, p);
+          if (k <= 0 || k == i) continue;
+          // Set semantics: a repeated neighbour counts once.  Every step merges
+          // the duplicates it creates, so lists repeat only when the input does.
+          if (C.multigraph) {
+            bool dup = false;
+            for (int q = 1; q < p; ++q)
+              if (nbref(C, j, q) == k) { dup = true; break; }
+            if (dup) continue;
+          }
+          if (nb_find(C, k, i) > 0) ++both;
+        }
       }
+      // largest count first, then earliest insertion
       const double key = (double)both * 2147483648.0 + (double)(0x7fffffff - E.seq);
       if (be < 0 || key > bv) { bv = key; be = e; }
     }
@@ -1313,7 +1425,6 @@ CATN_HDI inline long long select_team(Ctx& C, int* maxdim) {
       if (bi < 0 || key > bv) { bv = key; bi = ((long long)i << 32) | (unsigned)nb; }
     }
   }
-  // argmax breaks ties on the packed pair; keys are distinct per (sum, i)
   const long long best = T.argmax(bv, bi);
   if (best < 0) { fail_all(C, CATN_ESTATE); return 0; }
   return best;
@@ -1346,19 +1457,20 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
   O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
   const bool buckets = (C.P.select == 0 || C.P.select == 1);
   if (buckets) {
+    // select_edge_init!: all node ids
+    for (int k = 1 + T.rank(); k <= C.n; k += T.size()) C.list[k - 1] = k;
     T.sync();
-    if (T.leader()) {
-      // select_edge_init!: all node ids
-      for (int k = 1; k <= C.n; ++k) C.list[k - 1] = k;
-      count_add_nodes_leader(C, C.list, C.n);
-    }
-    refresh_status(C);
+    count_add_nodes_team(C, C.list, C.n);
   }
   int maxdim = -1;
   // Every step clears one node, so a network of n nodes needs fewer than n
   // steps; the cap only guards against corrupted state.
   const int step_cap = C.n + 16;
-  while (!failed(C) && has_real_edges(C)) {
+  for (;;) {
+    const long long tc0 = clk();
+    const bool more = !failed(C) && has_real_edges(C);
+    prof_add(C, PROF_CONTROL, (double)(clk() - tc0));
+    if (!more) break;
     if (O.nsteps > step_cap) {
       fail_all(C, CATN_ESTATE);
       break;
@@ -1371,20 +1483,22 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
     if (C.node[j].nsites > C.node[i].nsites) { int t = i; i = j; j = t; }
     // --- bookkeeping before any shape change ---
     if (buckets) {
+      int* list = C.list;
+      const int nl = 2 + C.node[i].nnbr + C.node[j].nnbr;
       T.sync();
       if (T.leader()) {
-        int* list = C.list;
-        int nl = 0;
-        list[nl++] = i;
-        list[nl++] = j;
-        for (int p = 1; p <= C.node[i].nnbr; ++p) list[nl++] = nbref(C, i, p);
-        for (int p = 1; p <= C.node[j].nnbr; ++p) list[nl++] = nbref(C, j, p);
-        count_remove_nodes_leader(C, list, nl);
-        // every node whose sites this step may change: i, j and their neighbours
-        for (int q = 0; q < nl; ++q)
-          if (list[q] > 0) C.ldv[list[q]] = 0;
+        int q = 0;
+        list[q++] = i;
+        list[q++] = j;
+        for (int p = 1; p <= C.node[i].nnbr; ++p) list[q++] = nbref(C, i, p);
+        for (int p = 1; p <= C.node[j].nnbr; ++p) list[q++] = nbref(C, j, p);
       }
-      refresh_status(C);
+      T.sync();
+      count_remove_nodes_team(C, list, nl);
+      // every node whose sites this step may change: i, j and their neighbours
+      for (int q = T.rank(); q < nl; q += T.size())
+        if (list[q] > 0) C.ldv[list[q]] = 0;
+      T.sync();
     }
     prof_add(C, PROF_BOOK, (double)(clk() - tb0));
     int idx_j_in_i = nb_find(C, i, j);
@@ -1459,15 +1573,15 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
     if (failed(C)) break;
     if (buckets) {
       const long long tb1 = clk();
+      int* list = C.list;
+      const int nl = 1 + C.node[i].nnbr;
       T.sync();
       if (T.leader()) {
-        int* list = C.list;
-        int nl = 0;
-        list[nl++] = i;
-        for (int p = 1; p <= C.node[i].nnbr; ++p) list[nl++] = nbref(C, i, p);
-        count_add_nodes_leader(C, list, nl);
+        list[0] = i;
+        for (int p = 1; p <= C.node[i].nnbr; ++p) list[p] = nbref(C, i, p);
       }
-      refresh_status(C);
+      T.sync();
+      count_add_nodes_team(C, list, nl);
       prof_add(C, PROF_BOOK, (double)(clk() - tb1));
     }
     const int nsi = C.node[i].nsites;
@@ -1531,9 +1645,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.nbr = (int*)(slot + L.off_nbr);
   C.ent = (EdgeEnt*)(slot + L.off_ent);
   C.ecap = L.ecap;
-  C.bhead = (int*)(slot + L.off_bhead);
-  C.btail = (int*)(slot + L.off_btail);
-  C.bcnt = (int*)(slot + L.off_bcnt);
+  C.fstack = (int*)(slot + L.off_fstack);
   C.emap = (int*)(slot + L.off_emap);
   C.ctl = (int*)(slot + L.off_ctl);
   C.pairs = (int*)(slot + L.off_pairs);
@@ -1562,6 +1674,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.sws = sws;
   C.sws_doubles = sws_doubles;
   C.status = 0;
+  C.multigraph = 1;
   C.trace = nullptr;
   C.trace_cap = 0;
   return C;
@@ -1571,10 +1684,9 @@ CATN_HDI inline void reset_slot(Ctx& C) {
   const Team& T = C.T;
   const long long nn = (long long)C.n + 1;
   for (long long e = T.rank(); e < nn * nn; e += T.size()) C.emap[e] = -1;
-  for (long long e = T.rank(); e < CATN_CMAX; e += T.size()) { C.bhead[e] = -1; C.btail[e] = -1; C.bcnt[e] = 0; }
   for (long long e = T.rank(); e < C.ecap; e += T.size()) {
     C.ent[e].alive = 0;
-    C.ent[e].next = (e + 1 < C.ecap) ? (int)(e + 1) : -1;
+    C.fstack[e] = (int)(C.ecap - 1 - e);   // pops hand out 0, 1, 2, ...
   }
   for (long long e = T.rank(); e < nn; e += T.size()) {
     C.node[e].nsites = 0; C.node[e].nnbr = 0; C.node[e].cano = 0; C.node[e].pad = 0;
@@ -1583,9 +1695,8 @@ CATN_HDI inline void reset_slot(Ctx& C) {
   for (long long e = T.rank(); e < CTL_WORDS; e += T.size()) C.ctl[e] = 0;
   T.sync();
   if (T.leader()) {
-    C.ctl[CTL_FREEENT] = C.ecap > 0 ? 0 : -1;
-    C.ctl[CTL_MINC] = 0;
-    for (int q = 0; q < 10; ++q) C.acct[q] = 0.0;
+    C.ctl[CTL_FTOP] = C.ecap;
+    for (int q = 0; q < 2 + PROF_SLOTS + 2; ++q) C.acct[q] = 0.0;
   }
   T.sync();
 }
@@ -1665,6 +1776,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
                                   const long long* i64, const int* i32, const double* dat,
                                   catn_result* res, int* trace_base, double* sws, long long sws_doubles) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
+  C.multigraph = D.multigraph;
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {
     C.trace = trace_base + D.trace_off;
@@ -1689,7 +1801,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     res->arena_peak = C.sp_peak + 2 * C.h_peak;
     res->flops = C.acct[0];
     res->bytes = C.acct[1];
-    for (int q = 0; q < 8; ++q) res->prof[q] = C.acct[2 + q];
+    for (int q = 0; q < PROF_SLOTS; ++q) res->prof[q] = C.acct[2 + q];
   }
   T.sync();
 }

@@ -4,6 +4,7 @@
 #pragma once
 #include <cmath>
 #include <cstring>
+#include <set>
 #include <string>
 #include <vector>
 #include "catn_layout.h"
@@ -64,8 +65,22 @@ struct Image {
     D.data_off = (long long)dat.size();
     D.data_len = ndata;
     dat.insert(dat.end(), site_data, site_data + ndata);
+    D.multigraph = has_repeats(n, nbr_counts, neighbors);
     finish(D, n, edges2 / 2 + 1, trace_cap);
     return "";
+  }
+
+  // Does any node list the same neighbour twice?
+  static int has_repeats(int n, const int* counts, const int* neighbors) {
+    long long pos = 0;
+    for (int k = 0; k < n; ++k) {
+      std::set<int> seen;
+      for (int q = 0; q < counts[k]; ++q, ++pos) {
+        int v = neighbors[pos];
+        if (v > 0 && !seen.insert(v).second) return 1;
+      }
+    }
+    return 0;
   }
 
   // Network of dense tensors; raw2mps runs on the device.
@@ -110,6 +125,7 @@ struct Image {
     D.data_off = (long long)dat.size();
     D.data_len = ndata;
     dat.insert(dat.end(), data, data + ndata);
+    D.multigraph = has_repeats(n, ndims, neighbors);
     finish(D, n, edges2 / 2 + 1, trace_cap);
     return "";
   }

@@ -18,15 +18,23 @@
 namespace catn {
 
 // Two-level index map: x -> (x % n1) * s1 + (x / n1) * s2.
+// Element counts of one operation stay below 2^31, so index splits use
+// 32-bit unsigned division (far cheaper than 64-bit on the GPU).
 struct IMap {
   int n1;
   long long s1, s2;
   CATN_HD long long at(long long x) const {
     if (n1 == 1) return x * s2;
-    long long q = x / n1;
-    return (x - q * n1) * s1 + q * s2;
+    const unsigned q = (unsigned)x / (unsigned)n1;
+    return ((long long)((unsigned)x - q * (unsigned)n1)) * s1 + (long long)q * s2;
   }
 };
+// (x % n, x / n) for 0 <= x < 2^31, n > 0.
+CATN_HD void divmod(long long x, long long n, long long* r, long long* q) {
+  const unsigned qq = (unsigned)x / (unsigned)n;
+  *q = qq;
+  *r = (long long)((unsigned)x - qq * (unsigned)n);
+}
 CATN_HD IMap imap(int n1, long long s1, long long s2) { IMap m; m.n1 = n1; m.s1 = s1; m.s2 = s2; return m; }
 // Plain column-major index: row r -> r, col c -> c*ld.
 CATN_HD IMap rows_plain() { return imap(1, 0, 1); }
@@ -120,7 +128,8 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
 #endif
   // Small problems (and the host build): one output element per thread.
   for (long long e = T.rank(); e < M * N; e += T.size()) {
-    long long r = e % M, c = e / M;
+    long long r, c;
+    divmod(e, M, &r, &c);
     double s = 0.0;
     for (long long k = 0; k < K; ++k) s = fma(A.ld(r, k), B.ld(k, c), s);
     C.ref(r, c) = s;
@@ -147,7 +156,8 @@ CATN_HDI inline void scale(const Team& T, double* dst, double v, long long n) {
 CATN_HDI inline void materialize(const Team& T, double* dst, long long rows, long long cols,
                                  long long ldd, const MOp& op) {
   for (long long e = T.rank(); e < rows * cols; e += T.size()) {
-    long long r = e % rows, c = e / rows;
+    long long r, c;
+    divmod(e, rows, &r, &c);
     dst[r + c * ldd] = op.ld(r, c);
   }
   T.sync();
@@ -319,11 +329,46 @@ CATN_HDI inline void qr_apply_q(const Team& T, const double* A, long long m, lon
 // (n x n, ld n).  Columns of B converge to U * diag(S).  Returns the number
 // of sweeps, or -1 when the sweep cap was reached.
 // ---------------------------------------------------------------------------
+// Jacobi rotation annihilating the off-diagonal g of the 2x2 Gram block
+// [[al, g], [g, be]] (Rutishauser's formula): returns false when the pair is
+// already orthogonal to tolerance (g^2 <= tol^2 al be) or a column is
+// numerically zero; otherwise c = cos, s = sin with
+// t = sign(d g) 2|g| / (|d| + sqrt(d^2 + 4 g^2)), d = be - al.
+CATN_HD bool jacobi_rotation(double al, double be, double g, double tol, double* c, double* s) {
+  if (al < 1e-250 || be < 1e-250) return false;
+  if (!(g * g > tol * tol * al * be)) return false;
+  const double d = be - al;
+  double t = (2.0 * fabs(g)) / (fabs(d) + sqrt(d * d + 4.0 * g * g));
+  if ((d < 0.0) != (g < 0.0)) t = -t;   // sign(d * g); d == 0 takes the sign of g
+  const double cc = 1.0 / sqrt(1.0 + t * t);
+  *c = cc;
+  *s = cc * t;
+  return true;
+}
+
+// Round-robin (circle method) schedule over np (even) players, player 0
+// fixed: in round r (0 <= r < np-1) position k holds player
+// ((k - 1 + r) mod (np - 1)) + 1 for k >= 1, and pair i joins the players at
+// positions i and np-1-i.  Division-free: r < np-1 and k < np.
+CATN_HD int rr_at(int np, int r, int k) {
+  if (k == 0) return 0;
+  int t = k - 1 + r;
+  if (t >= np - 1) t -= np - 1;
+  return t + 1;
+}
 CATN_HD void rr_pair(long long np, long long r, long long i, long long* a, long long* b) {
-  // circle method over np (even) players; player 0 fixed.
-  auto pos = [&](long long k) -> long long { return k == 0 ? 0 : ((k - 1 + r) % (np - 1)) + 1; };
-  *a = pos(i);
-  *b = pos(np - 1 - i);
+  *a = rr_at((int)np, (int)r, (int)i);
+  *b = rr_at((int)np, (int)r, (int)(np - 1 - i));
+}
+// Partner of player j in round r.
+CATN_HD int rr_partner(int np, int r, int j) {
+  int k = 0;   // position of player j
+  if (j != 0) {
+    k = j - 1 - r;
+    if (k < 0) k += np - 1;
+    k += 1;
+  }
+  return rr_at(np, r, np - 1 - k);
 }
 
 CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long long n, long long ldb,
@@ -363,14 +408,9 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
         al = T.wsum(al);
         be = T.wsum(be);
         ga = T.wsum(ga);
-        if (al < 1e-250 || be < 1e-250) continue;   // numerically zero column
-        if (!(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
+        double c, s;
+        if (!jacobi_rotation(al, be, ga, tol, &c, &s)) continue;
         rotated = 1;
-        double zeta = (be - al) / (2.0 * ga);
-        double t = fabs(zeta) > 1e150 ? 0.5 / zeta
-                                      : copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-        double c = 1.0 / sqrt(1.0 + t * t);
-        double s = c * t;
         T.wsync();
         for (long long i = T.lane(); i < m; i += T.wsize()) {
           double x = bp[i], y = bq[i];
@@ -424,5 +464,189 @@ CATN_HDI inline void sort_columns(const Team& T, const double* B, long long m, l
   }
   T.sync();
 }
+
+}  // namespace catn
+
+namespace catn {
+
+#if CATN_DEVICE_PASS
+// ---------------------------------------------------------------------------
+// Tiny SVD by one warp (nn <= NN <= 32, nn <= mm <= 64): the same method as
+// the team path -- pivoted Householder QR W P = Q R, one-sided Jacobi on
+// X = R^T, W = (Q V') Sigma (P U')^T -- with one lane per column, the Jacobi
+// columns held in registers and exchanged by shuffles, and warp-level
+// synchronisation only.  W (column-major, ld mm) is overwritten by the
+// Householder form; outputs: Ut (mm x nn) = Q V'[:, perm], Vt (nn x nn) =
+// P U'[:, perm], Sout (nn, descending).  Returns the sweep count (-1 when the
+// cap was reached).  Must be called by all 32 lanes of one warp.
+// ---------------------------------------------------------------------------
+template <int NN>
+__device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau, int* piv_s, double* Ut,
+                                          double* Vt, double* Sout, int max_sweeps) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const bool own = lane < nn;
+  // column norms and pivots (lane j owns column j)
+  double nrm = 0.0;
+  int piv = lane;
+  if (own)
+    for (int i = 0; i < mm; ++i) nrm = fma(W[i + lane * mm], W[i + lane * mm], nrm);
+  for (int k = 0; k < nn; ++k) {
+    // pivot: largest remaining partial norm, smallest index on ties
+    double bv = (own && lane >= k) ? nrm : -1.0;
+    int bi = (own && lane >= k) ? lane : 64;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(FULL, bv, o);
+      const int oi = __shfl_xor_sync(FULL, bi, o);
+      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+    }
+    const int p = bi;
+    if (p != k && p < nn) {
+      for (int i = lane; i < mm; i += 32) {
+        const double t = W[i + k * mm];
+        W[i + k * mm] = W[i + p * mm];
+        W[i + p * mm] = t;
+      }
+      const double nk = __shfl_sync(FULL, nrm, k), np = __shfl_sync(FULL, nrm, p);
+      const int qk = __shfl_sync(FULL, piv, k), qp = __shfl_sync(FULL, piv, p);
+      if (lane == k) { nrm = np; piv = qp; }
+      if (lane == p) { nrm = nk; piv = qk; }
+      __syncwarp();
+    }
+    // Householder reflector for column k (lanes over rows)
+    double loc = 0.0;
+    for (int i = k + 1 + lane; i < mm; i += 32) loc = fma(W[i + k * mm], W[i + k * mm], loc);
+    for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(FULL, loc, o);
+    const double alpha = W[k + k * mm];
+    double tk = 0.0;
+    if (loc > 0.0) {
+      const double beta = -copysign(sqrt(alpha * alpha + loc), alpha);
+      tk = (beta - alpha) / beta;
+      const double sc = 1.0 / (alpha - beta);
+      for (int i = k + 1 + lane; i < mm; i += 32) W[i + k * mm] *= sc;
+      __syncwarp();
+      if (lane == 0) W[k + k * mm] = beta;
+    }
+    if (lane == 0) tau[k] = tk;
+    __syncwarp();
+    // apply to the columns right of k (lane j owns column j) and update norms
+    if (own && lane > k) {
+      double* aj = W + lane * mm;
+      const double* ak = W + k * mm;
+      if (tk != 0.0) {
+        double w = aj[k];
+        for (int i = k + 1; i < mm; ++i) w = fma(ak[i], aj[i], w);
+        w *= tk;
+        aj[k] -= w;
+        for (int i = k + 1; i < mm; ++i) aj[i] = fma(-w, ak[i], aj[i]);
+      }
+      double s = 0.0;
+      for (int i = k + 1; i < mm; ++i) s = fma(aj[i], aj[i], s);
+      nrm = s;
+    }
+    __syncwarp();
+  }
+  if (own) piv_s[lane] = piv;
+  // X = R^T: lane j holds column j of X = row j of R
+  double x[NN], v[NN];
+#pragma unroll
+  for (int i = 0; i < NN; ++i) {
+    x[i] = (own && i < nn && i >= lane) ? W[lane + i * mm] : 0.0;
+    v[i] = (i == lane) ? 1.0 : 0.0;
+  }
+  // unit max-abs scale (numerically-zero columns below 1e-250 are skipped)
+  double mx = 0.0;
+#pragma unroll
+  for (int i = 0; i < NN; ++i) mx = fmax(mx, fabs(x[i]));
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
+  const double sc = mx > 0.0 ? 1.0 / mx : 1.0;
+#pragma unroll
+  for (int i = 0; i < NN; ++i) x[i] *= sc;
+  const int np = (nn % 2) ? nn + 1 : nn;
+  const double tol = 2.220446049250313e-16 * 16.0;
+  int result = -1;
+  for (int sweep = 0; sweep < max_sweeps && nn > 1; ++sweep) {
+    int rotated = 0;
+    for (int r = 0; r < np - 1; ++r) {
+      int partner = (lane < np) ? rr_partner(np, r, lane) : -1;
+      if (!own || partner >= nn) partner = -1;
+      const int src = partner >= 0 ? partner : lane;
+      // dot products with the partner column (every lane takes part in every shuffle)
+      double a_own = 0.0, a_par = 0.0, g = 0.0;
+#pragma unroll
+      for (int i = 0; i < NN; ++i) {
+        const double pxi = __shfl_sync(FULL, x[i], src);
+        a_own = fma(x[i], x[i], a_own);
+        a_par = fma(pxi, pxi, a_par);
+        g = fma(x[i], pxi, g);
+      }
+      bool doit = false, low = false;
+      double c = 1.0, s = 0.0;
+      if (partner >= 0) {
+        low = lane < partner;
+        const double al = low ? a_own : a_par, be = low ? a_par : a_own;
+        if (jacobi_rotation(al, be, g, tol, &c, &s)) {
+          doit = true;
+          rotated = 1;
+        }
+      }
+      // lower column: c*x_lo - s*x_hi ; higher column: s*x_lo + c*x_hi
+#pragma unroll
+      for (int i = 0; i < NN; ++i) {
+        const double pxi = __shfl_sync(FULL, x[i], src);
+        const double pvi = __shfl_sync(FULL, v[i], src);
+        if (doit) {
+          x[i] = low ? c * x[i] - s * pxi : s * pxi + c * x[i];
+          v[i] = low ? c * v[i] - s * pvi : s * pvi + c * v[i];
+        }
+      }
+    }
+    if (!__any_sync(FULL, rotated)) {
+      result = sweep + 1;
+      break;
+    }
+  }
+  if (nn <= 1) result = 0;
+  // singular values and descending order
+  double sg = 0.0;
+#pragma unroll
+  for (int i = 0; i < NN; ++i) sg = fma(x[i], x[i], sg);
+  sg = own ? sqrt(sg) / sc : -1.0;
+  int rank = 0;
+  for (int l = 0; l < nn; ++l) {
+    const double sl = __shfl_sync(FULL, sg, l);
+    rank += (sl > sg || (sl == sg && l < lane)) ? 1 : 0;
+  }
+  __syncwarp();
+  if (own) {
+    Sout[rank] = sg;
+    // right vectors of W: Vt[piv[i], rank] = X[i, lane] / sigma
+#pragma unroll
+    for (int i = 0; i < NN; ++i)
+      if (i < nn) Vt[piv_s[i] + rank * nn] = (sg > 0.0) ? (x[i] / sc) / sg : 0.0;
+    // left vectors before Q: Ut[:, rank] = [v; 0]
+#pragma unroll
+    for (int i = 0; i < NN; ++i)
+      if (i < nn) Ut[i + rank * mm] = v[i];
+    for (int i = nn; i < mm; ++i) Ut[i + rank * mm] = 0.0;
+  }
+  __syncwarp();
+  // Ut <- Q Ut (reflectors in W's lower part), lane c owns column c
+  for (int k = nn - 1; k >= 0; --k) {
+    const double tk = tau[k];
+    if (own && tk != 0.0) {
+      double* uc = Ut + lane * mm;
+      const double* ak = W + k * mm;
+      double w = uc[k];
+      for (int i = k + 1; i < mm; ++i) w = fma(ak[i], uc[i], w);
+      w *= tk;
+      uc[k] -= w;
+      for (int i = k + 1; i < mm; ++i) uc[i] = fma(-w, ak[i], uc[i]);
+    }
+    __syncwarp();
+  }
+  return result;
+}
+#endif
 
 }  // namespace catn

@@ -119,6 +119,40 @@ struct Team {
     sync();
     return bi;
   }
+  // Atomics on shared or global ints (plain operations in the host build).
+#if CATN_DEVICE_PASS
+  __device__ __forceinline__ int atomic_add(int* p, int v) const { return atomicAdd(p, v); }
+  __device__ __forceinline__ int atomic_cas(int* p, int cmp, int val) const { return atomicCAS(p, cmp, val); }
+#else
+  int atomic_add(int* p, int v) const { int o = *p; *p += v; return o; }
+  int atomic_cas(int* p, int cmp, int val) const { int o = *p; if (o == cmp) *p = val; return o; }
+#endif
+  // Exclusive prefix sum of one int per thread over the team (thread order);
+  // *total receives the sum.
+  CATN_HD int scan_excl(int v, int* total) const {
+#if CATN_DEVICE_PASS
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane() >= o) x += y;
+    }
+    sync();
+    int* ws = (int*)red;
+    if (lane() == 31) ws[warp()] = x;
+    sync();
+    int base = 0, tot = 0;
+    for (int w = 0; w < nwarps(); ++w) {
+      if (w < warp()) base += ws[w];
+      tot += ws[w];
+    }
+    sync();
+    *total = tot;
+    return base + x - v;
+#else
+    *total = v;
+    return 0;
+#endif
+  }
   // Value computed by the leader, returned to every thread.
   CATN_HD long long bcast(long long v) const {
     sync();
