@@ -139,6 +139,35 @@ catn_status catn_ising_create(const catn_params* p, int32_t n, int32_t n_edges,
                               double beta, int32_t pos1, int32_t val1, int32_t pos2, int32_t val2,
                               int64_t arena_bytes, catn_net** out);
 
+/* Device memory the allocation-free entry point below works in: one
+ * file-scope array in the library, present on every GPU that loads it until
+ * the process exits. */
+#define CATN_STATIC_SCRATCH_BYTES (64LL << 20)
+
+/* No counterpart in the reference.  Contracts one Ising / spin-glass network
+ * exactly like catn_ising_create + catn_contract (same arguments, same
+ * result), but allocates no device memory: the packed network, the
+ * contraction's working memory and the result all live in the library's
+ * fixed CATN_STATIC_SCRATCH_BYTES device array.  For callers that must not
+ * call cudaMalloc -- code running under a caller-owned memory pool or a
+ * strict device-memory budget, or inside a host loop where allocation
+ * latency and fragmentation are not acceptable.
+ *   - Networks whose working memory does not fit return CATN_ENOMEM with
+ *     the required and available sizes in catn_last_error().
+ *   - The first call on a device looks up the array's device address (once
+ *     per device, with that device current); make that first call before
+ *     any stream capture.
+ *   - Every call reuses the same array, so calls that overlap on the GPU
+ *     (different streams, threads or processes sharing a context) race;
+ *     serialise them.  The call synchronises `stream` before returning.
+ *   - `stream` is a cudaStream_t (NULL = default stream); trace recording
+ *     (p->trace) is not available here. */
+catn_status catn_ising_contract_static(const catn_params* p, int32_t n, int32_t n_edges,
+                                       const int32_t* edges, const double* weights,
+                                       const double* fields, double beta, int32_t pos1,
+                                       int32_t val1, int32_t pos2, int32_t val2, void* stream,
+                                       catn_result* res);
+
 /* Batched Ising instances contracted in ONE persistent kernel launch with a
  * device work queue (no reference counterpart: the reference loops on the
  * host, e.g. magnetization/correlation at src/ising.jl:263-339).
