@@ -12,7 +12,11 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcatn_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
+# Each unit compiles the device engine on its own (no device linking), so one
+# kernel's register allocation never depends on another unit's kernels.
+UNITS = ["capi.cu", "capi_static.cu"]
+OBJ = os.path.join(HERE, "_build")
 
 
 def _sources():
@@ -27,15 +31,26 @@ def _stale(target, deps):
 
 
 def build_library(force=False, verbose=False):
-    """Compile csrc/capi.cu (and the headers it includes) with nvcc."""
+    """Compile the translation units in UNITS with nvcc (in parallel) and link
+    them into libcatn_b200.so."""
     if not force and not _stale(LIB, _sources() + [__file__]):
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp",
-           os.path.join(CSRC, "capi.cu")]
+    os.makedirs(OBJ, exist_ok=True)
+    objs, procs = [], []
+    for u in UNITS:
+        obj = os.path.join(OBJ, u.replace(".cu", ".o"))
+        cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", "-o", obj, os.path.join(CSRC, u)]
+        if verbose:
+            print(" ".join(cmd))
+        objs.append(obj)
+        procs.append(subprocess.Popen(cmd))
+    if any(p.wait() != 0 for p in procs):
+        raise RuntimeError("nvcc failed on one of " + ", ".join(UNITS))
+    link = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB + ".tmp", *objs]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

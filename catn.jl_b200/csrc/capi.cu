@@ -14,10 +14,12 @@
 #include <vector>
 #include "engine.cuh"
 #include "host_image.h"
+#include "capi_internal.h"
 
 using namespace catn;
+using namespace catn_capi;
 
-namespace {
+namespace catn_capi {
 
 thread_local std::string g_err;
 
@@ -29,11 +31,6 @@ catn_status cuda_fail(cudaError_t e, const char* what) {
   g_err = std::string(what) + ": " + cudaGetErrorString(e);
   return CATN_ECUDA;
 }
-#define CUDA_TRY(expr)                                   \
-  do {                                                   \
-    cudaError_t _e = (expr);                             \
-    if (_e != cudaSuccess) return cuda_fail(_e, #expr);  \
-  } while (0)
 
 const char* status_text(int s) {
   switch (s) {
@@ -48,11 +45,19 @@ const char* status_text(int s) {
   return "unknown";
 }
 
-constexpr int kThreads = 256;
-// Dynamic shared memory per CTA: reduction area, GEMM tile staging, and the
-// small-SVD workspace (two CTAs fit on one SM).
-constexpr int kSmemBytes = 100 * 1024;
-constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+catn_status check_params(const catn_params* p) {
+  if (!p) return fail(CATN_EINVAL, "params is NULL");
+  if (p->chi < 1) return fail(CATN_EINVAL, "chi must be >= 1");
+  if (p->Dmax == 0) return fail(CATN_EINVAL, "Dmax must be nonzero (negative = exact mode)");
+  if (p->norm_method < 0 || p->norm_method > 2) return fail(CATN_EINVAL, "norm_method must be 0, 1 or 2");
+  if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
+  if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
+  return CATN_OK;
+}
+
+}  // namespace catn_capi
+
+namespace {
 
 // `order` lists instance ids by descending work estimate, so the longest
 // contractions start first (longest-processing-time scheduling).
@@ -95,27 +100,6 @@ __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
     meta[2] = C.ctl[CTL_STATUS];
     for (int q = 0; q < nd && q < 64; ++q) meta[3 + q] = dims[q];
   }
-}
-
-// ---------------------------------------------------------------------------
-// Allocation-free single-network path.  All device memory it touches is this
-// fixed array: [result | packed input image | slot (control state + arena)].
-// ---------------------------------------------------------------------------
-static __device__ __align__(256) char g_static_scratch[CATN_STATIC_SCRATCH_BYTES];
-
-__global__ void __launch_bounds__(kThreads) catn_static_kernel(char* base, long long off_res, long long off_desc,
-                                                               long long off_i64, long long off_i32,
-                                                               long long off_dat, long long off_slot,
-                                                               SlotLayout L) {
-  extern __shared__ double smem[];
-  Team T;
-  T.red = smem;
-  T.stage = (char*)(smem + 64);
-  T.stage_bytes = GEMM_STAGE_BYTES;
-  double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
-  const InstDesc D = *(const InstDesc*)(base + off_desc);
-  run_instance(T, base + off_slot, L, D, (const long long*)(base + off_i64), (const int*)(base + off_i32),
-               (const double*)(base + off_dat), (catn_result*)(base + off_res), nullptr, sws, kSwsDoubles);
 }
 
 // Device copy of an Image plus slots and results.  The input image is packed
@@ -239,16 +223,6 @@ void catn_params_default(catn_params* p) {
   p->cut_bond = 0;
   p->seed = 1;
   p->trace = 0;
-}
-
-static catn_status check_params(const catn_params* p) {
-  if (!p) return fail(CATN_EINVAL, "params is NULL");
-  if (p->chi < 1) return fail(CATN_EINVAL, "chi must be >= 1");
-  if (p->Dmax == 0) return fail(CATN_EINVAL, "Dmax must be nonzero (negative = exact mode)");
-  if (p->norm_method < 0 || p->norm_method > 2) return fail(CATN_EINVAL, "norm_method must be 0, 1 or 2");
-  if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
-  if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
-  return CATN_OK;
 }
 
 static long long default_arena(long long a) { return a > 0 ? a : (1LL << 30); }
@@ -425,77 +399,6 @@ catn_status catn_batch_destroy(catn_batch* b) {
   if (!b) return CATN_OK;
   b->R.release();
   delete b;
-  return CATN_OK;
-}
-
-// Device address of g_static_scratch, looked up once per device (with that
-// device current) on the first call there.
-static catn_status static_scratch_address(char** out) {
-  static std::mutex mu;
-  static char* addr[256] = {nullptr};
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) return fail(CATN_EINVAL, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* ptr = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress(&ptr, g_static_scratch));
-    CUDA_TRY(cudaFuncSetAttribute(catn_static_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    addr[dev] = (char*)ptr;
-  }
-  *out = addr[dev];
-  return CATN_OK;
-}
-
-catn_status catn_ising_contract_static(const catn_params* p, int32_t n, int32_t n_edges, const int32_t* edges,
-                                       const double* weights, const double* fields, double beta, int32_t pos1,
-                                       int32_t val1, int32_t pos2, int32_t val2, void* stream,
-                                       catn_result* res) {
-  if (catn_status s = check_params(p)) return s;
-  if (!res || (n_edges > 0 && (!edges || !weights)) || !fields) return fail(CATN_EINVAL, "NULL argument");
-  catn_params q = *p;
-  q.trace = 0;
-  Image im;   // host-side packing only
-  std::string e = im.add_ising(q, n, n_edges, edges, weights, fields, beta, pos1, val1, pos2, val2, 0);
-  if (!e.empty()) return fail(CATN_EINVAL, e);
-  // carve the fixed array: result, input image, slot
-  const long long off_res = 0;
-  const long long off_desc = align256((long long)sizeof(catn_result));
-  const long long off_i64 = off_desc + align256((long long)sizeof(InstDesc));
-  const long long off_i32 = off_i64 + align256((long long)(sizeof(long long) * im.i64.size()));
-  const long long off_dat = off_i32 + align256((long long)(sizeof(int) * im.i32.size()));
-  const long long off_slot = off_dat + align256((long long)(sizeof(double) * im.dat.size()));
-  const SlotLayout L0 = make_layout(im.nmax, default_maxs(im), im.emax + 64, 0);
-  const long long min_arena = 1LL << 20;
-  const long long avail = CATN_STATIC_SCRATCH_BYTES - off_slot - L0.slot_bytes;
-  if (avail < min_arena)
-    return fail(CATN_ENOMEM, "network needs " + std::to_string(off_slot + L0.slot_bytes + min_arena) +
-                                 " bytes of device scratch; the static maximum is " +
-                                 std::to_string((long long)CATN_STATIC_SCRATCH_BYTES));
-  const SlotLayout L = make_layout(im.nmax, default_maxs(im), im.emax + 64, avail & ~255LL);
-  char* base = nullptr;
-  if (catn_status s = static_scratch_address(&base)) return s;
-  cudaStream_t st = (cudaStream_t)stream;
-  // inputs in; the previous call's result is cleared so that a failed launch
-  // cannot return stale values
-  CUDA_TRY(cudaMemsetAsync(base + off_res, 0, sizeof(catn_result), st));
-  CUDA_TRY(cudaMemcpyAsync(base + off_desc, im.desc.data(), sizeof(InstDesc), cudaMemcpyHostToDevice, st));
-  if (!im.i64.empty())
-    CUDA_TRY(cudaMemcpyAsync(base + off_i64, im.i64.data(), sizeof(long long) * im.i64.size(),
-                             cudaMemcpyHostToDevice, st));
-  if (!im.i32.empty())
-    CUDA_TRY(cudaMemcpyAsync(base + off_i32, im.i32.data(), sizeof(int) * im.i32.size(), cudaMemcpyHostToDevice,
-                             st));
-  if (!im.dat.empty())
-    CUDA_TRY(cudaMemcpyAsync(base + off_dat, im.dat.data(), sizeof(double) * im.dat.size(),
-                             cudaMemcpyHostToDevice, st));
-  catn_static_kernel<<<1, kThreads, kSmemBytes, st>>>(base, off_res, off_desc, off_i64, off_i32, off_dat, off_slot,
-                                                       L);
-  CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(res, base + off_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaStreamSynchronize(st));
-  if (res->status != CATN_OK)
-    return fail((catn_status)res->status, std::string("contraction failed: ") + status_text(res->status));
   return CATN_OK;
 }
 
