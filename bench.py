@@ -12,6 +12,17 @@ Workload (one "step" = one persistent-kernel pass over one batch):
          host->device copy of the packed inputs, the launch, device->host
          read of every instance's result (CUDA events on the same stream)
 
+  grad   the other half of the metric: d lnZ / d w and d lnZ / d h (every
+         <s_i s_j>, <s_k> of every instance) from one device gradient run
+         of the whole batch, against the reference's pinning definition,
+         which needs 1 + 2n + 4|E| contractions per instance (priced at the
+         measured forward rate, and timed directly on one sample instance)
+
+  plain_gpu_form  the same instances through the plain GPU form
+         (baseline/plain_gpu_form.py: PyTorch FP64, one library call per
+         op from a host loop, one instance at a time), a bounded sample on
+         rank 0 at N=1, with its |dlnZ|/n against the engine
+
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
 Multi-GPU: one process per GPU (torchrun); every rank contracts its own
@@ -79,6 +90,30 @@ def cpu_sample_rate(instances, seconds, nproc, pool=None):
     if own:
         pool.terminate()
     return done / dt, done, lz
+
+
+def plain_form_rate(instances, engine_lnZ, seconds):
+    """Contract instances in order through the plain GPU form until about
+    `seconds` have passed; return (instances/s, count, max |dlnZ|/n vs the
+    engine)."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "baseline"))
+    import plain_gpu_form as PG
+    sys.path.pop(0)
+    w = instances[0]   # warm-up: cuSOLVER/cuBLAS handles and workspaces
+    PG.contraction(PG.ising_network(w["n"], w["edges"], w["weights"], w["fields"], w["beta"], **PARAMS))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done, dev = 0, 0.0
+    for d, ref in zip(instances, engine_lnZ):
+        lz, _, _ = PG.contraction(PG.ising_network(d["n"], d["edges"], d["weights"], d["fields"], d["beta"],
+                                                   **PARAMS))
+        done += 1
+        dev = max(dev, abs(lz - ref) / d["n"])
+        if time.perf_counter() - t0 > seconds:
+            break
+    torch.cuda.synchronize()
+    return done / (time.perf_counter() - t0), done, dev
 
 
 def host_cores():
@@ -209,6 +244,9 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient leg")
+    ap.add_argument("--plain-seconds", type=float, default=15.0,
+                    help="time budget of the plain GPU form sample (0 = skip)")
     ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
     ap.add_argument("--arena-mb", type=int, default=64, help="device arena per slot, MiB")
     args = ap.parse_args()
@@ -240,8 +278,10 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
+    import ctypes
     import __graft_entry__
     catn = __graft_entry__.load_package()
+    from catn_b200 import _lib as catn_lib
     insts = make_instances(args.instances, args.seed + 7919 * rank)
     batch = catn.IsingBatch(insts, slot_arena_bytes=args.arena_mb << 20, max_slots=args.max_slots, **PARAMS)
     stream = torch.cuda.current_stream()
@@ -320,8 +360,8 @@ def main():
                    "contraction_steps_total": int(sum(steps_per_inst))},
         "e2e": {"value": round(e2e_value, 3), "unit": "instances/s",
                 "h2d_bytes_per_step": int(batch.input_bytes),
-                "d2h_bytes_per_step": int(args.instances * 64)},
-        "gpu_launches": args.steps,
+                "d2h_bytes_per_step": int(args.instances * ctypes.sizeof(catn_lib.Result))},
+        "gpu_launches": 2 * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 3), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 6), "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
@@ -332,10 +372,70 @@ def main():
     }
     if cpu:
         out["cpu_baseline"] = cpu
+    if world == 1 and not args.no_grad:
+        out["grad"] = grad_leg(catn, batch, insts, value, stream, sh)
+    if world == 1 and args.plain_seconds > 0:
+        rate, cnt, dev = plain_form_rate(insts, [r.lnZ for r in res], args.plain_seconds)
+        out["plain_gpu_form"] = {
+            "value": round(rate, 3), "unit": "instances/s", "value_over_plain": round(value / rate, 1),
+            "max_abs_dlnZ_per_spin_vs_engine": dev,
+            "sample": f"first {cnt} of the {args.instances} workload instances in order, one at a time, "
+                      f"PyTorch FP64 on cuda:{local} (torch.linalg.svd/qr + einsum per op, host loop), "
+                      f"~{args.plain_seconds:.0f} s wall clock"}
     print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def grad_leg(catn, batch, insts, forward_rate, stream, sh):
+    """Adjoint of the whole batch (one launch) against pinning."""
+    import torch
+    batch.grad_launch(sh)   # first call allocates the gradient slots
+    batch.grad_fetch(sh)
+    times = []
+    for _ in range(2):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch.grad_launch(sh)
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) / 1000.0)
+    res, dw, dh = batch.grad_fetch(sh)
+    t_grad = sum(times) / len(times)
+    pin = [1 + 2 * d["n"] + 4 * len(d["edges"]) for d in insts]
+    t_pin = sum(pin) / forward_rate
+    # one instance timed both ways: its pinned set in one batch launch, and
+    # its gradient run alone; observables compared
+    d = min(insts, key=lambda x: x["n"])
+    kw = dict(PARAMS)
+    t0 = time.perf_counter()
+    m_pin = catn.magnetization(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
+    c_pin = catn.correlation(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
+    t_pin1 = time.perf_counter() - t0
+    tn = catn.ising_network(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
+    catn.gradient(tn)   # allocation of its gradient slot
+    t0 = time.perf_counter()
+    _, gw, gh = catn.gradient(tn)
+    t_adj1 = time.perf_counter() - t0
+    dev = max(float(np.max(np.abs(gh / d["beta"] - m_pin))), float(np.max(np.abs(gw / d["beta"] - c_pin))))
+    return {
+        "what": "d lnZ/d w_e = beta <s_i s_j> for every edge and d lnZ/d h_k = beta <s_k> for every spin of "
+                "every instance, one device gradient run (taped forward + backward) of the whole batch",
+        "adjoint_ms_per_batch": round(1000 * t_grad, 3),
+        "adjoint_instances_per_s": round(len(insts) / t_grad, 3),
+        "pinning_contractions_per_batch": int(sum(pin)),
+        "pinning_ms_per_batch_at_forward_rate": round(1000 * t_pin, 3),
+        "speedup_vs_pinning": round(t_pin / t_grad, 1),
+        "sample_instance": {"n": d["n"], "edges": len(d["edges"]), "pinned_contractions": pin[insts.index(d)],
+                            "pinning_s_wall": round(t_pin1, 4), "adjoint_s_wall": round(t_adj1, 4),
+                            "speedup_wall": round(t_pin1 / t_adj1, 1),
+                            "max_abs_observable_diff_vs_pinning": dev},
+        "timing": "CUDA events around catn_batch_grad_launch (input upload + one launch), mean of 2; "
+                  "sample instance: host wall clock around the public calls",
+    }
 
 
 def ct_stream(stream):

@@ -102,33 +102,9 @@ __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
   }
 }
 
-// Device copy of an Image plus slots and results.  The input image is packed
-// into one pinned host buffer and one device buffer, so an upload is a single
-// host-to-device copy.
-struct DeviceRun {
-  char* h_input = nullptr;   // pinned
-  char* d_input = nullptr;
-  InstDesc* d_desc = nullptr;
-  int* d_order = nullptr;
-  long long* d_i64 = nullptr;
-  int* d_i32 = nullptr;
-  double* d_dat = nullptr;
-  char* d_slots = nullptr;
-  catn_result* d_res = nullptr;
-  int* d_trace = nullptr;
-  int* d_queue = nullptr;
-  SlotLayout L;
-  int nslots = 0;
-  int ninst = 0;
-  long long input_bytes = 0;
+}  // namespace
 
-  void release() {
-    cudaFreeHost(h_input);
-    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
-    h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
-    d_desc = nullptr; d_order = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
-  }
-};
+namespace catn_capi {
 
 catn_status prepare(const Image& im, long long arena_bytes, int max_slots, DeviceRun& R) {
   R.ninst = (int)im.desc.size();
@@ -180,10 +156,33 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   return CATN_OK;
 }
 
-catn_status upload(const Image&, DeviceRun& R, cudaStream_t st) {
+catn_status upload(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemcpyAsync(R.d_input, R.h_input, (size_t)R.input_bytes, cudaMemcpyHostToDevice, st));
   return CATN_OK;
 }
+
+// Arena of a single network when the caller passes 0: the largest two-site
+// matrix a swap can form is (chi*Dmax)^2 doubles, and a full-rank SVD of it
+// holds five such buffers on the scratch stack (40 % of the arena), so take
+// 16x that matrix, at least 1 GiB and at most 48 GiB or a quarter of the
+// free device memory.  Exact mode (Dmax < 0) keeps 1 GiB: its networks are
+// small by construction.
+long long default_arena(long long a, const catn_params& p) {
+  if (a > 0) return a;
+  long long arena = 1LL << 30;
+  if (p.Dmax > 0) {
+    const long long m = (long long)std::min(p.chi, 16384) * std::min(p.Dmax, 16384);
+    arena = std::max(arena, 16 * 8 * m * m);
+  }
+  arena = std::min(arena, 48LL << 30);
+  size_t freeb = 0, totalb = 0;
+  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) arena = std::min(arena, (long long)(freeb / 4));
+  return std::max(arena, 1LL << 30);
+}
+
+}  // namespace catn_capi
+
+namespace {
 
 catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, sizeof(int), st));
@@ -196,16 +195,6 @@ catn_status launch(DeviceRun& R, cudaStream_t st) {
 
 }  // namespace
 
-struct catn_net {
-  Image im;
-  DeviceRun R;
-  bool contracted = false;
-};
-
-struct catn_batch {
-  Image im;
-  DeviceRun R;
-};
 
 extern "C" {
 
@@ -225,10 +214,12 @@ void catn_params_default(catn_params* p) {
   p->trace = 0;
 }
 
-static long long default_arena(long long a) { return a > 0 ? a : (1LL << 30); }
-
 static catn_status net_finish(catn_net* net, long long arena_bytes, catn_net** out) {
-  catn_status s = prepare(net->im, default_arena(arena_bytes), 1, net->R);
+  if (net->im.desc.empty()) {
+    delete net;
+    return fail(CATN_EINVAL, "no instances");
+  }
+  catn_status s = prepare(net->im, default_arena(arena_bytes, net->im.desc[0].P), 1, net->R);
   if (s != CATN_OK) {
     net->R.release();
     delete net;
@@ -285,7 +276,7 @@ catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32
   if (!net || !res) return fail(CATN_EINVAL, "NULL argument");
   if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
   cudaStream_t st = 0;
-  if (catn_status s = upload(net->im, net->R, st)) return s;
+  if (catn_status s = upload(net->R, st)) return s;
   if (catn_status s = launch(net->R, st)) return s;
   CUDA_TRY(cudaMemcpyAsync(res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
@@ -330,6 +321,7 @@ catn_status catn_result_tensor(catn_net* net, double* out, int64_t cap, int64_t*
 
 catn_status catn_net_destroy(catn_net* net) {
   if (!net) return CATN_OK;
+  grad_release(net->grad);
   net->R.release();
   delete net;
   return CATN_OK;
@@ -355,6 +347,7 @@ catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const 
     if (!e.empty()) { delete b; return fail(CATN_EINVAL, "instance " + std::to_string(q) + ": " + e); }
   }
   long long arena = slot_arena_bytes > 0 ? slot_arena_bytes : (128LL << 20);
+  b->arena = arena;
   if (catn_status s = prepare(b->im, arena, max_slots, b->R)) {
     b->R.release();
     delete b;
@@ -366,7 +359,7 @@ catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const 
 
 catn_status catn_batch_upload(catn_batch* b, void* stream) {
   if (!b) return fail(CATN_EINVAL, "NULL batch");
-  return upload(b->im, b->R, (cudaStream_t)stream);
+  return upload(b->R, (cudaStream_t)stream);
 }
 
 catn_status catn_batch_launch(catn_batch* b, void* stream) {
@@ -397,6 +390,7 @@ int64_t catn_batch_input_bytes(const catn_batch* b) { return b ? b->R.input_byte
 
 catn_status catn_batch_destroy(catn_batch* b) {
   if (!b) return CATN_OK;
+  grad_release(b->grad);
   b->R.release();
   delete b;
   return CATN_OK;

@@ -1,13 +1,15 @@
 // Host-side helpers shared by the translation units of libcatn_b200
 // (capi.cu: the persistent-kernel entry points; capi_static.cu: the
-// allocation-free entry point).  Each unit compiles the device engine on its
-// own, so the register allocation of one kernel's call tree never depends on
-// another kernel that shares the engine's out-of-line routines.
+// allocation-free entry point; capi_grad.cu: the adjoint).  Each unit
+// compiles the device engine on its own, so the register allocation of one
+// kernel's call tree never depends on another kernel that shares the
+// engine's out-of-line routines.
 #pragma once
 #include <cuda_runtime.h>
 #include <string>
 #include "catn_b200.h"
 #include "linalg.cuh"
+#include "host_image.h"
 
 namespace catn_capi {
 
@@ -24,7 +26,66 @@ const char* status_text(int s);
 // Argument checks shared by every create/contract entry point.
 catn_status check_params(const catn_params* p);
 
+// Device copy of an Image plus slots and results.  The input image is packed
+// into one pinned host buffer and one device buffer, so an upload is a single
+// host-to-device copy.
+struct DeviceRun {
+  char* h_input = nullptr;   // pinned
+  char* d_input = nullptr;
+  catn::InstDesc* d_desc = nullptr;
+  int* d_order = nullptr;
+  long long* d_i64 = nullptr;
+  int* d_i32 = nullptr;
+  double* d_dat = nullptr;
+  char* d_slots = nullptr;
+  catn_result* d_res = nullptr;
+  int* d_trace = nullptr;
+  int* d_queue = nullptr;
+  catn::SlotLayout L;
+  int nslots = 0;
+  int ninst = 0;
+  long long input_bytes = 0;
+
+  void release() {
+    cudaFreeHost(h_input);
+    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
+    h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
+    d_desc = nullptr; d_order = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
+  }
+};
+
+// Device buffers of a gradient run: its own slots (heap + shadow + tape) and
+// the gradients of the input sites, in the image's data layout.
+struct GradRun {
+  DeviceRun R;
+  double* d_gimg = nullptr;
+  double* h_gimg = nullptr;   // pinned
+  long long arena = 0;
+};
+
+// Sizes slots and packs the image (capi.cu).
+catn_status prepare(const catn::Image& im, long long arena_bytes, int max_slots, DeviceRun& R);
+catn_status upload(DeviceRun& R, cudaStream_t st);
+// Arena of a single network when the caller passes 0 (capi.cu).
+long long default_arena(long long a, const catn_params& p);
+// Frees a gradient run (capi_grad.cu).
+void grad_release(GradRun* g);
+
 }  // namespace catn_capi
+
+struct catn_net {
+  catn::Image im;
+  catn_capi::DeviceRun R;
+  bool contracted = false;
+  catn_capi::GradRun* grad = nullptr;
+};
+
+struct catn_batch {
+  catn::Image im;
+  catn_capi::DeviceRun R;
+  long long arena = 0;
+  catn_capi::GradRun* grad = nullptr;
+};
 
 #define CUDA_TRY(expr)                                                \
   do {                                                                \

@@ -29,6 +29,30 @@
 
 namespace catn {
 
+// One operation of the adjoint tape (gradient runs).  Every operation that
+// writes site data appends one record naming its input and output versions
+// by heap byte offset (the heap is append-only on a gradient run, so an
+// offset names one version for the whole run) plus what its backward needs.
+enum {
+  OP_CANO_R = 1,   // a: dl d dr nkeep nx.d nx.dr    o: site nx | new site, new nx | S V
+  OP_CANO_L,       // a: dl d dr nkeep pv.dl pv.d    o: site pv | new site, new pv | S V
+  OP_SWAP,         // a: d0 d1 d2 d3 k myd i<j       o: tl tr | lo hi | S, U or V
+  OP_REVERSE,      // a: dl d dr                     o: old new
+  OP_MERGE,        // a: dl da k db dr               o: a b | fused
+  OP_EAT_A,        // a: d                           o: vi vj          v: r, flag: |r| > cutoff
+  OP_EAT_B,        // a: Dl dd ne                    o: last tj prev | new
+  OP_EAT_C,        // a: Dl dd Dr pr                 o: last hj prev | new
+  OP_NORM,         // a: len method                  o: x | x / nrm    v: nrm
+  OP_CUT,          // a: dl d dr dl2 dr2 myd         o: Ai Aj | new Ai, new Aj | S
+  OP_LOGZ          // a: len                         o: scalar site    v: z
+};
+struct TapeRec {
+  int op, flag;
+  int a[10];
+  long long o[8];
+  double v[2];
+};
+
 struct Ctx {
   Team T;
   catn_params P;
@@ -67,6 +91,13 @@ struct Ctx {
   int multigraph; // the input lists some neighbour twice
   int* trace;
   int trace_cap;
+  // Adjoint tape (tape != 0 on gradient runs only): the site heap is
+  // append-only, records go to rec[0, rcap), and the gradient of the double
+  // at heap byte offset o lives at byte offset o + gshift (the shadow heap).
+  int tape;
+  TapeRec* rec;
+  long long nrec, rcap, gshift;
+  long long heap_first;   // first byte of the sites loaded from the image
 };
 
 // ---------------------------------------------------------------------------
@@ -172,9 +203,10 @@ CATN_HDI inline void heap_compact(Ctx& C) {
 }
 
 // Make room for `bytes` of new sites (may compact: re-read site refs after).
+// A gradient run never compacts: every version stays where it was written.
 CATN_HDI inline bool heap_reserve(Ctx& C, long long bytes) {
   if (C.hb + bytes <= C.he) return true;
-  heap_compact(C);
+  if (!C.tape) heap_compact(C);
   if (C.hb + bytes <= C.he) return true;
   fail_all(C, CATN_ENOMEM);
   return false;
@@ -185,6 +217,25 @@ CATN_HD long long heap_take(Ctx& C, long long bytes) {
   long long used = C.hb - (C.half ? C.h_lo1 : C.h_lo0);
   if (used > C.h_peak) C.h_peak = used;
   return off;
+}
+
+// Append one tape record (all threads call it alike; the leader writes).
+CATN_HD TapeRec trec(int op) {
+  TapeRec r;
+  r.op = op;
+  r.flag = 0;
+  for (int q = 0; q < 10; ++q) r.a[q] = 0;
+  for (int q = 0; q < 8; ++q) r.o[q] = -1;
+  r.v[0] = r.v[1] = 0.0;
+  return r;
+}
+CATN_HD void tape_push(Ctx& C, const TapeRec& r) {
+  if (C.nrec >= C.rcap) {
+    fail_all(C, CATN_ENOMEM);
+    return;
+  }
+  if (C.T.leader()) C.rec[C.nrec] = r;
+  C.nrec += 1;
 }
 
 // Algorithmic work counters.
@@ -529,10 +580,21 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       const long long te = clk();
       const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
       SiteRef nx = sref(C, k, i + 1);
-      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * nkeep * nx.d * nx.dr))) return;
+      const long long tb = C.tape ? al256(8LL * nkeep) + al256(8 * n * nkeep) : 0;
+      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * nkeep * nx.d * nx.dr) + tb)) return;
       nx = sref(C, k, i + 1);
       const long long ni = heap_take(C, 8 * m * nkeep);
       const long long nn2 = heap_take(C, 8LL * nkeep * nx.d * nx.dr);
+      if (C.tape) {
+        TapeRec r = trec(OP_CANO_R);
+        r.a[0] = s.dl; r.a[1] = s.d; r.a[2] = s.dr; r.a[3] = nkeep; r.a[4] = nx.d; r.a[5] = nx.dr;
+        r.o[0] = s.off; r.o[1] = nx.off; r.o[2] = ni; r.o[3] = nn2;
+        r.o[4] = heap_take(C, 8LL * nkeep);
+        r.o[5] = heap_take(C, 8 * n * nkeep);
+        copy(T, dptr(C, r.o[4]), R.S, nkeep);
+        copy(T, dptr(C, r.o[5]), R.V, n * nkeep);
+        tape_push(C, r);
+      }
       copy(T, dptr(C, ni), R.U, m * nkeep);
       // next <- (S V^H)[1:nkeep, :] * next
       gemm(T, nkeep, (long long)nx.d * nx.dr, n, mop(R.V, imap(1, 0, n), rows_plain(), R.S, nullptr),
@@ -563,10 +625,21 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
       const long long te = clk();
       const int nkeep = keep_all_if_none(C, R, C.P.cutoff);
       SiteRef pv = sref(C, k, i - 1);
-      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * pv.dl * pv.d * nkeep))) return;
+      const long long tb = C.tape ? al256(8LL * nkeep) + al256(8 * dl * nkeep) : 0;
+      if (!heap_reserve(C, al256(8 * m * nkeep) + al256(8LL * pv.dl * pv.d * nkeep) + tb)) return;
       pv = sref(C, k, i - 1);
       const long long ni = heap_take(C, 8 * m * nkeep);
       const long long np = heap_take(C, 8LL * pv.dl * pv.d * nkeep);
+      if (C.tape) {
+        TapeRec r = trec(OP_CANO_L);
+        r.a[0] = s.dl; r.a[1] = s.d; r.a[2] = s.dr; r.a[3] = nkeep; r.a[4] = pv.dl; r.a[5] = pv.d;
+        r.o[0] = s.off; r.o[1] = pv.off; r.o[2] = ni; r.o[3] = np;
+        r.o[4] = heap_take(C, 8LL * nkeep);
+        r.o[5] = heap_take(C, 8 * dl * nkeep);
+        copy(T, dptr(C, r.o[4]), R.S, nkeep);
+        copy(T, dptr(C, r.o[5]), R.V, dl * nkeep);
+        tape_push(C, r);
+      }
       // new site = permutedims(reshape(U[:, 1:nkeep], d, dr, nkeep), (3,1,2)) = U^T
       materialize(T, dptr(C, ni), nkeep, m, nkeep, transposed(R.U, m));
       // prev <- prev * (S V^H)^T
@@ -634,9 +707,23 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   } else {
     myd = keep_rule(C, R, C.P.cutoff, C.P.chi, &err);
   }
-  if (!heap_reserve(C, al256(8 * m * myd) + al256(8 * n * myd))) return err;
+  const long long tb = C.tape ? al256(8LL * myd) + al256(8 * (i < j ? n : m) * myd) : 0;
+  if (!heap_reserve(C, al256(8 * m * myd) + al256(8 * n * myd) + tb)) return err;
   const long long nl = heap_take(C, 8 * m * myd);
   const long long nr = heap_take(C, 8 * n * myd);
+  if (C.tape) {
+    // i < j stores U verbatim and S V^H; i > j stores U S and V^H verbatim:
+    // keep S and the factor that is not stored as it is
+    TapeRec r = trec(OP_SWAP);
+    r.a[0] = (int)d0; r.a[1] = (int)d1; r.a[2] = (int)d2; r.a[3] = (int)d3; r.a[4] = (int)kk; r.a[5] = myd;
+    r.a[6] = i < j;
+    r.o[0] = tl.off; r.o[1] = tr.off; r.o[2] = nl; r.o[3] = nr;
+    r.o[4] = heap_take(C, 8LL * myd);
+    r.o[5] = heap_take(C, 8 * (i < j ? n : m) * myd);
+    copy(T, dptr(C, r.o[4]), R.S, myd);
+    copy(T, dptr(C, r.o[5]), i < j ? R.V : R.U, (i < j ? n : m) * myd);
+    tape_push(C, r);
+  }
   if (i < j) {
     copy(T, dptr(C, nl), R.U, m * myd);
     materialize(T, dptr(C, nr), myd, n, myd, mop(R.V, imap(1, 0, n), rows_plain(), R.S, nullptr));
@@ -719,6 +806,18 @@ CATN_HDI inline void reverse_node(Ctx& C, int k) {
     cur += al256(8 * tot);
   }
   T.sync();
+  if (C.tape) {
+    long long c2 = first;
+    for (int p = 1; p <= ns; ++p) {
+      const SiteRef s = sref(C, k, p);
+      TapeRec r = trec(OP_REVERSE);
+      r.a[0] = s.dl; r.a[1] = s.d; r.a[2] = s.dr;
+      r.o[0] = s.off; r.o[1] = c2;
+      tape_push(C, r);
+      c2 += al256(sbytes(s));
+    }
+    T.sync();
+  }
   if (T.leader()) {
     // old site p was copied (transposed) to `first + sum of earlier sizes`;
     // it becomes position ns + 1 - p
@@ -794,6 +893,12 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
   b = sref(C, k, idx1 + 1);
   const long long f = heap_take(C, 8 * rows * cols);
   gemm(T, rows, cols, a.dr, colmajor(sdata(C, a), rows), colmajor(sdata(C, b), a.dr), colmajor(dptr(C, f), rows));
+  if (C.tape) {
+    TapeRec r = trec(OP_MERGE);
+    r.a[0] = a.dl; r.a[1] = a.d; r.a[2] = a.dr; r.a[3] = b.d; r.a[4] = b.dr;
+    r.o[0] = a.off; r.o[1] = b.off; r.o[2] = f;
+    tape_push(C, r);
+  }
   account(C, 2.0 * rows * a.dr * cols, 8.0 * ((double)rows * a.dr + (double)a.dr * cols + (double)rows * cols));
   if (T.leader()) {
     sref(C, k, idx1) = mksite(a.dl, a.d * b.d, b.dr, f);
@@ -803,6 +908,33 @@ CATN_HDI inline double merge_dup(Ctx& C, int k, int j, bool cross) {
   prof_add(C, PROF_MERGE, (double)(clk() - tf));
   cano_to(C, k, idx1);
   return err;
+}
+
+// Divide site (k, pos) by nrm.  A gradient run writes the quotient as a new
+// recorded version (same arithmetic as the in-place scale).
+CATN_HDI inline bool normalize_site(Ctx& C, int k, int pos, double nrm) {
+  const Team& T = C.T;
+  SiteRef s = sref(C, k, pos);
+  const long long len = (long long)s.dl * s.d * s.dr;
+  if (!C.tape || C.P.norm_method == 0) {
+    scale(T, sdata(C, s), 1.0 / nrm, len);
+    return true;
+  }
+  if (!heap_reserve(C, al256(8 * len))) return false;
+  const long long xo = heap_take(C, 8 * len);
+  const double inv = 1.0 / nrm;
+  const double* x = sdata(C, s);
+  double* y = dptr(C, xo);
+  for (long long e = T.rank(); e < len; e += T.size()) y[e] = x[e] * inv;
+  T.sync();
+  TapeRec r = trec(OP_NORM);
+  r.a[0] = (int)len; r.a[1] = C.P.norm_method;
+  r.o[0] = s.off; r.o[1] = xo;
+  r.v[0] = nrm;
+  tape_push(C, r);
+  if (T.leader()) sref(C, k, pos).off = xo;
+  T.sync();
+  return true;
 }
 
 // ---------------------------------------------------------------------------
@@ -824,6 +956,11 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
     for (long long e = T.rank(); e < d; e += T.size()) loc = fma(vi[e], vj[e], loc);
     double r = T.sum(loc);
     double absr = fabs(r);
+    if (C.tape) {
+      TapeRec q = trec(OP_EAT_A);
+      q.a[0] = (int)d; q.o[0] = si.off; q.o[1] = sj.off; q.v[0] = r; q.flag = absr > cutoff;
+      tape_push(C, q);
+    }
     T.sync();
     if (T.leader()) {
       C.node[ki].nsites = 0;
@@ -851,6 +988,12 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
     prev = sref(C, ki, hi.nsites - 1);
     const long long nt = heap_take(C, 8 * ne);
     gemm(T, ne, 1, prev.dr, colmajor(sdata(C, prev), ne), colmajor(vbuf, prev.dr), colmajor(dptr(C, nt), ne));
+    if (C.tape) {
+      TapeRec q = trec(OP_EAT_B);
+      q.a[0] = last.dl; q.a[1] = last.d; q.a[2] = (int)ne;
+      q.o[0] = last.off; q.o[1] = tj.off; q.o[2] = prev.off; q.o[3] = nt;
+      tape_push(C, q);
+    }
     account(C, 2.0 * last.dl * last.d + 2.0 * ne * prev.dr, 8.0 * ((double)last.dl * last.d + ne * prev.dr + ne));
     const double nrm = norm_of(C, dptr(C, nt), ne);
     if (T.leader()) {
@@ -862,7 +1005,7 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
     T.sync();
     C.sp = mark;
     if (nrm <= cutoff) return 0.0;
-    scale(T, dptr(C, nt), 1.0 / nrm, ne);
+    if (!normalize_site(C, ki, hi.nsites - 1, nrm)) return 0.0;
     return log(nrm);
   }
   // (c) general
@@ -881,6 +1024,12 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   prev = sref(C, ki, hi.nsites - 1);
   const long long nt = heap_take(C, 8 * pr * Dr);
   gemm(T, pr, Dr, prev.dr, colmajor(sdata(C, prev), pr), colmajor(mat, Dl), colmajor(dptr(C, nt), pr));
+  if (C.tape) {
+    TapeRec q = trec(OP_EAT_C);
+    q.a[0] = (int)Dl; q.a[1] = (int)dd; q.a[2] = (int)Dr; q.a[3] = (int)pr;
+    q.o[0] = last.off; q.o[1] = hj.off; q.o[2] = prev.off; q.o[3] = nt;
+    tape_push(C, q);
+  }
   account(C, 2.0 * Dl * dd * Dr + 2.0 * pr * prev.dr * Dr,
           8.0 * ((double)Dl * dd + (double)dd * Dr + (double)pr * prev.dr + (double)pr * Dr));
   T.sync();
@@ -911,7 +1060,7 @@ CATN_HDI inline double eat(Ctx& C, int ki, int kj, int idx, int idxi, double* er
   const long long ce = (long long)ctr.dl * ctr.d * ctr.dr;
   const double nrm = norm_of(C, sdata(C, ctr), ce);
   if (nrm <= cutoff) return 0.0;
-  scale(T, sdata(C, ctr), 1.0 / nrm, ce);
+  if (!normalize_site(C, ki, C.node[ki].cano, nrm)) return 0.0;
   return log(nrm);
 }
 
@@ -1097,9 +1246,18 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   materialize(T, vj, qj.rrows, myd, qj.rrows, mop(R.V, rows_plain(), cols_plain(qj.rrows), nullptr, sq));
   qr_expand(C, qi, ui, myd, fi);   // (da_l*da_r) x myd
   qr_expand(C, qj, vj, myd, fj);
-  if (!heap_reserve(C, al256(8LL * Ai.dl * myd * Ai.dr) + al256(8LL * Aj.dl * myd * Aj.dr))) return 0.0;
+  const long long tb = C.tape ? al256(8LL * myd) : 0;
+  if (!heap_reserve(C, al256(8LL * Ai.dl * myd * Ai.dr) + al256(8LL * Aj.dl * myd * Aj.dr) + tb)) return 0.0;
   const long long ni = heap_take(C, 8LL * Ai.dl * myd * Ai.dr);
   const long long nj = heap_take(C, 8LL * Aj.dl * myd * Aj.dr);
+  if (C.tape) {
+    TapeRec r = trec(OP_CUT);
+    r.a[0] = Ai.dl; r.a[1] = (int)d; r.a[2] = Ai.dr; r.a[3] = Aj.dl; r.a[4] = Aj.dr; r.a[5] = myd;
+    r.o[0] = Ai.off; r.o[1] = Aj.off; r.o[2] = ni; r.o[3] = nj;
+    r.o[4] = heap_take(C, 8LL * myd);
+    copy(T, dptr(C, r.o[4]), R.S, myd);
+    tape_push(C, r);
+  }
   {
     // new site = permutedims(reshape(mat, dl, dr, myd), (1,3,2))
     double* O = dptr(C, ni);
@@ -1456,6 +1614,7 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
   ContractOut O;
   O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
   const bool buckets = (C.P.select == 0 || C.P.select == 1);
+  if (C.tape && C.P.compress) fail_all(C, CATN_EINVAL);   // no adjoint of the compress sweeps
   if (buckets) {
     // select_edge_init!: all node ids
     for (int k = 1 + T.rank(); k <= C.n; k += T.size()) C.list[k - 1] = k;
@@ -1618,6 +1777,20 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
     if (z < 0) nneg += 1.0;
     if (z == 0) nzero += 1.0;
   }
+  if (C.tape) {
+    // every thread walks the nodes alike so that the records are uniform
+    for (int k = 1; k <= C.n; ++k) {
+      NodeHdr h = C.node[k];
+      if (h.nsites != 1 || sref(C, k, 1).d != 1) continue;
+      SiteRef s = sref(C, k, 1);
+      const double* x = dptr(C, s.off);
+      double z = 0.0;
+      for (long long e = 0; e < (long long)s.dl * s.dr; ++e) z += x[e];
+      TapeRec r = trec(OP_LOGZ);
+      r.a[0] = s.dl * s.dr; r.o[0] = s.off; r.v[0] = z;
+      tape_push(C, r);
+    }
+  }
   lsum = T.sum(lsum);
   nneg = T.sum(nneg);
   nzero = T.sum(nzero);
@@ -1677,6 +1850,10 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.multigraph = 1;
   C.trace = nullptr;
   C.trace_cap = 0;
+  C.tape = 0;
+  C.rec = nullptr;
+  C.nrec = C.rcap = C.gshift = 0;
+  C.heap_first = 0;
   return C;
 }
 
@@ -1721,6 +1898,7 @@ CATN_HDI inline void load_instance(Ctx& C, const InstDesc& D, const long long* i
     }
     if (!heap_reserve(C, total)) return;
     const long long first = C.hb;
+    C.heap_first = first;
     C.hb += total;
     if (C.hb - C.h_lo0 > C.h_peak) C.h_peak = C.hb - C.h_lo0;
     if (T.leader()) {

@@ -11,6 +11,17 @@
 
 namespace catn {
 
+// Parameters of one Ising instance, kept on the host for the chain rule of
+// the adjoint (ising_param_grad).
+struct IsingSpec {
+  int n = 0;
+  std::vector<int> edges;
+  std::vector<double> w, h;
+  double beta = 0.0;
+  int pos1 = 0, val1 = 0, pos2 = 0, val2 = 0;
+  int inst = -1;   // index into Image::desc
+};
+
 struct Image {
   std::vector<long long> i64;
   std::vector<int> i32;
@@ -20,6 +31,7 @@ struct Image {
   int emax = 0;       // largest real-edge count
   int smax = 0;       // largest per-node site / neighbour count at load
   long long trace_total = 0;
+  std::vector<IsingSpec> ising;   // Ising instances, in the order added
 
   // Network in MPS form.  Returns an error message or "".
   std::string add_mps(const catn_params& P, int n, const int* site_counts, const int* nbr_counts,
@@ -219,7 +231,19 @@ struct Image {
       }
       for (int v : nbr[k]) nb.push_back(v);
     }
-    return add_mps(P, n, sc.data(), nc.data(), cn.data(), dims.data(), data.data(), nb.data(), trace_cap);
+    std::string err = add_mps(P, n, sc.data(), nc.data(), cn.data(), dims.data(), data.data(), nb.data(), trace_cap);
+    if (err.empty()) {
+      IsingSpec sp;
+      sp.n = n;
+      sp.edges.assign(edges, edges + 2 * n_edges);
+      sp.w.assign(w, w + n_edges);
+      sp.h.assign(h, h + n);
+      sp.beta = beta;
+      sp.pos1 = pos1; sp.val1 = val1; sp.pos2 = pos2; sp.val2 = val2;
+      sp.inst = (int)desc.size() - 1;
+      ising.push_back(sp);
+    }
+    return err;
   }
 
  private:
@@ -233,6 +257,99 @@ struct Image {
     if (edges > emax) emax = edges;
   }
 };
+
+// d lnZ / d w_e and d lnZ / d h_k from the gradients of the sites that
+// add_ising built (`gsite`: same order and layout as its data), by the chain
+// rule through B = exp(beta w s_i s_j) on the first endpoint's site and the
+// field factors exp(beta h s) folded into each node's first (or leaf) site.
+// Follows add_ising's construction step by step.
+inline void ising_param_grad(int n, int n_edges, const int* edges, const double* w, const double* h, double beta,
+                             int pos1, int val1, int pos2, int val2, const double* gsite, double* dw, double* dh) {
+  std::vector<int> degree(n + 1, 0);
+  for (int e = 0; e < n_edges; ++e) {
+    degree[edges[2 * e]] += 1;
+    degree[edges[2 * e + 1]] += 1;
+  }
+  // one entry per site, in the order add_ising pushes them per node
+  struct SiteInfo { int edge, layout; bool isB; double s[2], other[2], f[2]; };   // layout: 0 leaf 1 first 2 last 3 interior
+  std::vector<std::vector<SiteInfo>> sites(n + 1);
+  auto spins = [&](int k, double s[2]) {
+    s[0] = 1.0;
+    s[1] = -1.0;
+    if (k == pos1) s[val1 - 1] = 0.0;
+    else if (k == pos2) s[val2 - 1] = 0.0;
+  };
+  auto layout_of = [&](int k) {
+    if (degree[k] == 1) return 0;
+    if (sites[k].empty()) return 1;
+    if ((int)sites[k].size() == degree[k] - 1) return 2;
+    return 3;
+  };
+  for (int e = 0; e < n_edges; ++e) {
+    const int i = edges[2 * e], j = edges[2 * e + 1];
+    SiteInfo a, b;
+    spins(i, a.s);
+    spins(j, a.other);
+    a.edge = e; a.isB = true; a.layout = layout_of(i);
+    for (int q = 0; q < 2; ++q) a.f[q] = std::exp(beta * h[i - 1] * a.s[q]);
+    sites[i].push_back(a);
+    spins(j, b.s);
+    spins(i, b.other);
+    b.edge = e; b.isB = false; b.layout = layout_of(j);
+    for (int q = 0; q < 2; ++q) b.f[q] = std::exp(beta * h[j - 1] * b.s[q]);
+    sites[j].push_back(b);
+  }
+  for (int e = 0; e < n_edges; ++e) dw[e] = 0.0;
+  for (int k = 0; k < n; ++k) dh[k] = 0.0;
+  long long off = 0;
+  for (int k = 1; k <= n; ++k) {
+    if (degree[k] == 0) {
+      dh[k - 1] += gsite[off] * beta * (std::exp(beta * h[k - 1]) - std::exp(-beta * h[k - 1]));
+      off += 1;
+      continue;
+    }
+    for (const SiteInfo& si : sites[k]) {
+      const int e = si.edge;
+      double Q[2][2];
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          Q[a][b] = si.isB ? std::exp(beta * w[e] * (si.s[a] * si.other[b])) : (a == b ? 1.0 : 0.0);
+      double Qb[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, fb[2] = {0.0, 0.0};
+      const double* G = gsite + off;
+      if (si.layout == 0) {          // v[b] = sum_a f_a Q[a][b]
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) {
+            Qb[a][b] = G[b] * si.f[a];
+            fb[a] += G[b] * Q[a][b];
+          }
+        off += 2;
+      } else if (si.layout == 1) {   // v[a + 2b] = f_b Q[b][a]
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) {
+            Qb[b][a] = G[a + 2 * b] * si.f[b];
+            fb[b] += G[a + 2 * b] * Q[b][a];
+          }
+        off += 4;
+      } else if (si.layout == 2) {   // v[a + 2b] = Q[a][b]
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) Qb[a][b] = G[a + 2 * b];
+        off += 4;
+      } else {                       // v[a + 2 sp + 4 a] = Q[a][sp]
+        for (int a = 0; a < 2; ++a)
+          for (int sp = 0; sp < 2; ++sp) Qb[a][sp] = G[a + 2 * sp + 4 * a];
+        off += 8;
+      }
+      if (si.isB) {
+        double g = 0.0;
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b) g += Qb[a][b] * beta * si.s[a] * si.other[b] * Q[a][b];
+        dw[e] += g;
+      }
+      if (si.layout <= 1)
+        for (int a = 0; a < 2; ++a) dh[k - 1] += fb[a] * beta * si.s[a] * si.f[a];
+    }
+  }
+}
 
 // Site / neighbour capacity per node: the largest order a node can reach
 // is bounded by its initial order plus everything it can absorb.

@@ -63,13 +63,13 @@ CATN_HD MOp colmajor(double* p, long long ld) { return mop(p, rows_plain(), cols
 CATN_HD MOp transposed(double* p, long long ld) { return mop(p, cols_plain(ld), rows_plain()); }
 
 // ---------------------------------------------------------------------------
-// GEMM: C(M x N) = A(M x K) * B(K x N), overwrite.
+// GEMM: C(M x N) = A(M x K) * B(K x N), overwrite (or C += A * B with accum).
 // ---------------------------------------------------------------------------
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
 constexpr int GEMM_STAGE_BYTES = (GEMM_BM + GEMM_BN) * GEMM_BK * 8;
 
 CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, const MOp& A,
-                          const MOp& B, const MOp& C) {
+                          const MOp& B, const MOp& C, bool accum = false) {
   if (M <= 0 || N <= 0) return;
 #if CATN_DEVICE_PASS
   if (T.size() == 256 && T.stage_bytes >= GEMM_STAGE_BYTES && M * N >= 256) {
@@ -117,7 +117,7 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
 #pragma unroll
           for (int y = 0; y < 4; ++y) {
             long long c = n0 + tx * 4 + y;
-            if (c < N) C.ref(r, c) = acc[x][y];
+            if (c < N) C.ref(r, c) = accum ? C.ref(r, c) + acc[x][y] : acc[x][y];
           }
         }
       }
@@ -132,7 +132,7 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
     divmod(e, M, &r, &c);
     double s = 0.0;
     for (long long k = 0; k < K; ++k) s = fma(A.ld(r, k), B.ld(k, c), s);
-    C.ref(r, c) = s;
+    C.ref(r, c) = accum ? C.ref(r, c) + s : s;
   }
   T.sync();
 }

@@ -7,6 +7,13 @@ reference's runs in Julia), and ``contraction`` contracts it on the device.
 definition (ising.jl:263-339) but contract all 1+2n or 1+4|E| pinned
 networks in ONE persistent kernel launch instead of a host loop.
 ``IsingBatch`` is the batched entry point (many instances, one launch).
+
+``gradient`` (and ``method="adjoint"`` of the two observables) replaces the
+pinning loops with the device adjoint: one taped forward contraction and one
+backward pass give d lnZ / d w_e = beta <s_i s_j> and d lnZ / d h_k =
+beta <s_k> for every edge and spin at once (no reference counterpart; the
+reference only has pinning).  ``IsingLnZ`` wraps it as a
+``torch.autograd.Function``.
 """
 import ctypes as ct
 
@@ -58,6 +65,22 @@ class IsingNetwork(TensorNetwork):
 def ising_network(n, edges, weights, fields, beta, **kw):
     """``ising_network`` (ising.jl:20-227)."""
     return IsingNetwork(n, edges, weights, fields, beta, **kw)
+
+
+def gradient(tn):
+    """``(lnZ, dlnZ_dw, dlnZ_dh)`` of an Ising network from one forward
+    contraction with a tape plus one backward pass, both on the device.
+    ``dlnZ_dw[e] = beta <s_i s_j>``, ``dlnZ_dh[k] = beta <s_k>`` (exact up to
+    the contraction's own truncations).  Does not consume ``tn``."""
+    if not isinstance(tn, IsingNetwork):
+        raise TypeError("gradient: networks built by ising_network only")
+    dev = tn._ensure_device()
+    lib = L.load()
+    res = L.Result()
+    dw = np.zeros(max(tn.edges.shape[0], 1))
+    dh = np.zeros(tn.n)
+    L.check(lib, lib.catn_ising_grad(dev.handle, ct.byref(res), L.ptr(dw), L.ptr(dh), 0))
+    return res.lnZ, dw[:tn.edges.shape[0]], dh
 
 
 def free_energy(tn):
@@ -132,6 +155,26 @@ class IsingBatch:
         L.check(self.lib, self.lib.catn_batch_run(self.handle, self.results))
         return self.results
 
+    def grad_launch(self, stream=None):
+        """Upload and start the gradient run of every instance (one launch)."""
+        L.check(self.lib, self.lib.catn_batch_grad_launch(self.handle, stream))
+
+    def grad_fetch(self, stream=None):
+        """Results and gradients of the last gradient run: (results, dlnZ_dw,
+        dlnZ_dh), the gradients concatenated per instance."""
+        a = self._arrays
+        dw = np.zeros(max(int(a[2][-1]), 1))
+        dh = np.zeros(int(a[1][-1]))
+        L.check(self.lib, self.lib.catn_batch_grad_results(self.handle, self.results, L.ptr(dw), L.ptr(dh), stream))
+        return self.results, dw[:int(a[2][-1])], dh
+
+    def grad(self):
+        """Gradient run of every instance; per instance (lnZ, dlnZ_dw, dlnZ_dh)."""
+        self.grad_launch()
+        res, dw, dh = self.grad_fetch()
+        a = self._arrays
+        return [(res[q].lnZ, dw[a[2][q]:a[2][q + 1]], dh[a[1][q]:a[1][q + 1]]) for q in range(self.size)]
+
     def lnZ(self):
         return np.array([r.lnZ for r in self.results])
 
@@ -152,16 +195,30 @@ def _pinned_batch(n, edges, weights, fields, beta, pins, **kw):
     return b.lnZ()
 
 
-def magnetization(n, edges, weights, fields, beta, **kw):
-    """<s_k> by spin pinning (ising.jl:263-290): 1 + 2n contractions, all in one launch."""
+def magnetization(n, edges, weights, fields, beta, method="pinning", **kw):
+    """<s_k> by spin pinning (ising.jl:263-290): 1 + 2n contractions, all in
+    one launch; ``method="adjoint"`` gives d lnZ / d h / beta from one
+    gradient run instead."""
+    if method == "adjoint":
+        _, _, dh = gradient(ising_network(n, edges, weights, fields, beta, **kw))
+        return dh / beta
+    if method != "pinning":
+        raise ValueError("method must be 'pinning' or 'adjoint'")
     pins = [(0, 0, 0, 0)] + [(k, v, 0, 0) for k in range(1, n + 1) for v in (1, 2)]
     lz = _pinned_batch(n, edges, weights, fields, beta, pins, **kw)
     p = np.exp(lz[1:] - lz[0]).reshape(n, 2)
     return p[:, 1] - p[:, 0]
 
 
-def correlation(n, edges, weights, fields, beta, **kw):
-    """<s_i s_j> per edge by pinning both ends (ising.jl:309-339): 1 + 4|E| contractions, one launch."""
+def correlation(n, edges, weights, fields, beta, method="pinning", **kw):
+    """<s_i s_j> per edge by pinning both ends (ising.jl:309-339): 1 + 4|E|
+    contractions, one launch; ``method="adjoint"`` gives d lnZ / d w / beta
+    from one gradient run instead."""
+    if method == "adjoint":
+        _, dw, _ = gradient(ising_network(n, edges, weights, fields, beta, **kw))
+        return dw / beta
+    if method != "pinning":
+        raise ValueError("method must be 'pinning' or 'adjoint'")
     pins = [(0, 0, 0, 0)]
     for (m, nn) in edges:
         for v1 in (1, 2):
@@ -170,3 +227,39 @@ def correlation(n, edges, weights, fields, beta, **kw):
     lz = _pinned_batch(n, edges, weights, fields, beta, pins, **kw)
     p = np.exp(lz[1:] - lz[0]).reshape(len(edges), 2, 2)
     return p[:, 0, 0] - p[:, 0, 1] - p[:, 1, 0] + p[:, 1, 1]
+
+
+def _make_autograd():
+    import torch
+
+    class IsingLnZ(torch.autograd.Function):
+        """lnZ(weights, fields) of ``ising_network(n, edges, weights, fields,
+        beta, **params)`` as a differentiable function: forward and backward
+        both come from one device gradient run (the Python counterpart of the
+        ChainRulesCore ``rrule`` a Julia caller would attach)."""
+
+        @staticmethod
+        def forward(ctx, weights, fields, n, edges, beta, params):
+            lnZ, dw, dh = gradient(ising_network(n, edges, weights.detach().cpu().double().numpy(),
+                                                 fields.detach().cpu().double().numpy(), beta, **params))
+            ctx.save_for_backward(torch.from_numpy(dw).to(weights), torch.from_numpy(dh).to(fields))
+            return weights.new_tensor(lnZ)
+
+        @staticmethod
+        def backward(ctx, g):
+            dw, dh = ctx.saved_tensors
+            return g * dw, g * dh, None, None, None, None
+
+    return IsingLnZ
+
+
+def ising_lnZ(weights, fields, n, edges, beta, **params):
+    """Differentiable lnZ (torch tensors in, torch scalar out); see
+    ``IsingLnZ``."""
+    global IsingLnZ
+    if IsingLnZ is None:
+        IsingLnZ = _make_autograd()
+    return IsingLnZ.apply(weights, fields, n, edges, beta, params)
+
+
+IsingLnZ = None

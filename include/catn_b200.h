@@ -197,6 +197,32 @@ int32_t catn_batch_slots(const catn_batch* b);
 int64_t catn_batch_input_bytes(const catn_batch* b);
 catn_status catn_batch_destroy(catn_batch* b);
 
+/* ---- adjoint (gradient of lnZ) ------------------------------------------
+ * No reference counterpart: the reference obtains <s_k> and <s_i s_j> by
+ * pinning, 1 + 2n and 1 + 4|E| full contractions (magnetization /
+ * correlation, src/ising.jl:263-339).  Here one forward contraction records
+ * a tape on the device and one backward pass gives
+ *   dlnZ_dw[e] = d lnZ / d w_e  (= beta <s_i s_j> for edge e = (i, j)),
+ *   dlnZ_dh[k] = d lnZ / d h_k  (= beta <s_k>),
+ * exact up to the truncations of the contraction itself (the truncated part
+ * of every SVD, and kept values below 1e-10 of the largest, count as zero in
+ * the backward pass).  Networks from catn_ising_create only; compress = 1 is
+ * rejected (CATN_EINVAL).  The gradient run allocates its own device slots
+ * (2.5x the forward arena: tape, append-only heap and its shadow) on the
+ * first call and keeps them until destroy.
+ *
+ * ckpt_interval must be 0: the tape of the whole contraction is kept on the
+ * device; checkpointed recomputation is not implemented (CATN_EINVAL). */
+catn_status catn_ising_grad(catn_net* net, catn_result* res, double* dlnZ_dw, double* dlnZ_dh,
+                            int32_t ckpt_interval);
+/* Every instance of a batch in one persistent launch (inputs uploaded by the
+ * call); results and gradients are read back by catn_batch_grad_results,
+ * dlnZ_dw / dlnZ_dh concatenated per instance in the edge_off / node_off
+ * order of catn_ising_batch_create. */
+catn_status catn_batch_grad_launch(catn_batch* b, void* stream);
+catn_status catn_batch_grad_results(catn_batch* b, catn_result* results, double* dlnZ_dw, double* dlnZ_dh,
+                                    void* stream);
+
 /* Thread-local message of the last failure (always NUL-terminated). */
 size_t catn_last_error(char* buf, size_t cap);
 

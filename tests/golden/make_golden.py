@@ -12,6 +12,12 @@ Fixtures (seeded synthetic inputs with the workload shapes):
   rrg_sample.json        n=24 random 3-regular +-1 spin glass, beta in
                          {0.5,1,1.5}, Dmax 8, chi 32 (small stand-in for the
                          n=200 configuration): oracle lnZ/err/trace
+  rrg200.json            the n=200 random 3-regular +-1 spin glass itself
+                         (300 edges, h~N(0,0.01), beta in {0.5,1,1.5}, Dmax 32,
+                         chi 128): oracle lnZ/err/psi/maxdim/trace (about 35 s
+                         of oracle time per beta, hence frozen here)
+
+    python tests/golden/make_golden.py [name ...]   # regenerate only these
 The trace row format is the device's (see include/catn_b200.h).
 """
 import json
@@ -56,7 +62,23 @@ def spinglass(count, seed):
     return out
 
 
+def rrg200():
+    rng = np.random.default_rng(200)
+    e = X.random_regular_graph(200, 3, rng)
+    w = rng.choice([-1.0, 1.0], size=len(e)).tolist()
+    h = rng.normal(0, 0.1, 200).tolist()
+    d = dict(n=200, edges=e, weights=w, fields=h, params=dict(Dmax=32, chi=128, cutoff=1e-15), betas=[0.5, 1.0, 1.5])
+    d["oracle"] = [run(200, e, w, h, b, Dmax=32, chi=128) for b in d["betas"]]
+    json.dump(d, open(os.path.join(HERE, "rrg200.json"), "w"))
+
+
 def main():
+    only = set(sys.argv[1:])
+    if only:
+        if "rrg200" in only:
+            rrg200()
+        print("golden fixtures written:", " ".join(sorted(only)))
+        return
     e = X.square_edges(8)
     w, h = [1.0] * len(e), [0.0] * 64
     c1 = dict(n=64, edges=e, weights=w, fields=h, beta=0.44, params=dict(Dmax=20, chi=200, cutoff=1e-15))
@@ -80,6 +102,7 @@ def main():
     rr["oracle"] = [run(24, e, w, h, b, Dmax=8, chi=32) for b in rr["betas"]]
     rr["exact_lnZ"] = [X.brute_lnZ(24, e, w, h, b) for b in rr["betas"]]
     json.dump(rr, open(os.path.join(HERE, "rrg_sample.json"), "w"))
+    rrg200()
     print("golden fixtures written")
 
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <vector>
 #include "../../catn.jl_b200/csrc/engine.cuh"
+#include "../../catn.jl_b200/csrc/adjoint.cuh"
 #include "../../catn.jl_b200/csrc/host_image.h"
 
 using namespace catn;
@@ -43,6 +44,34 @@ int catn_hostcheck_ising(const catn_params* p, int n, int n_edges, const int* ed
   std::string e = im.add_ising(*p, n, n_edges, edges, w, h, beta, pos1, val1, pos2, val2, trace_cap);
   if (!e.empty()) return CATN_EINVAL;
   return run_image(im, arena_bytes, res, trace);
+}
+
+// Gradient run (tape + adjoint) of one Ising network: lnZ in res, d lnZ/d w
+// and d lnZ/d h through the host chain rule.
+int catn_hostcheck_ising_grad(const catn_params* p, int n, int n_edges, const int* edges, const double* w,
+                              const double* h, double beta, int pos1, int val1, int pos2, int val2,
+                              long long arena_bytes, catn_result* res, double* dw, double* dh) {
+  Image im;
+  std::string e = im.add_ising(*p, n, n_edges, edges, w, h, beta, pos1, val1, pos2, val2, 0);
+  if (!e.empty()) return CATN_EINVAL;
+  SlotLayout L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
+  std::vector<char> slot((size_t)L.slot_bytes + 256);
+  char* sp = (char*)(((uintptr_t)slot.data() + 255) & ~(uintptr_t)255);
+  std::vector<double> red(64);
+  Team T;
+  T.red = red.data();
+  T.stage = nullptr;
+  T.stage_bytes = 0;
+  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  if (const char* ev = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(ev);
+  std::vector<double> sws((size_t)(sws_doubles > 0 ? sws_doubles : 1));
+  std::vector<double> gimg(im.dat.size() + 1, 0.0);
+  run_instance_grad(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, gimg.data(),
+                    sws.data(), sws_doubles);
+  if (res->status == CATN_OK)
+    ising_param_grad(n, n_edges, edges, w, h, beta, pos1, val1, pos2, val2, gimg.data() + im.desc[0].data_off, dw,
+                     dh);
+  return res->status;
 }
 
 int catn_hostcheck_dense(const catn_params* p, int n, const int* ndims, const long long* dims,

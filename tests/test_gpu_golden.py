@@ -1,0 +1,73 @@
+"""GPU parity against the committed golden fixtures (tests/golden/*.json,
+made by tests/golden/make_golden.py from the oracle and the exact checkers):
+the configurations whose oracle runs are too slow to repeat at test time.
+
+Bar: the per-step integer trace identical to the oracle's, |dlnZ|/n <= 1e-10
+against the FP64 oracle, psi and maxdim_intermediate equal, and rtol 1e-9
+against exact lnZ where the fixture holds one (test/test_ising.jl:19,39).
+"""
+import json
+import os
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _load(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+def _contract(catn, d, beta, params):
+    tn = catn.ising_network(d["n"], [tuple(e) for e in d["edges"]], d["weights"], d["fields"], beta, **params)
+    lnZ, err, psi = catn.contraction(tn, trace=True)
+    rows = [[int(x) for x in r[:7]] for r in tn.trace]
+    return lnZ, err, psi, tn.maxdim_intermediate, rows
+
+
+def _check(got, ref, n):
+    lnZ, err, psi, maxdim, rows = got
+    assert rows == ref["trace"]
+    assert abs(lnZ - ref["lnZ"]) / n <= 1e-10
+    assert abs(err - ref["err"]) <= 1e-12 + 1e-6 * abs(ref["err"])
+    assert psi == ref["psi"]
+    assert maxdim == ref["maxdim"]
+
+
+def test_config1_ferromagnet_golden(catn):
+    d = _load("config1_ferro8.json")
+    got = _contract(catn, d, d["beta"], d["params"])
+    _check(got, d["oracle"], d["n"])
+    assert got[0] == pytest.approx(d["exact_lnZ"], rel=1e-9)
+
+
+# The n=200 configuration ends in full-rank 4096 x 4096 swap SVDs, which one
+# CTA (the engine's unit of work per network) takes tens of minutes over; it
+# runs only on request until large SVDs are spread over the whole GPU.
+LONG = os.environ.get("CATN_LONG_GPU_TESTS") == "1"
+
+
+@pytest.mark.parametrize("name", ["rrg_sample.json",
+                                  pytest.param("rrg200.json", marks=pytest.mark.skipif(
+                                      not LONG, reason="single-CTA 4096^2 SVDs: set CATN_LONG_GPU_TESTS=1"))])
+def test_random_regular_spin_glass_golden(catn, name):
+    """The n=200 random 3-regular +-1 configuration (and its n=24 stand-in)
+    at beta 0.5, 1.0, 1.5."""
+    d = _load(name)
+    for k, beta in enumerate(d["betas"]):
+        _check(_contract(catn, d, beta, d["params"]), d["oracle"][k], d["n"])
+        if "exact_lnZ" in d and d["params"]["Dmax"] < 0:
+            assert d["oracle"][k]["lnZ"] == pytest.approx(d["exact_lnZ"][k], rel=1e-9)
+
+
+def test_spinglass_workload_sample_golden(catn):
+    """12 instances of the batched workload, one network at a time."""
+    d = _load("spinglass_sample.json")
+    for inst in d["instances"]:
+        got = _contract(catn, inst, inst["beta"], d["params"])
+        _check(got, inst["oracle"], inst["n"])
+        if "exact_lnZ" in inst:
+            assert abs(got[0] - inst["exact_lnZ"]) / inst["n"] <= 1e-6
