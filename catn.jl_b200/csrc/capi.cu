@@ -272,12 +272,29 @@ catn_status catn_ising_create(const catn_params* p, int32_t n, int32_t n_edges, 
   return net_finish(net, arena_bytes, out);
 }
 
+catn_status catn_braket_create(const catn_params* p, int32_t n, const int32_t* ndims, const int64_t* dims,
+                               const double* data, const int32_t* labels, int64_t arena_bytes, catn_net** out) {
+  if (catn_status s = check_params(p)) return s;
+  if (!out || !ndims || !dims || !data || !labels) return fail(CATN_EINVAL, "NULL argument");
+  catn_net* net = new catn_net();
+  long long legs = 0;
+  for (int k = 0; k < n; ++k) legs += ndims[k];
+  const int tc = p->trace ? (int)(legs + 16) : 0;
+  std::string e = net->im.add_braket(*p, n, ndims, (const long long*)dims, data, labels, tc);
+  if (!e.empty()) { delete net; return fail(CATN_EINVAL, e); }
+  return net_finish(net, arena_bytes, out);
+}
+
 catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32_t trace_cap) {
   if (!net || !res) return fail(CATN_EINVAL, "NULL argument");
   if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
   cudaStream_t st = 0;
   if (catn_status s = upload(net->R, st)) return s;
-  if (catn_status s = launch(net->R, st)) return s;
+  if (net->im.desc[0].kind == 2) {
+    if (catn_status s = braket_launch(net->R, st)) return s;
+  } else if (catn_status s = launch(net->R, st)) {
+    return s;
+  }
   CUDA_TRY(cudaMemcpyAsync(res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   net->contracted = true;

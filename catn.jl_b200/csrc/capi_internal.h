@@ -1,6 +1,7 @@
 // Host-side helpers shared by the translation units of libcatn_b200
 // (capi.cu: the persistent-kernel entry points; capi_static.cu: the
-// allocation-free entry point; capi_grad.cu: the adjoint).  Each unit
+// allocation-free entry point; capi_grad.cu: the adjoint; capi_braket.cu:
+// the BraKet kernel).  Each unit
 // compiles the device engine on its own, so the register allocation of one
 // kernel's call tree never depends on another kernel that shares the
 // engine's out-of-line routines.
@@ -70,6 +71,8 @@ catn_status upload(DeviceRun& R, cudaStream_t st);
 long long default_arena(long long a, const catn_params& p);
 // Frees a gradient run (capi_grad.cu).
 void grad_release(GradRun* g);
+// Runs the BraKet kernel over a prepared run (capi_braket.cu).
+catn_status braket_launch(DeviceRun& R, cudaStream_t st);
 
 }  // namespace catn_capi
 

@@ -46,7 +46,8 @@ enum {
 struct InstDesc {
   catn_params P;
   int n;            // nodes
-  int kind;         // 0 = MPS form, 1 = dense tensors (raw2mps on device)
+  int kind;         // 0 = MPS form, 1 = dense tensors (raw2mps on device),
+                    // 2 = BraKet <psi|psi> (braket_node on device)
   long long hdr_off;   // int64 image: per node 4 words
                        //   MPS:   nsites, nnbr, cano, 0
                        //   dense: ndims, nnbr(=ndims), 0, 0
@@ -59,6 +60,9 @@ struct InstDesc {
   int multigraph;      // some node lists the same neighbour twice
   int pad2;
   long long trace_off; // int32 offset into the trace buffer
+  long long edge_off;  // BraKet (kind 2): int32 image, edge pairs in processing order
+  int n_edges;
+  int pad3;
 };
 
 // Byte layout of one CTA slot (control state + arena).

@@ -142,6 +142,139 @@ struct Image {
     return "";
   }
 
+  // braket_network (src/braket.jl:369-508) for real tensors: `labels` holds
+  // one positive label per axis, tensors in order.  A label on one tensor is
+  // that tensor's physical index (exactly one per tensor), on two tensors a
+  // virtual bond; cyclic bond graphs are rejected.  Per node the image holds
+  // (deg, d), the virtual dims, the ket neighbours in axis order and the
+  // data Tk (virtual axes, then physical) followed by Tbra (physical, then
+  // virtual); the edges follow the first appearance of their labels.
+  std::string add_braket(const catn_params& P, int n, const int* ndims, const long long* dims, const double* data,
+                         const int* labels, int trace_cap) {
+    if (n < 1) return "braket_network: no tensors";
+    std::vector<long long> aoff(n + 1, 0), doff(n + 1, 0);
+    for (int k = 0; k < n; ++k) {
+      if (ndims[k] < 1) return "braket_network: every tensor needs at least one index";
+      aoff[k + 1] = aoff[k] + ndims[k];
+      long long tot = 1;
+      for (int q = 0; q < ndims[k]; ++q) {
+        if (dims[aoff[k] + q] < 1) return "tensor dimensions must be >= 1";
+        tot *= dims[aoff[k] + q];
+      }
+      doff[k + 1] = doff[k] + tot;
+    }
+    // label -> owners (node ids), in first-appearance order
+    std::vector<int> order;
+    std::vector<std::vector<int>> owners;
+    std::vector<int> label_of;   // index into owners by label position
+    auto find_label = [&](int l) {
+      for (size_t q = 0; q < order.size(); ++q)
+        if (order[q] == l) return (int)q;
+      return -1;
+    };
+    for (int k = 0; k < n; ++k)
+      for (int q = 0; q < ndims[k]; ++q) {
+        const int l = labels[aoff[k] + q];
+        int x = find_label(l);
+        if (x < 0) {
+          order.push_back(l);
+          owners.push_back({});
+          x = (int)order.size() - 1;
+        }
+        owners[x].push_back(k + 1);
+        label_of.push_back(x);
+      }
+    for (size_t x = 0; x < order.size(); ++x)
+      if (owners[x].size() > 2)
+        return "braket_network: label " + std::to_string(order[x]) + " appears " +
+               std::to_string(owners[x].size()) + " times (expected 1 or 2)";
+    for (int k = 0; k < n; ++k) {
+      int nphys = 0;
+      for (int q = 0; q < ndims[k]; ++q) nphys += owners[label_of[aoff[k] + q]].size() == 1;
+      if (nphys != 1)
+        return "braket_network: tensor " + std::to_string(k + 1) + " has " + std::to_string(nphys) +
+               " physical (open) labels, expected 1";
+    }
+    std::vector<int> parent(n + 1);
+    for (int k = 0; k <= n; ++k) parent[k] = k;
+    auto root = [&](int x) {
+      while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; }
+      return x;
+    };
+    std::vector<int> epairs;
+    for (size_t x = 0; x < order.size(); ++x) {
+      if (owners[x].size() != 2) continue;
+      const int a = root(owners[x][0]), b = root(owners[x][1]);
+      if (a == b)
+        return "braket_network: virtual-bond graph contains a cycle — cyclic graphs are not supported in v1";
+      parent[a] = b;
+      epairs.push_back(owners[x][0]);
+      epairs.push_back(owners[x][1]);
+    }
+    InstDesc D;
+    std::memset(&D, 0, sizeof(D));
+    D.P = P;
+    D.n = n;
+    D.kind = 2;
+    D.hdr_off = (long long)i64.size();
+    std::vector<int> phys(n);
+    for (int k = 0; k < n; ++k) {
+      for (int q = 0; q < ndims[k]; ++q)
+        if (owners[label_of[aoff[k] + q]].size() == 1) phys[k] = q;
+      i64.push_back(ndims[k] - 1);
+      i64.push_back(dims[aoff[k] + phys[k]]);
+      i64.push_back(0);
+      i64.push_back(0);
+      if (2 * (ndims[k] - 1) > smax) smax = 2 * (ndims[k] - 1);
+    }
+    D.dim_off = (long long)i64.size();
+    for (int k = 0; k < n; ++k)
+      for (int q = 0; q < ndims[k]; ++q)
+        if (q != phys[k]) i64.push_back(dims[aoff[k] + q]);
+    D.nbr_off = (long long)i32.size();
+    for (int k = 0; k < n; ++k)
+      for (int q = 0; q < ndims[k]; ++q) {
+        if (q == phys[k]) continue;
+        const std::vector<int>& o = owners[label_of[aoff[k] + q]];
+        i32.push_back(o[0] == k + 1 ? o[1] : o[0]);
+      }
+    D.edge_off = (long long)i32.size();
+    D.n_edges = (int)(epairs.size() / 2);
+    for (int v : epairs) i32.push_back(v);
+    D.data_off = (long long)dat.size();
+    for (int k = 0; k < n; ++k) {
+      const int nd = ndims[k];
+      const long long* dk = dims + aoff[k];
+      std::vector<long long> stride(nd, 1), perm;
+      for (int q = 1; q < nd; ++q) stride[q] = stride[q - 1] * dk[q - 1];
+      for (int q = 0; q < nd; ++q)
+        if (q != phys[k]) perm.push_back(q);
+      perm.push_back(phys[k]);
+      const long long tot = doff[k + 1] - doff[k];
+      const double* src = data + doff[k];
+      // Tk(i_perm0, .., i_perm(nd-1)) = Ti(...) and Tbra(p, v...) = Tk(v..., p)
+      std::vector<double> tk(tot), tb(tot);
+      std::vector<long long> idx(nd, 0);
+      const long long d = dk[phys[k]];
+      for (long long e = 0; e < tot; ++e) {
+        long long so = 0;
+        for (int q = 0; q < nd; ++q) so += idx[perm[q]] * stride[perm[q]];
+        tk[e] = src[so];
+        const long long pi = idx[perm[nd - 1]];
+        tb[pi + d * (e % (tot / d))] = src[so];
+        for (int q = 0; q < nd; ++q) {   // next multi-index in Tk order
+          if (++idx[perm[q]] < dk[perm[q]]) break;
+          idx[perm[q]] = 0;
+        }
+      }
+      dat.insert(dat.end(), tk.begin(), tk.end());
+      dat.insert(dat.end(), tb.begin(), tb.end());
+    }
+    D.data_len = (long long)dat.size() - D.data_off;
+    finish(D, n, D.n_edges + 1, trace_cap);
+    return "";
+  }
+
   // ising_network (src/ising.jl:20-227): one site per incident edge, B =
   // exp(beta w s_i s_j) on the first endpoint, identity on the second, field
   // folded into the first (or leaf) site, degree-0 spins as 2cosh(beta h).

@@ -197,6 +197,20 @@ int32_t catn_batch_slots(const catn_batch* b);
 int64_t catn_batch_input_bytes(const catn_batch* b);
 catn_status catn_batch_destroy(catn_batch* b);
 
+/* braket_network(tensors, ixs; chi, cutoff, norm_method, svdopt, swapopt)
+ * (src/braket.jl:369-508): the double-layer network <psi|psi> of a real ket
+ * state.  Tensor k has ndims[k] axes with sizes dims[...] (concatenated) and
+ * column-major data; labels[...] holds one positive label per axis.  A label
+ * on one tensor is its physical index (exactly one per tensor), a label on
+ * two tensors a virtual bond; a cyclic bond graph is rejected (CATN_EINVAL,
+ * as the reference errors).  Contract it with catn_contract: lnZ = log of
+ * <psi|psi> up to psi, err = discarded weight, maxdim = largest leg seen.
+ * Only p->chi, cutoff, norm_method and svdopt are used.  The edges are taken
+ * in the order their labels first appear (the reference iterates a Julia
+ * Dict there, src/braket.jl:489-497). */
+catn_status catn_braket_create(const catn_params* p, int32_t n, const int32_t* ndims, const int64_t* dims,
+                               const double* data, const int32_t* labels, int64_t arena_bytes, catn_net** out);
+
 /* ---- adjoint (gradient of lnZ) ------------------------------------------
  * No reference counterpart: the reference obtains <s_k> and <s_i s_j> by
  * pinning, 1 + 2n and 1 + 4|E| full contractions (magnetization /

@@ -7,6 +7,7 @@
 #include <vector>
 #include "../../catn.jl_b200/csrc/engine.cuh"
 #include "../../catn.jl_b200/csrc/adjoint.cuh"
+#include "../../catn.jl_b200/csrc/braket.cuh"
 #include "../../catn.jl_b200/csrc/host_image.h"
 
 using namespace catn;
@@ -71,6 +72,30 @@ int catn_hostcheck_ising_grad(const catn_params* p, int n, int n_edges, const in
   if (res->status == CATN_OK)
     ising_param_grad(n, n_edges, edges, w, h, beta, pos1, val1, pos2, val2, gimg.data() + im.desc[0].data_off, dw,
                      dh);
+  return res->status;
+}
+
+// BraKet network <psi|psi> (catn_braket_create's inputs).
+int catn_hostcheck_braket(const catn_params* p, int n, const int* ndims, const long long* dims, const double* data,
+                          const int* labels, long long arena_bytes, catn_result* res, int* trace, int trace_cap) {
+  Image im;
+  std::string e = im.add_braket(*p, n, ndims, dims, data, labels, trace_cap);
+  if (!e.empty()) return CATN_EINVAL;
+  SlotLayout L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
+  std::vector<char> slot((size_t)L.slot_bytes + 256);
+  char* sp = (char*)(((uintptr_t)slot.data() + 255) & ~(uintptr_t)255);
+  std::vector<double> red(64);
+  Team T;
+  T.red = red.data();
+  T.stage = nullptr;
+  T.stage_bytes = 0;
+  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  std::vector<double> sws((size_t)sws_doubles);
+  std::vector<int> tr((size_t)im.trace_total + 8);
+  run_instance_braket(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
+                      sws_doubles);
+  if (trace && im.desc[0].trace_cap > 0)
+    std::memcpy(trace, tr.data(), sizeof(int) * 8 * (size_t)std::min(trace_cap, im.desc[0].trace_cap));
   return res->status;
 }
 
