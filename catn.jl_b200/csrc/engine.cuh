@@ -358,8 +358,11 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
   double* tau2 = spush(C, r);
   double* nrm2 = spush(C, r);
   int* piv2 = (int*)spush(C, r / 2 + 1);
-  double* X2 = spush(C, r * r);
-  double* Vb2 = spush(C, r * r);
+  // the Jacobi pair lives in the shared-memory workspace when it fits (the
+  // large path leaves it unused): its rounds are latency-bound in global memory
+  const bool jsm = 2 * r * r <= C.sws_doubles;
+  double* X2 = jsm ? C.sws : spush(C, r * r);
+  double* Vb2 = jsm ? C.sws + r * r : spush(C, r * r);
   double* sig2 = spush(C, r);
   double* S2 = spush(C, r);
   int* perm2 = (int*)spush(C, r / 2 + 1);
@@ -380,7 +383,7 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
     X2[e] = (j <= i) ? Tt[j + i * nn] : 0.0;
   }
   T.sync();
-  int sweeps = jacobi_sweeps(T, X2, r, r, r, Vb2, 60);
+  int sweeps = jacobi_sweeps(T, X2, r, r, r, Vb2, 60, nrm2);
   if (sweeps < 0) fail_all(C, CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X2, r, r, r, sig2, S2, perm2);
@@ -487,8 +490,9 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   const long long r = qrcp_inplace(T, s.W, mm, nn, mm, tau, piv, nrm, stop);
   if (r < nn) return svd_truncated(C, s, r, tau, piv, t0);
   if (!s.smem) {
-    X = spush(C, nn * nn);
-    Vb = spush(C, nn * nn);
+    const bool jsm = 2 * nn * nn <= C.sws_doubles;   // Jacobi pair in shared memory when it fits
+    X = jsm ? C.sws : spush(C, nn * nn);
+    Vb = jsm ? C.sws + nn * nn : spush(C, nn * nn);
     Vt = spush(C, nn * nn);
     Ut = spush(C, mm * nn);
     sig = spush(C, nn);
@@ -502,7 +506,7 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
   }
   T.sync();
-  int sweeps = jacobi_sweeps(T, X, nn, nn, nn, Vb, 60);
+  int sweeps = jacobi_sweeps(T, X, nn, nn, nn, Vb, 60, nrm);
   if (sweeps < 0) fail_all(C, CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X, nn, nn, nn, sig, Sout, perm);

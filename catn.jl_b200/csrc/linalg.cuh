@@ -372,7 +372,7 @@ CATN_HD int rr_partner(int np, int r, int j) {
 }
 
 CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long long n, long long ldb,
-                                  double* V, int max_sweeps) {
+                                  double* V, int max_sweeps, double* nrm) {
   for (long long e = T.rank(); e < n * n; e += T.size()) V[e] = (e % n == e / n) ? 1.0 : 0.0;
   T.sync();
   if (n < 2) return 0;
@@ -387,42 +387,87 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
     for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] *= sc;
   T.sync();
   const long long np = (n % 2) ? n + 1 : n;
+  const long long npair = np / 2;
   const double tol = 2.220446049250313e-16 * (double)(m > 16 ? m : 16);
+  const int nw = T.nwarps();
   int result = -1;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    // squared column norms, recomputed each sweep; within a sweep a rotation
+    // by t updates them as |b_p|^2 -= t g, |b_q|^2 += t g (Rutishauser)
+    for (long long c = T.warp(); c < n; c += nw) {
+      const double* bc = B + c * ldb;
+      double s2 = 0.0;
+      for (long long i = T.lane(); i < m; i += T.wsize()) s2 = fma(bc[i], bc[i], s2);
+      s2 = T.wsum(s2);
+      if (T.lane() == 0) nrm[c] = s2;
+    }
+    T.sync();
     int rotated = 0;
     for (long long r = 0; r < np - 1; ++r) {
-      for (long long pi = T.warp(); pi < np / 2; pi += T.nwarps()) {
-        long long p, q;
-        rr_pair(np, r, pi, &p, &q);
-        if (p >= n || q >= n) continue;
-        double* bp = B + p * ldb;
-        double* bq = B + q * ldb;
-        double al = 0.0, be = 0.0, ga = 0.0;
+      // two pairs per warp in flight, so that their memory latencies overlap
+      for (long long pi = T.warp(); pi < npair; pi += 2 * nw) {
+        long long p0, q0, p1 = 0, q1 = 0;
+        rr_pair(np, r, pi, &p0, &q0);
+        const bool h1 = pi + nw < npair;
+        if (h1) rr_pair(np, r, pi + nw, &p1, &q1);
+        const bool a0 = p0 < n && q0 < n, a1 = h1 && p1 < n && q1 < n;
+        double* bp0 = B + p0 * ldb;
+        double* bq0 = B + q0 * ldb;
+        double* bp1 = B + p1 * ldb;
+        double* bq1 = B + q1 * ldb;
+        double g0 = 0.0, g1 = 0.0;
         for (long long i = T.lane(); i < m; i += T.wsize()) {
-          double x = bp[i], y = bq[i];
-          al = fma(x, x, al);
-          be = fma(y, y, be);
-          ga = fma(x, y, ga);
+          if (a0) g0 = fma(bp0[i], bq0[i], g0);
+          if (a1) g1 = fma(bp1[i], bq1[i], g1);
         }
-        al = T.wsum(al);
-        be = T.wsum(be);
-        ga = T.wsum(ga);
-        double c, s;
-        if (!jacobi_rotation(al, be, ga, tol, &c, &s)) continue;
+        g0 = T.wsum(g0);
+        g1 = T.wsum(g1);
+        double c0 = 1.0, s0 = 0.0, c1 = 1.0, s1 = 0.0;
+        const bool r0 = a0 && jacobi_rotation(nrm[p0], nrm[q0], g0, tol, &c0, &s0);
+        const bool r1 = a1 && jacobi_rotation(nrm[p1], nrm[q1], g1, tol, &c1, &s1);
+        if (!r0 && !r1) continue;
         rotated = 1;
         T.wsync();
         for (long long i = T.lane(); i < m; i += T.wsize()) {
-          double x = bp[i], y = bq[i];
-          bp[i] = c * x - s * y;
-          bq[i] = s * x + c * y;
+          if (r0) {
+            const double x = bp0[i], y = bq0[i];
+            bp0[i] = c0 * x - s0 * y;
+            bq0[i] = s0 * x + c0 * y;
+          }
+          if (r1) {
+            const double x = bp1[i], y = bq1[i];
+            bp1[i] = c1 * x - s1 * y;
+            bq1[i] = s1 * x + c1 * y;
+          }
         }
-        double* vp = V + p * n;
-        double* vq = V + q * n;
+        double* vp0 = V + p0 * n;
+        double* vq0 = V + q0 * n;
+        double* vp1 = V + p1 * n;
+        double* vq1 = V + q1 * n;
         for (long long i = T.lane(); i < n; i += T.wsize()) {
-          double x = vp[i], y = vq[i];
-          vp[i] = c * x - s * y;
-          vq[i] = s * x + c * y;
+          if (r0) {
+            const double x = vp0[i], y = vq0[i];
+            vp0[i] = c0 * x - s0 * y;
+            vq0[i] = s0 * x + c0 * y;
+          }
+          if (r1) {
+            const double x = vp1[i], y = vq1[i];
+            vp1[i] = c1 * x - s1 * y;
+            vq1[i] = s1 * x + c1 * y;
+          }
+        }
+        T.wsync();
+        if (T.lane() == 0) {
+          if (r0) {
+            const double t = s0 / c0;
+            nrm[p0] -= t * g0;
+            nrm[q0] += t * g0;
+          }
+          if (r1) {
+            const double t = s1 / c1;
+            nrm[p1] -= t * g1;
+            nrm[q1] += t * g1;
+          }
         }
         T.wsync();
       }
