@@ -59,11 +59,17 @@ catn_status check_params(const catn_params* p) {
 
 namespace {
 
+// Smallest column count whose Jacobi sweeps are opened to helper warps.
+constexpr int kSharedJacobiMinN = 96;
+
 // `order` lists instance ids by descending work estimate, so the longest
-// contractions start first (longest-processing-time scheduling).
+// contractions start first (longest-processing-time scheduling).  With a job
+// board, a CTA that finds the queue drained lends its warps to the large
+// SVDs of the CTAs still contracting (help_jacobi) until all are finished.
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
-    const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue) {
+    const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue,
+    JacobiJob* board) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -71,6 +77,11 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
   T.stage_bytes = GEMM_STAGE_BYTES;
   double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
+  JobLink jl;
+  jl.job = board ? board + blockIdx.x : nullptr;
+  jl.qhead = queue;
+  jl.ninst = ninst;
+  jl.min_n = kSharedJacobiMinN;
   for (;;) {
     long long inst = 0;
     if (threadIdx.x == 0) {
@@ -79,8 +90,11 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     }
     inst = T.bcast(inst);
     if (inst >= ninst) break;
-    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles);
+    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles,
+                 board ? &jl : nullptr);
+    if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
   }
+  if (board) help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
 }
 
 __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
@@ -152,7 +166,8 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   CUDA_TRY(cudaMalloc(&R.d_slots, (size_t)(R.L.slot_bytes * ns)));
   CUDA_TRY(cudaMalloc(&R.d_res, sizeof(catn_result) * im.desc.size()));
   CUDA_TRY(cudaMalloc(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
-  CUDA_TRY(cudaMalloc(&R.d_queue, sizeof(int)));
+  CUDA_TRY(cudaMalloc(&R.d_queue, 4 * sizeof(int)));
+  if (R.nslots > 1) CUDA_TRY(cudaMalloc(&R.d_board, sizeof(JacobiJob) * R.nslots));
   return CATN_OK;
 }
 
@@ -185,10 +200,11 @@ long long default_arena(long long a, const catn_params& p) {
 namespace {
 
 catn_status launch(DeviceRun& R, cudaStream_t st) {
-  CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, sizeof(int), st));
+  CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, 4 * sizeof(int), st));
+  if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.nslots, st));
   catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
                                                                 R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
-                                                                R.d_queue);
+                                                                R.d_queue, R.d_board);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

@@ -41,7 +41,8 @@ struct DeviceRun {
   char* d_slots = nullptr;
   catn_result* d_res = nullptr;
   int* d_trace = nullptr;
-  int* d_queue = nullptr;
+  int* d_queue = nullptr;    // [0] work-queue head, [1] instances finished
+  catn::JacobiJob* d_board = nullptr;   // shared Jacobi jobs, one per slot (batches only)
   catn::SlotLayout L;
   int nslots = 0;
   int ninst = 0;
@@ -49,8 +50,9 @@ struct DeviceRun {
 
   void release() {
     cudaFreeHost(h_input);
-    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue);
+    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue); cudaFree(d_board);
     h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
+    d_board = nullptr;
     d_desc = nullptr; d_order = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
   }
 };

@@ -98,6 +98,19 @@ struct Ctx {
   TapeRec* rec;
   long long nrec, rcap, gshift;
   long long heap_first;   // first byte of the sites loaded from the image
+  // Shared Jacobi (batch kernel): this CTA's job board entry, the launch's
+  // work-queue head and instance count (helpers exist once the queue is
+  // drained), and the smallest column count worth sharing.
+  JacobiJob* job;
+  const int* qhead;
+  int ninst, job_min_n;
+};
+
+// Where a batch CTA publishes its shared Jacobi sweeps (null: never).
+struct JobLink {
+  JacobiJob* job;
+  const int* qhead;
+  int ninst, min_n;
 };
 
 // ---------------------------------------------------------------------------
@@ -345,6 +358,16 @@ CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
   T.sync();
 }
 
+// Whether the Jacobi sweeps on an n-column matrix in global memory go to the
+// shared job (helpers exist only once the launch's queue is drained); the
+// same answer in every thread.
+CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X) {
+  if (!C.job || n < C.job_min_n || X == C.sws) return false;
+  long long drained = 0;
+  if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
+  return C.T.bcast(drained) != 0;
+}
+
 // Large input whose pivoted QR W P = Q R stopped at rank r (trailing block
 // dropped): SVD of the r x nn top block T = [R11 R12] P^T through its
 // transpose (pivoted QR + Jacobi again), then U_W = Q1 * V_T, V_W = U_T.
@@ -383,8 +406,9 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
     X2[e] = (j <= i) ? Tt[j + i * nn] : 0.0;
   }
   T.sync();
-  int sweeps = jacobi_sweeps(T, X2, r, r, r, Vb2, 60, nrm2);
-  if (sweeps < 0) fail_all(C, CATN_ENOCONV);
+  int sweeps = share_jacobi(C, r, X2) ? jacobi_sweeps_shared(T, C.job, X2, r, r, r, Vb2, 60, nrm2)
+                                     : jacobi_sweeps(T, X2, r, r, r, Vb2, 60, nrm2);
+  if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X2, r, r, r, sig2, S2, perm2);
   for (long long e = T.rank(); e < nn * r; e += T.size()) {
@@ -506,8 +530,9 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
   }
   T.sync();
-  int sweeps = jacobi_sweeps(T, X, nn, nn, nn, Vb, 60, nrm);
-  if (sweeps < 0) fail_all(C, CATN_ENOCONV);
+  int sweeps = share_jacobi(C, nn, X) ? jacobi_sweeps_shared(T, C.job, X, nn, nn, nn, Vb, 60, nrm)
+                                      : jacobi_sweeps(T, X, nn, nn, nn, Vb, 60, nrm);
+  if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X, nn, nn, nn, sig, Sout, perm);
   for (long long e = T.rank(); e < mm * nn; e += T.size()) {
@@ -1858,6 +1883,10 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.rec = nullptr;
   C.nrec = C.rcap = C.gshift = 0;
   C.heap_first = 0;
+  C.job = nullptr;
+  C.qhead = nullptr;
+  C.ninst = 0;
+  C.job_min_n = 1 << 30;
   return C;
 }
 
@@ -1956,9 +1985,16 @@ CATN_HDI inline void load_instance(Ctx& C, const InstDesc& D, const long long* i
 // Load, contract and report one instance in the given slot.
 CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L, const InstDesc& D,
                                   const long long* i64, const int* i32, const double* dat,
-                                  catn_result* res, int* trace_base, double* sws, long long sws_doubles) {
+                                  catn_result* res, int* trace_base, double* sws, long long sws_doubles,
+                                  const JobLink* jl = nullptr) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
   C.multigraph = D.multigraph;
+  if (jl) {
+    C.job = jl->job;
+    C.qhead = jl->qhead;
+    C.ninst = jl->ninst;
+    C.job_min_n = jl->min_n;
+  }
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {
     C.trace = trace_base + D.trace_off;

@@ -485,6 +485,265 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
   return result;
 }
 
+// Jacobi sweeps of one CTA's large SVD opened to idle warps of other CTAs
+// (the batch kernel's tail).  `word` = (round sequence << 32) | pairs
+// claimed in the current round; the owner advances a round only when
+// `done` reaches `npair`, so a claim always refers to the round it counted in.
+struct JacobiJob {
+  unsigned long long word;
+  int done, rotated, round, npair;
+  int m, n, ldb, np;
+  double tol;
+  double* B;
+  double* V;
+  double* nrm;
+  long long pad[2];
+};
+
+// ---------------------------------------------------------------------------
+// Jacobi sweeps shared with helper warps of other CTAs.  Every access to the
+// shared columns, V and the norms goes through L2 (ld/st .cg): an SM's L1 is
+// not coherent with writes of other SMs.
+// ---------------------------------------------------------------------------
+#if CATN_DEVICE_PASS
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ void stcg(double* p, double v) { __stcg(p, v); }
+__device__ __forceinline__ int ldcg_i(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned long long ldcg_u(const unsigned long long* p) { return __ldcg(p); }
+__device__ __forceinline__ void fence_gpu() { __threadfence(); }
+#else
+inline double ldcg(const double* p) { return *p; }
+inline void stcg(double* p, double v) { *p = v; }
+inline int ldcg_i(const int* p) { return *p; }
+inline unsigned long long ldcg_u(const unsigned long long* p) { return *p; }
+inline void fence_gpu() {}
+#endif
+
+// Pair pi of round r (round-robin order) on B (m x n) and V (n x n) with
+// the squared norms in nrm; warp-level.  Returns whether it rotated.
+CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double* nrm, long long m, long long n,
+                                    long long ldb, long long np, long long r, long long pi, double tol) {
+  long long p, q;
+  rr_pair(np, r, pi, &p, &q);
+  if (p >= n || q >= n) return false;
+  double* bp = B + p * ldb;
+  double* bq = B + q * ldb;
+  double g = 0.0;
+  for (long long i = T.lane(); i < m; i += T.wsize()) g = fma(ldcg(bp + i), ldcg(bq + i), g);
+  g = T.wsum(g);
+  const double al = ldcg(nrm + p), be = ldcg(nrm + q);
+  double c, s;
+  if (!jacobi_rotation(al, be, g, tol, &c, &s)) return false;
+  for (long long i = T.lane(); i < m; i += T.wsize()) {
+    const double x = ldcg(bp + i), y = ldcg(bq + i);
+    stcg(bp + i, c * x - s * y);
+    stcg(bq + i, s * x + c * y);
+  }
+  double* vp = V + p * n;
+  double* vq = V + q * n;
+  for (long long i = T.lane(); i < n; i += T.wsize()) {
+    const double x = ldcg(vp + i), y = ldcg(vq + i);
+    stcg(vp + i, c * x - s * y);
+    stcg(vq + i, s * x + c * y);
+  }
+  T.wsync();
+  if (T.lane() == 0) {
+    const double t = s / c;
+    stcg(nrm + p, al - t * g);
+    stcg(nrm + q, be + t * g);
+  }
+  T.wsync();
+  return true;
+}
+
+// One claim on J by the calling warp: the pair index in the current round
+// (round index in *r), or -1 when the round has none left.
+CATN_HDI inline long long job_claim(const Team& T, JacobiJob* J, long long* r) {
+#if CATN_DEVICE_PASS
+  unsigned long long old = 0;
+  if (T.lane() == 0) old = atomicAdd(&J->word, 1ULL);
+  old = __shfl_sync(0xffffffffu, old, 0);
+#else
+  const unsigned long long old = J->word;
+  J->word = old + 1;
+#endif
+  const long long k = (long long)(old & 0xffffffffULL);
+  if (k >= ldcg_i(&J->npair)) return -1;
+  fence_gpu();
+  *r = ldcg_i(&J->round);
+  return k;
+}
+
+// The calling warp's share of the current round of J: claims until none is
+// left, reports each pair done.
+CATN_HDI inline void job_work(const Team& T, JacobiJob* J) {
+  for (;;) {
+    long long r;
+    const long long k = job_claim(T, J, &r);
+    if (k < 0) return;
+    // the job's fields through L2 as well: this SM may hold lines of an earlier job
+    double* B = (double*)ldcg_u((const unsigned long long*)&J->B);
+    double* V = (double*)ldcg_u((const unsigned long long*)&J->V);
+    double* nrm = (double*)ldcg_u((const unsigned long long*)&J->nrm);
+    const bool rot = jacobi_pair_l2(T, B, V, nrm, ldcg_i(&J->m), ldcg_i(&J->n), ldcg_i(&J->ldb), ldcg_i(&J->np), r, k,
+                                    ldcg(&J->tol));
+    fence_gpu();
+    if (T.lane() == 0) {
+#if CATN_DEVICE_PASS
+      if (rot) atomicOr(&J->rotated, 1);
+      atomicAdd(&J->done, 1);
+#else
+      if (rot) J->rotated = 1;
+      J->done += 1;
+#endif
+    }
+    T.wsync();
+  }
+}
+
+// jacobi_sweeps with every round's pairs claimed dynamically through J by
+// the team's warps and by helper warps of idle CTAs (help_jacobi).  Returns
+// the sweep count, -1 without convergence, -2 when a wait for claimed pairs
+// ran out (the caller reports it as an error).  B and V are rewritten
+// through the calling SM at the end, so later plain loads see the helpers'
+// writes.
+CATN_HDI inline int jacobi_sweeps_shared(const Team& T, JacobiJob* J, double* B, long long m, long long n,
+                                         long long ldb, double* V, int max_sweeps, double* nrm) {
+  for (long long e = T.rank(); e < n * n; e += T.size()) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  T.sync();
+  if (n < 2) return 0;
+  double mx = 0.0;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) mx = fmax(mx, fabs(B[i + c * ldb]));
+  mx = T.maxv(mx);
+  const double sc = mx > 0.0 ? 1.0 / mx : 1.0;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] *= sc;
+  const long long np = (n % 2) ? n + 1 : n;
+  const int npair = (int)(np / 2);
+  const double tol = 2.220446049250313e-16 * (double)(m > 16 ? m : 16);
+  unsigned long long seq = (ldcg_u(&J->word) >> 32) + 1;
+  T.sync();
+  if (T.leader()) {
+    // closed (no claim can count) before the job becomes visible through npair
+#if CATN_DEVICE_PASS
+    atomicExch(&J->word, (seq << 32) | 0x7fffffffULL);
+#else
+    J->word = (seq << 32) | 0x7fffffffULL;
+#endif
+    fence_gpu();
+    J->B = B; J->V = V; J->nrm = nrm;
+    J->m = (int)m; J->n = (int)n; J->ldb = (int)ldb; J->np = (int)np; J->tol = tol;
+    J->done = 0; J->rotated = 0; J->round = 0;
+    fence_gpu();
+    J->npair = npair;
+    fence_gpu();
+  }
+  ++seq;
+  T.sync();
+  int result = -1;
+  int timed_out = 0;
+  for (int sweep = 0; sweep < max_sweeps && !timed_out; ++sweep) {
+    for (long long c = T.warp(); c < n; c += T.nwarps()) {
+      const double* bc = B + c * ldb;
+      double s2 = 0.0;
+      for (long long i = T.lane(); i < m; i += T.wsize()) {
+        const double x = ldcg(bc + i);
+        s2 = fma(x, x, s2);
+      }
+      s2 = T.wsum(s2);
+      if (T.lane() == 0) stcg(nrm + c, s2);
+    }
+    fence_gpu();
+    T.sync();
+    if (T.leader()) J->rotated = 0;
+    for (long long r = 0; r < np - 1 && !timed_out; ++r) {
+      if (T.leader()) {
+        J->round = (int)r;
+        J->done = 0;
+        fence_gpu();
+#if CATN_DEVICE_PASS
+        atomicExch(&J->word, seq << 32);
+#else
+        J->word = seq << 32;
+#endif
+      }
+      ++seq;
+      T.sync();
+      job_work(T, J);
+      if (T.leader()) {
+        long long spins = 0;
+        while (ldcg_i(&J->done) < npair) {
+          if (++spins > (1LL << 24)) {   // claimed pairs never take this long
+            timed_out = 1;
+            break;
+          }
+#if CATN_DEVICE_PASS
+          __nanosleep(64);
+#endif
+        }
+        fence_gpu();
+        T.red[0] = timed_out ? 1.0 : 0.0;
+      }
+      T.sync();
+      timed_out = T.red[0] > 0.5;
+      T.sync();
+    }
+    fence_gpu();
+    T.sync();
+    const int rot = ldcg_i(&J->rotated);
+    T.sync();
+    if (!rot) {
+      result = sweep + 1;
+      break;
+    }
+  }
+  // close the job: no claim can succeed from here on
+  if (T.leader()) {
+    J->npair = 0;
+    fence_gpu();
+#if CATN_DEVICE_PASS
+    atomicExch(&J->word, (seq << 32) | 0x7fffffffULL);
+#else
+    J->word = (seq << 32) | 0x7fffffffULL;
+#endif
+  }
+  const double inv = 1.0 / sc;
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] = ldcg(B + i + c * ldb) * inv;
+  for (long long e = T.rank(); e < n * n; e += T.size()) V[e] = ldcg(V + e);
+  T.sync();
+  return timed_out ? -2 : result;
+}
+
+#if defined(__CUDACC__)
+// An idle CTA's warps help the shared Jacobi sweeps of the CTAs still
+// contracting, until every instance of the launch has finished (or after a
+// long stretch with nothing to do).
+__device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, const int* finished, int ninst) {
+  const int w = (int)blockIdx.x * T.nwarps() + T.warp();
+  long long idle = 0;
+  while (idle < (1LL << 22)) {
+    if (ldcg_i(finished) >= ninst) return;
+    bool worked = false;
+    for (int s2 = 0; s2 < nslots && !worked; ++s2) {
+      JacobiJob* J = board + (s2 + w) % nslots;
+      const int npair = ldcg_i(&J->npair);
+      if (npair == 0) continue;
+      if ((long long)(ldcg_u(&J->word) & 0xffffffffULL) >= npair) continue;
+      job_work(T, J);
+      worked = true;
+    }
+    if (worked) {
+      idle = 0;
+    } else {
+      ++idle;
+      __nanosleep(256);
+    }
+  }
+}
+#endif
+
 // Column norms of B (n columns), then stable descending order.
 // S_out[r] = sigma of the r-th largest column, perm[r] = its column index.
 CATN_HDI inline void sort_columns(const Team& T, const double* B, long long m, long long n,

@@ -29,8 +29,19 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   // large-matrix path, including its rank-revealing truncation)
   if (const char* e = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(e);
   std::vector<double> sws((size_t)(sws_doubles > 0 ? sws_doubles : 1));
+  // CATN_HOSTCHECK_JOB=1 sends the Jacobi sweeps of every SVD on the global
+  // path through the shared-job protocol (no helpers: the team claims all)
+  JacobiJob job;
+  std::memset(&job, 0, sizeof(job));
+  const int qhead = 1;
+  JobLink jl;
+  jl.job = &job;
+  jl.qhead = &qhead;
+  jl.ninst = 1;
+  jl.min_n = 2;
+  const char* je = std::getenv("CATN_HOSTCHECK_JOB");
   run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
-               sws_doubles);
+               sws_doubles, (je && je[0] == '1') ? &jl : nullptr);
   if (trace && im.desc[0].trace_cap > 0)
     std::memcpy(trace, tr.data(), sizeof(int) * 8 * (size_t)im.desc[0].trace_cap);
   return res->status;

@@ -71,3 +71,20 @@ def test_spinglass_workload_sample_golden(catn):
         _check(got, inst["oracle"], inst["n"])
         if "exact_lnZ" in inst:
             assert abs(got[0] - inst["exact_lnZ"]) / inst["n"] <= 1e-6
+
+
+def test_spinglass_sample_as_one_batch_golden(catn):
+    """The 12 workload instances in ONE persistent launch: the queue drains at
+    once, so CTAs that finish early join the large SVDs' Jacobi sweeps of the
+    others (shared jobs); results as the oracle's."""
+    d = _load("spinglass_sample.json")
+    insts = [dict(n=i["n"], edges=[tuple(e) for e in i["edges"]], weights=i["weights"], fields=i["fields"],
+                  beta=i["beta"]) for i in d["instances"]]
+    res = catn.IsingBatch(insts, **d["params"]).run()
+    for inst, r in zip(d["instances"], res):
+        o = inst["oracle"]
+        assert r.status == 0
+        assert r.nsteps == o["steps"]
+        assert r.maxdim == o["maxdim"]
+        assert abs(r.lnZ - o["lnZ"]) / inst["n"] <= 1e-10
+        assert abs(r.err - o["err"]) <= 1e-12 + 1e-6 * abs(o["err"])

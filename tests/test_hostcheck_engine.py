@@ -191,3 +191,19 @@ def test_large_svd_path_everywhere(host, name, L, beta, kw, monkeypatch):
     assert st == 0 and rows == orows
     assert abs(res.lnZ - lz) / (L * L) < 1e-12
     assert abs(res.err - err) <= 1e-12 + 1e-6 * abs(err)
+
+
+@pytest.mark.parametrize("name,L,beta,kw", CASES[:4], ids=[c[0] for c in CASES[:4]])
+def test_shared_jacobi_protocol(host, name, L, beta, kw, monkeypatch):
+    """Every SVD through the global path with its Jacobi sweeps run through the
+    shared-job protocol that idle CTAs join on the GPU (here the team claims
+    every pair itself): same trace, same lnZ."""
+    monkeypatch.setenv("CATN_HOSTCHECK_SWS", "0")
+    monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
+    r = np.random.default_rng(zlib.crc32(name.encode()) % 1000)
+    e = X.square_edges(L)
+    w, h = r.normal(size=len(e)), r.normal(0, 0.1, L * L)
+    st, res, rows = run_ising(host, L * L, e, w, h, beta, **kw)
+    (lz, err, psi), orows, tn = oracle_ising(L * L, e, w, h, beta, **kw)
+    assert st == 0 and rows == orows
+    assert abs(res.lnZ - lz) / (L * L) < 1e-12
