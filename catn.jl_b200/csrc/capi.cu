@@ -7,6 +7,7 @@
 // slot that stays resident afterwards for result_tensor.
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -59,17 +60,26 @@ catn_status check_params(const catn_params* p) {
 
 namespace {
 
-// Smallest column count whose Jacobi sweeps are opened to helper warps.
-constexpr int kSharedJacobiMinN = 96;
+// Batch launches keep kHelperCtas CTAs that only help the large SVDs of the
+// others, and open the Jacobi sweeps of SVDs with at least kSharedJacobiMinN
+// columns to them: a launch lasts as long as its slowest instance, whose
+// time is mostly the Jacobi sweeps of such SVDs.  Measured on the
+// 512-instance spin-glass batch (ms per launch): no pool 471; pool 24 with
+// threshold 48 / 64 / 96 / 128 / 200 / 256: 459 / 437 / 437 / 417-422 / 417 /
+// 477; threshold 128-160 with pool 16 / 24 / 32: 424-426 / 417-426 / 441.
+// CATN_HELPER_CTAS and CATN_SHARED_JACOBI_MIN_N override the two.
+constexpr int kSharedJacobiMinN = 128;
+constexpr int kHelperCtas = 24;
 
 // `order` lists instance ids by descending work estimate, so the longest
 // contractions start first (longest-processing-time scheduling).  With a job
-// board, a CTA that finds the queue drained lends its warps to the large
-// SVDs of the CTAs still contracting (help_jacobi) until all are finished.
+// board, the last `nhelp` CTAs and every CTA that finds the queue drained
+// lend their warps to the large SVDs of the CTAs still contracting
+// (help_jacobi) until all are finished.
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue,
-    JacobiJob* board) {
+    JacobiJob* board, int nhelp, int share_min_n) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -81,7 +91,12 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
   jl.job = board ? board + blockIdx.x : nullptr;
   jl.qhead = queue;
   jl.ninst = ninst;
-  jl.min_n = kSharedJacobiMinN;
+  jl.min_n = share_min_n;
+  jl.pool = nhelp > 0;
+  if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
+    help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
+    return;
+  }
   for (;;) {
     long long inst = 0;
     if (threadIdx.x == 0) {
@@ -202,9 +217,14 @@ namespace {
 catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, 4 * sizeof(int), st));
   if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.nslots, st));
+  int nhelp = kHelperCtas;
+  if (const char* e = std::getenv("CATN_HELPER_CTAS")) nhelp = std::atoi(e);
+  if (!R.d_board || nhelp < 0 || 4 * nhelp > R.nslots || 4 * nhelp > R.ninst) nhelp = 0;
+  int min_n = kSharedJacobiMinN;
+  if (const char* e = std::getenv("CATN_SHARED_JACOBI_MIN_N")) min_n = std::max(2, std::atoi(e));
   catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
                                                                 R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
-                                                                R.d_queue, R.d_board);
+                                                                R.d_queue, R.d_board, nhelp, min_n);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

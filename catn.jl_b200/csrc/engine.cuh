@@ -104,6 +104,7 @@ struct Ctx {
   JacobiJob* job;
   const int* qhead;
   int ninst, job_min_n;
+  int job_pool;   // CTAs of the launch do nothing but help: share from the start
 };
 
 // Where a batch CTA publishes its shared Jacobi sweeps (null: never).
@@ -111,6 +112,7 @@ struct JobLink {
   JacobiJob* job;
   const int* qhead;
   int ninst, min_n;
+  int pool;   // the launch has dedicated helper CTAs
 };
 
 // ---------------------------------------------------------------------------
@@ -359,10 +361,12 @@ CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
 }
 
 // Whether the Jacobi sweeps on an n-column matrix in global memory go to the
-// shared job (helpers exist only once the launch's queue is drained); the
-// same answer in every thread.
+// shared job: always when the launch has dedicated helper CTAs, otherwise
+// once the launch's queue is drained (idle CTAs then help); the same answer
+// in every thread.
 CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X) {
   if (!C.job || n < C.job_min_n || X == C.sws) return false;
+  if (C.job_pool) return true;
   long long drained = 0;
   if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
   return C.T.bcast(drained) != 0;
@@ -1887,6 +1891,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.qhead = nullptr;
   C.ninst = 0;
   C.job_min_n = 1 << 30;
+  C.job_pool = 0;
   return C;
 }
 
@@ -1994,6 +1999,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     C.qhead = jl->qhead;
     C.ninst = jl->ninst;
     C.job_min_n = jl->min_n;
+    C.job_pool = jl->pool;
   }
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {
