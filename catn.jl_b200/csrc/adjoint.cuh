@@ -407,9 +407,17 @@ CATN_HDI inline void site_gradients_out(Ctx& C, const InstDesc& D, const long lo
 // Load, contract with the tape on, run the adjoint and report one instance.
 CATN_HDI inline void run_instance_grad(const Team& T, char* slot, const SlotLayout& L, const InstDesc& D,
                                        const long long* i64, const int* i32, const double* dat, catn_result* res,
-                                       double* gimg, double* sws, long long sws_doubles) {
+                                       double* gimg, double* sws, long long sws_doubles,
+                                       const JobLink* jl = nullptr) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
   C.multigraph = D.multigraph;
+  if (jl) {
+    C.job = jl->job;
+    C.qhead = jl->qhead;
+    C.ninst = jl->ninst;
+    C.job_min_n = jl->min_n;
+    C.job_pool = jl->pool;
+  }
   reset_slot(C);
   tape_enable(C, L.arena_bytes);
   if (D.kind != 0) fail_all(C, CATN_EINVAL);   // gradients of MPS-form inputs only

@@ -154,6 +154,8 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   if (ns * R.L.slot_bytes > budget) ns = budget / R.L.slot_bytes;
   if (ns < 1) return fail(CATN_ENOMEM, "not enough device memory for one slot");
   R.nslots = (int)ns;
+  // one network: the other resident CTAs only help its large SVDs (no slots)
+  R.ngrid = (R.ninst == 1 && ns == 1 && resident > 1) ? (int)resident : (int)ns;
   const long long b_desc = align256((long long)(sizeof(InstDesc) * im.desc.size())) +
                            align256((long long)(sizeof(int) * im.desc.size()));
   std::vector<int> order(im.desc.size());
@@ -182,8 +184,19 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   CUDA_TRY(cudaMalloc(&R.d_res, sizeof(catn_result) * im.desc.size()));
   CUDA_TRY(cudaMalloc(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
   CUDA_TRY(cudaMalloc(&R.d_queue, 4 * sizeof(int)));
-  if (R.nslots > 1) CUDA_TRY(cudaMalloc(&R.d_board, sizeof(JacobiJob) * R.nslots));
+  if (R.ngrid > 1) CUDA_TRY(cudaMalloc(&R.d_board, sizeof(JacobiJob) * R.ngrid));
   return CATN_OK;
+}
+
+void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n) {
+  int h = pool ? kHelperCtas : 0;
+  if (const char* e = std::getenv("CATN_HELPER_CTAS")) h = std::atoi(e);
+  if (!R.d_board || h < 0 || 4 * h > R.nslots || 4 * h > R.ninst) h = 0;
+  if (R.d_board && R.ngrid > R.nslots) h = R.ngrid - R.nslots;
+  int m = kSharedJacobiMinN;
+  if (const char* e = std::getenv("CATN_SHARED_JACOBI_MIN_N")) m = std::max(2, std::atoi(e));
+  *nhelp = h;
+  *min_n = m;
 }
 
 catn_status upload(DeviceRun& R, cudaStream_t st) {
@@ -193,16 +206,16 @@ catn_status upload(DeviceRun& R, cudaStream_t st) {
 
 // Arena of a single network when the caller passes 0: the largest two-site
 // matrix a swap can form is (chi*Dmax)^2 doubles, and a full-rank SVD of it
-// holds five such buffers on the scratch stack (40 % of the arena), so take
-// 16x that matrix, at least 1 GiB and at most 48 GiB or a quarter of the
-// free device memory.  Exact mode (Dmax < 0) keeps 1 GiB: its networks are
+// holds five such buffers on the scratch stack (40 % of the arena) beside
+// the scratch of the operations around it, so take 32x that matrix, at
+// least 1 GiB and at most 48 GiB or a quarter of the free device memory.  Exact mode (Dmax < 0) keeps 1 GiB: its networks are
 // small by construction.
 long long default_arena(long long a, const catn_params& p) {
   if (a > 0) return a;
   long long arena = 1LL << 30;
   if (p.Dmax > 0) {
     const long long m = (long long)std::min(p.chi, 16384) * std::min(p.Dmax, 16384);
-    arena = std::max(arena, 16 * 8 * m * m);
+    arena = std::max(arena, 32 * 8 * m * m);
   }
   arena = std::min(arena, 48LL << 30);
   size_t freeb = 0, totalb = 0;
@@ -216,13 +229,10 @@ namespace {
 
 catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, 4 * sizeof(int), st));
-  if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.nslots, st));
-  int nhelp = kHelperCtas;
-  if (const char* e = std::getenv("CATN_HELPER_CTAS")) nhelp = std::atoi(e);
-  if (!R.d_board || nhelp < 0 || 4 * nhelp > R.nslots || 4 * nhelp > R.ninst) nhelp = 0;
-  int min_n = kSharedJacobiMinN;
-  if (const char* e = std::getenv("CATN_SHARED_JACOBI_MIN_N")) min_n = std::max(2, std::atoi(e));
-  catn_persistent_kernel<<<R.nslots, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
+  if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.ngrid, st));
+  int nhelp = 0, min_n = 0;
+  helper_config(R, true, &nhelp, &min_n);
+  catn_persistent_kernel<<<R.ngrid, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
                                                                 R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
                                                                 R.d_queue, R.d_board, nhelp, min_n);
   CUDA_TRY(cudaGetLastError());

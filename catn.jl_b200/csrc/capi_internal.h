@@ -45,6 +45,7 @@ struct DeviceRun {
   catn::JacobiJob* d_board = nullptr;   // shared Jacobi jobs, one per slot (batches only)
   catn::SlotLayout L;
   int nslots = 0;
+  int ngrid = 0;   // CTAs per launch: nslots, or every resident CTA for one network (the rest help)
   int ninst = 0;
   long long input_bytes = 0;
 
@@ -69,6 +70,10 @@ struct GradRun {
 // Sizes slots and packs the image (capi.cu).
 catn_status prepare(const catn::Image& im, long long arena_bytes, int max_slots, DeviceRun& R);
 catn_status upload(DeviceRun& R, cudaStream_t st);
+// Dedicated helper CTAs of a launch of R and the smallest column count whose
+// Jacobi sweeps are shared (capi.cu).  `pool`: keep the batch helper pool
+// (one network always gets every other resident CTA as a helper).
+void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n);
 // Arena of a single network when the caller passes 0 (capi.cu).
 long long default_arena(long long a, const catn_params& p);
 // Frees a gradient run (capi_grad.cu).
