@@ -417,6 +417,7 @@ CATN_HDI inline void run_instance_grad(const Team& T, char* slot, const SlotLayo
     C.ninst = jl->ninst;
     C.job_min_n = jl->min_n;
     C.job_pool = jl->pool;
+    C.job_min_qr = jl->min_qr;
   }
   reset_slot(C);
   tape_enable(C, L.arena_bytes);

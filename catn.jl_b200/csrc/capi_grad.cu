@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
   jl.ninst = ninst;
   jl.min_n = share_min_n;
   jl.pool = nhelp > 0;
+  jl.min_qr = kSharedHouseMinElems;
   if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
     help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
     return;

@@ -19,6 +19,10 @@ constexpr int kThreads = 256;
 // small-SVD workspace (two CTAs fit on one SM).
 constexpr int kSmemBytes = 100 * 1024;
 constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - catn::GEMM_STAGE_BYTES) / 8;
+// Smallest rows x columns whose Householder steps (pivoted QR, applying Q)
+// are shared with helper warps: rounds must hold thousands of columns to
+// outweigh one publish/claim/wait per reflector.
+constexpr long long kSharedHouseMinElems = 1LL << 20;
 
 // Records `msg` as the calling thread's last error and returns `s`.
 catn_status fail(catn_status s, const std::string& msg);

@@ -104,7 +104,8 @@ struct Ctx {
   JacobiJob* job;
   const int* qhead;
   int ninst, job_min_n;
-  int job_pool;   // CTAs of the launch do nothing but help: share from the start
+  int job_pool;        // CTAs of the launch do nothing but help: share from the start
+  long long job_min_qr;   // smallest rows x columns whose Householder work is shared
 };
 
 // Where a batch CTA publishes its shared Jacobi sweeps (null: never).
@@ -113,6 +114,7 @@ struct JobLink {
   const int* qhead;
   int ninst, min_n;
   int pool;   // the launch has dedicated helper CTAs
+  long long min_qr;
 };
 
 // ---------------------------------------------------------------------------
@@ -372,6 +374,39 @@ CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X) {
   return C.T.bcast(drained) != 0;
 }
 
+// Whether the Householder work on a rows x cols matrix in global memory goes
+// to the shared job (same rule as share_jacobi, by element count).
+CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const double* X) {
+  if (!C.job || rows * cols < C.job_min_qr || X == C.sws) return false;
+  if (C.job_pool) return true;
+  long long drained = 0;
+  if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
+  return C.T.bcast(drained) != 0;
+}
+// qr_apply_q, shared when large; false when a shared wait ran out.
+CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
+                             double* Cm, long long ncols, long long ldc) {
+  if (share_house(C, m, ncols, Cm)) {
+    if (qr_apply_q_shared(C.T, C.job, A, m, n, lda, tau, Cm, ncols, ldc)) {
+      fail_all(C, CATN_ETIMEOUT);
+      return false;
+    }
+    return true;
+  }
+  qr_apply_q(C.T, A, m, n, lda, tau, Cm, ncols, ldc);
+  return true;
+}
+// qrcp_inplace, shared when large; -2 when a shared wait ran out.
+CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long long lda, double* tau, int* piv,
+                               double* nrm, double stop_tol) {
+  if (share_house(C, m, n, A)) {
+    const long long r = qrcp_shared(C.T, C.job, A, m, n, lda, tau, piv, nrm, stop_tol);
+    if (r == -2) fail_all(C, CATN_ETIMEOUT);
+    return r;
+  }
+  return qrcp_inplace(C.T, A, m, n, lda, tau, piv, nrm, stop_tol);
+}
+
 // Large input whose pivoted QR W P = Q R stopped at rank r (trailing block
 // dropped): SVD of the r x nn top block T = [R11 R12] P^T through its
 // transpose (pivoted QR + Jacobi again), then U_W = Q1 * V_T, V_W = U_T.
@@ -403,7 +438,7 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
     Tt[(long long)piv[j] + nn * i] = (j >= i) ? s.W[i + j * mm] : 0.0;
   }
   T.sync();
-  qrcp_inplace(T, Tt, nn, r, nn, tau2, piv2, nrm2, 0.0);
+  if (qrcp(C, Tt, nn, r, nn, tau2, piv2, nrm2, 0.0) < 0) return R;
   for (long long e = T.rank(); e < r * r; e += T.size()) {
     long long i, j;
     divmod(e, r, &i, &j);
@@ -427,14 +462,14 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
     Vin[(long long)piv2[i] + c * r] = (sv > 0.0) ? X2[i + (long long)perm2[c] * r] / sv : 0.0;
   }
   T.sync();
-  qr_apply_q(T, Tt, nn, r, nn, tau2, Uin, r, nn);
+  if (!apply_q(C, Tt, nn, r, nn, tau2, Uin, r, nn)) return R;
   for (long long e = T.rank(); e < mm * r; e += T.size()) {
     long long rr, c;
     divmod(e, mm, &rr, &c);
     Uw[e] = (rr < r) ? Vin[rr + c * r] : 0.0;
   }
   T.sync();
-  qr_apply_q(T, s.W, mm, r, mm, tau, Uw, r, mm);
+  if (!apply_q(C, s.W, mm, r, mm, tau, Uw, r, mm)) return R;
   prof_add(C, PROF_SVD_LARGE, (double)(clk() - t0));
   prof_add(C, PROF_N_LARGE, 1.0);
   R.p = r;
@@ -515,7 +550,8 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     f2 = T.sum(f2);
     if (sqrt(f2) > 1e6 * s.tol) stop = s.tol;
   }
-  const long long r = qrcp_inplace(T, s.W, mm, nn, mm, tau, piv, nrm, stop);
+  const long long r = qrcp(C, s.W, mm, nn, mm, tau, piv, nrm, stop);
+  if (r < 0) return R;
   if (r < nn) return svd_truncated(C, s, r, tau, piv, t0);
   if (!s.smem) {
     const bool jsm = 2 * nn * nn <= C.sws_doubles;   // Jacobi pair in shared memory when it fits
@@ -551,7 +587,7 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     Vt[(long long)piv[i] + c * nn] = (sv > 0.0) ? X[i + (long long)perm[c] * nn] / sv : 0.0;
   }
   T.sync();
-  qr_apply_q(T, s.W, mm, nn, mm, tau, Ut, nn, mm);
+  if (!apply_q(C, s.W, mm, nn, mm, tau, Ut, nn, mm)) return R;
   prof_add(C, s.smem ? PROF_SVD_SMALL : PROF_SVD_LARGE, (double)(clk() - t0));
   prof_add(C, s.smem ? PROF_N_SMALL : PROF_N_LARGE, 1.0);
   R.p = nn;
@@ -1892,6 +1928,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.ninst = 0;
   C.job_min_n = 1 << 30;
   C.job_pool = 0;
+  C.job_min_qr = 1LL << 62;
   return C;
 }
 
@@ -2000,6 +2037,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     C.ninst = jl->ninst;
     C.job_min_n = jl->min_n;
     C.job_pool = jl->pool;
+    C.job_min_qr = jl->min_qr;
   }
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {

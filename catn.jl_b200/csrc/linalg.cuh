@@ -485,25 +485,32 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
   return result;
 }
 
-// Jacobi sweeps of one CTA's large SVD opened to idle warps of other CTAs
-// (the batch kernel's tail).  `word` = (round sequence << 32) | pairs
-// claimed in the current round; the owner advances a round only when
-// `done` reaches `npair`, so a claim always refers to the round it counted in.
+// Work of one CTA's large SVD opened to idle warps of other CTAs (helper
+// CTAs of a batch, the other CTAs of a single-network launch).  A job runs
+// in rounds; each round has `count` items that warps claim through `word` =
+// (round sequence << 40) | (count << 20) | claims so far, so a claim always
+// knows the count of the round it counted in.  The owner publishes a round
+// only after every item of the previous one reported done, and the round's
+// payload (round, k, tk, c0) is written before the round is published, so a
+// valid claim may read it.  Kinds: Jacobi column pairs of one round-robin
+// round (B, V, nrm); Householder reflector k applied to 4-column chunks of C
+// from column c0 (reflector in column k of A), with the trailing squared
+// norms recomputed into nrm when nrm is set (pivoted QR).
+enum { JOB_JACOBI = 0, JOB_HOUSE = 1 };
+constexpr int JOB_CHUNK = 4;   // columns per Householder claim
 struct JacobiJob {
   unsigned long long word;
-  int done, rotated, round, npair;
-  int m, n, ldb, np;
-  double tol;
-  double* B;
-  double* V;
+  int done, rotated, round, open;
+  int kind, m, n, ldb, np, k, c0, ldc;
+  double tol, tk;
+  double* B;     // Jacobi columns / Householder reflectors (A)
+  double* V;     // Jacobi rotations / Householder target (C)
   double* nrm;
-  long long pad[2];
 };
 
 // ---------------------------------------------------------------------------
-// Jacobi sweeps shared with helper warps of other CTAs.  Every access to the
-// shared columns, V and the norms goes through L2 (ld/st .cg): an SM's L1 is
-// not coherent with writes of other SMs.
+// Shared jobs.  Every access to the shared matrices, V and the norms goes
+// through L2 (ld/st .cg): an SM's L1 is not coherent with writes of other SMs.
 // ---------------------------------------------------------------------------
 #if CATN_DEVICE_PASS
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
@@ -518,6 +525,17 @@ inline int ldcg_i(const int* p) { return *p; }
 inline unsigned long long ldcg_u(const unsigned long long* p) { return *p; }
 inline void fence_gpu() {}
 #endif
+
+CATN_HD unsigned long long job_word(unsigned long long seq, long long count) {
+  return (seq << 40) | ((unsigned long long)count << 20);
+}
+CATN_HD void job_set_word(JacobiJob* J, unsigned long long w) {
+#if CATN_DEVICE_PASS
+  atomicExch(&J->word, w);
+#else
+  J->word = w;
+#endif
+}
 
 // Pair pi of round r (round-robin order) on B (m x n) and V (n x n) with
 // the squared norms in nrm; warp-level.  Returns whether it rotated.
@@ -556,9 +574,37 @@ CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double*
   return true;
 }
 
-// One claim on J by the calling warp: the pair index in the current round
-// (round index in *r), or -1 when the round has none left.
-CATN_HDI inline long long job_claim(const Team& T, JacobiJob* J, long long* r) {
+// Reflector k (v = A[k+1:m, k] with an implicit 1 at k, factor tk) applied to
+// column j of C; with nrm, the squared norm of C[k+1:m, j] goes to nrm[j].
+// Warp-level, through L2.
+CATN_HDI inline void house_col_l2(const Team& T, const double* A, long long m, long long lda, long long k, double tk,
+                                  double* C, long long ldc, long long j, double* nrm) {
+  const double* ak = A + k * lda;
+  double* cj = C + j * ldc;
+  if (tk != 0.0) {
+    double w = 0.0;
+    for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ldcg(ak + i), ldcg(cj + i), w);
+    w = (T.wsum(w) + ldcg(cj + k)) * tk;
+    T.wsync();
+    if (T.lane() == 0) stcg(cj + k, ldcg(cj + k) - w);
+    for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) stcg(cj + i, ldcg(cj + i) - w * ldcg(ak + i));
+    T.wsync();
+  }
+  if (nrm) {
+    double s = 0.0;
+    for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) {
+      const double x = ldcg(cj + i);
+      s = fma(x, x, s);
+    }
+    s = T.wsum(s);
+    if (T.lane() == 0) stcg(nrm + j, s);
+    T.wsync();
+  }
+}
+
+// One claim on J by the calling warp: the item index in the current round,
+// or -1 when the round has none left.
+CATN_HDI inline long long job_claim(const Team& T, JacobiJob* J) {
 #if CATN_DEVICE_PASS
   unsigned long long old = 0;
   if (T.lane() == 0) old = atomicAdd(&J->word, 1ULL);
@@ -567,26 +613,34 @@ CATN_HDI inline long long job_claim(const Team& T, JacobiJob* J, long long* r) {
   const unsigned long long old = J->word;
   J->word = old + 1;
 #endif
-  const long long k = (long long)(old & 0xffffffffULL);
-  if (k >= ldcg_i(&J->npair)) return -1;
+  const long long item = (long long)(old & 0xfffffULL);
+  const long long count = (long long)((old >> 20) & 0xfffffULL);
+  if (item >= count) return -1;
   fence_gpu();
-  *r = ldcg_i(&J->round);
-  return k;
+  return item;
 }
 
 // The calling warp's share of the current round of J: claims until none is
-// left, reports each pair done.
+// left, reports each item done.
 CATN_HDI inline void job_work(const Team& T, JacobiJob* J) {
   for (;;) {
-    long long r;
-    const long long k = job_claim(T, J, &r);
-    if (k < 0) return;
+    const long long item = job_claim(T, J);
+    if (item < 0) return;
     // the job's fields through L2 as well: this SM may hold lines of an earlier job
     double* B = (double*)ldcg_u((const unsigned long long*)&J->B);
     double* V = (double*)ldcg_u((const unsigned long long*)&J->V);
     double* nrm = (double*)ldcg_u((const unsigned long long*)&J->nrm);
-    const bool rot = jacobi_pair_l2(T, B, V, nrm, ldcg_i(&J->m), ldcg_i(&J->n), ldcg_i(&J->ldb), ldcg_i(&J->np), r, k,
-                                    ldcg(&J->tol));
+    bool rot = false;
+    if (ldcg_i(&J->kind) == JOB_JACOBI) {
+      rot = jacobi_pair_l2(T, B, V, nrm, ldcg_i(&J->m), ldcg_i(&J->n), ldcg_i(&J->ldb), ldcg_i(&J->np),
+                           ldcg_i(&J->round), item, ldcg(&J->tol));
+    } else {
+      const long long m = ldcg_i(&J->m), lda = ldcg_i(&J->ldb), k = ldcg_i(&J->k), ldc = ldcg_i(&J->ldc);
+      const long long c0 = ldcg_i(&J->c0), cend = ldcg_i(&J->n);
+      const double tk = ldcg(&J->tk);
+      for (long long j = c0 + item * JOB_CHUNK; j < cend && j < c0 + (item + 1) * JOB_CHUNK; ++j)
+        house_col_l2(T, B, m, lda, k, tk, V, ldc, j, nrm);
+    }
     fence_gpu();
     if (T.lane() == 0) {
 #if CATN_DEVICE_PASS
@@ -601,8 +655,59 @@ CATN_HDI inline void job_work(const Team& T, JacobiJob* J) {
   }
 }
 
+// Owner side: open J (closed word first, then the fields the caller set,
+// then `open`), returning the first round's sequence number.
+CATN_HDI inline unsigned long long job_open(const Team& T, JacobiJob* J) {
+  unsigned long long seq = (ldcg_u(&J->word) >> 40) + 1;
+  T.sync();
+  if (T.leader()) {
+    job_set_word(J, job_word(seq, 0));   // closed: no claim can count
+    fence_gpu();
+  }
+  return seq + 1;
+}
+// Publish one round of `count` items (the leader has written its payload),
+// do the team's share, wait (bounded) until every item is done.  Returns 1
+// when the wait ran out.
+CATN_HDI inline int job_round(const Team& T, JacobiJob* J, unsigned long long seq, long long count) {
+  if (T.leader()) {
+    J->done = 0;
+    fence_gpu();
+    job_set_word(J, job_word(seq, count));
+  }
+  T.sync();
+  job_work(T, J);
+  int timed_out = 0;
+  if (T.leader()) {
+    long long spins = 0;
+    while (ldcg_i(&J->done) < count) {
+      if (++spins > (1LL << 24)) {   // claimed items never take this long
+        timed_out = 1;
+        break;
+      }
+#if CATN_DEVICE_PASS
+      __nanosleep(64);
+#endif
+    }
+    fence_gpu();
+    T.red[0] = timed_out ? 1.0 : 0.0;
+  }
+  T.sync();
+  timed_out = T.red[0] > 0.5;
+  T.sync();
+  return timed_out;
+}
+CATN_HDI inline void job_close(const Team& T, JacobiJob* J, unsigned long long seq) {
+  if (T.leader()) {
+    J->open = 0;
+    fence_gpu();
+    job_set_word(J, job_word(seq, 0));
+  }
+  T.sync();
+}
+
 // jacobi_sweeps with every round's pairs claimed dynamically through J by
-// the team's warps and by helper warps of idle CTAs (help_jacobi).  Returns
+// the team's warps and by helper warps of other CTAs (help_jobs).  Returns
 // the sweep count, -1 without convergence, -2 when a wait for claimed pairs
 // ran out (the caller reports it as an error).  B and V are rewritten
 // through the calling SM at the end, so later plain loads see the helpers'
@@ -622,24 +727,16 @@ CATN_HDI inline int jacobi_sweeps_shared(const Team& T, JacobiJob* J, double* B,
   const long long np = (n % 2) ? n + 1 : n;
   const int npair = (int)(np / 2);
   const double tol = 2.220446049250313e-16 * (double)(m > 16 ? m : 16);
-  unsigned long long seq = (ldcg_u(&J->word) >> 32) + 1;
-  T.sync();
+  unsigned long long seq = job_open(T, J);
   if (T.leader()) {
-    // closed (no claim can count) before the job becomes visible through npair
-#if CATN_DEVICE_PASS
-    atomicExch(&J->word, (seq << 32) | 0x7fffffffULL);
-#else
-    J->word = (seq << 32) | 0x7fffffffULL;
-#endif
-    fence_gpu();
+    J->kind = JOB_JACOBI;
     J->B = B; J->V = V; J->nrm = nrm;
     J->m = (int)m; J->n = (int)n; J->ldb = (int)ldb; J->np = (int)np; J->tol = tol;
-    J->done = 0; J->rotated = 0; J->round = 0;
+    J->rotated = 0; J->round = 0;
     fence_gpu();
-    J->npair = npair;
+    J->open = 1;
     fence_gpu();
   }
-  ++seq;
   T.sync();
   int result = -1;
   int timed_out = 0;
@@ -658,36 +755,9 @@ CATN_HDI inline int jacobi_sweeps_shared(const Team& T, JacobiJob* J, double* B,
     T.sync();
     if (T.leader()) J->rotated = 0;
     for (long long r = 0; r < np - 1 && !timed_out; ++r) {
-      if (T.leader()) {
-        J->round = (int)r;
-        J->done = 0;
-        fence_gpu();
-#if CATN_DEVICE_PASS
-        atomicExch(&J->word, seq << 32);
-#else
-        J->word = seq << 32;
-#endif
-      }
+      if (T.leader()) J->round = (int)r;
+      timed_out = job_round(T, J, seq, npair);
       ++seq;
-      T.sync();
-      job_work(T, J);
-      if (T.leader()) {
-        long long spins = 0;
-        while (ldcg_i(&J->done) < npair) {
-          if (++spins > (1LL << 24)) {   // claimed pairs never take this long
-            timed_out = 1;
-            break;
-          }
-#if CATN_DEVICE_PASS
-          __nanosleep(64);
-#endif
-        }
-        fence_gpu();
-        T.red[0] = timed_out ? 1.0 : 0.0;
-      }
-      T.sync();
-      timed_out = T.red[0] > 0.5;
-      T.sync();
     }
     fence_gpu();
     T.sync();
@@ -698,16 +768,7 @@ CATN_HDI inline int jacobi_sweeps_shared(const Team& T, JacobiJob* J, double* B,
       break;
     }
   }
-  // close the job: no claim can succeed from here on
-  if (T.leader()) {
-    J->npair = 0;
-    fence_gpu();
-#if CATN_DEVICE_PASS
-    atomicExch(&J->word, (seq << 32) | 0x7fffffffULL);
-#else
-    J->word = (seq << 32) | 0x7fffffffULL;
-#endif
-  }
+  job_close(T, J, seq);
   const double inv = 1.0 / sc;
   for (long long c = 0; c < n; ++c)
     for (long long i = T.rank(); i < m; i += T.size()) B[i + c * ldb] = ldcg(B + i + c * ldb) * inv;
@@ -716,10 +777,134 @@ CATN_HDI inline int jacobi_sweeps_shared(const Team& T, JacobiJob* J, double* B,
   return timed_out ? -2 : result;
 }
 
+// qrcp_inplace with each step's trailing update (and norm recomputation)
+// shared through J in 4-column chunks.  Same arithmetic per column; returns
+// the rank reached, or -2 when a wait ran out.  A is rewritten through the
+// calling SM at the end.
+CATN_HDI inline long long qrcp_shared(const Team& T, JacobiJob* J, double* A, long long m, long long n, long long lda,
+                                      double* tau, int* piv, double* nrm, double stop_tol) {
+  for (long long j = T.warp(); j < n; j += T.nwarps()) {
+    const double* aj = A + j * lda;
+    double s = 0.0;
+    for (long long i = T.lane(); i < m; i += T.wsize()) s = fma(aj[i], aj[i], s);
+    s = T.wsum(s);
+    if (T.lane() == 0) { stcg(nrm + j, s); piv[j] = (int)j; }
+  }
+  fence_gpu();
+  T.sync();
+  unsigned long long seq = job_open(T, J);
+  if (T.leader()) {
+    J->kind = JOB_HOUSE;
+    J->B = A; J->V = A; J->nrm = nrm;
+    J->m = (int)m; J->n = (int)n; J->ldb = (int)lda; J->ldc = (int)lda;
+    fence_gpu();
+    J->open = 1;
+    fence_gpu();
+  }
+  T.sync();
+  long long rank = n;
+  int timed_out = 0;
+  for (long long k = 0; k < n && !timed_out; ++k) {
+    double bv = -1.0, rem = 0.0;
+    long long bi = -1;
+    for (long long j = k + T.rank(); j < n; j += T.size()) {
+      const double v = ldcg(nrm + j);
+      rem += v;
+      if (bi < 0 || v > bv) { bv = v; bi = j; }
+    }
+    if (stop_tol > 0.0 && k > 0) {
+      rem = T.sum(rem);
+      if (rem <= stop_tol * stop_tol) { rank = k; break; }
+    }
+    const long long p = T.argmax(bv, bi);
+    double* ak = A + k * lda;
+    if (p != k && p >= 0) {
+      double* ap = A + p * lda;
+      for (long long i = T.rank(); i < m; i += T.size()) {
+        const double t = ldcg(ak + i);
+        stcg(ak + i, ldcg(ap + i));
+        stcg(ap + i, t);
+      }
+      T.sync();
+      if (T.leader()) {
+        const double t = ldcg(nrm + k);
+        stcg(nrm + k, ldcg(nrm + p));
+        stcg(nrm + p, t);
+        const int q = piv[k]; piv[k] = piv[p]; piv[p] = q;
+      }
+      T.sync();
+    }
+    double loc = 0.0;
+    for (long long i = k + 1 + T.rank(); i < m; i += T.size()) {
+      const double x = ldcg(ak + i);
+      loc = fma(x, x, loc);
+    }
+    const double xnorm2 = T.sum(loc);
+    const double alpha = ldcg(ak + k);
+    double tk = 0.0;
+    if (xnorm2 > 0.0) {
+      const double beta = -copysign(sqrt(alpha * alpha + xnorm2), alpha);
+      tk = (beta - alpha) / beta;
+      const double sc = 1.0 / (alpha - beta);
+      for (long long i = k + 1 + T.rank(); i < m; i += T.size()) stcg(ak + i, ldcg(ak + i) * sc);
+      T.sync();
+      if (T.leader()) stcg(ak + k, beta);
+    }
+    if (T.leader()) {
+      tau[k] = tk;
+      J->k = (int)k; J->tk = tk; J->c0 = (int)(k + 1);
+    }
+    fence_gpu();
+    T.sync();
+    const long long cols = n - k - 1;
+    if (cols > 0) {
+      timed_out = job_round(T, J, seq, (cols + JOB_CHUNK - 1) / JOB_CHUNK);
+      ++seq;
+    }
+  }
+  job_close(T, J, seq);
+  for (long long c = 0; c < n; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) A[i + c * lda] = ldcg(A + i + c * lda);
+  for (long long j = T.rank(); j < n; j += T.size()) nrm[j] = ldcg(nrm + j);
+  T.sync();
+  return timed_out ? -2 : rank;
+}
+
+// qr_apply_q with each reflector's update of C shared through J in 4-column
+// chunks; returns 1 when a wait ran out.  C is rewritten through the
+// calling SM at the end.
+CATN_HDI inline int qr_apply_q_shared(const Team& T, JacobiJob* J, const double* A, long long m, long long n,
+                                      long long lda, const double* tau, double* C, long long ncols, long long ldc) {
+  fence_gpu();
+  unsigned long long seq = job_open(T, J);
+  if (T.leader()) {
+    J->kind = JOB_HOUSE;
+    J->B = (double*)A; J->V = C; J->nrm = nullptr;
+    J->m = (int)m; J->n = (int)ncols; J->ldb = (int)lda; J->ldc = (int)ldc; J->c0 = 0;
+    fence_gpu();
+    J->open = 1;
+    fence_gpu();
+  }
+  T.sync();
+  int timed_out = 0;
+  for (long long k = n - 1; k >= 0 && !timed_out; --k) {
+    const double tk = tau[k];
+    if (tk == 0.0) continue;
+    if (T.leader()) { J->k = (int)k; J->tk = tk; }
+    timed_out = job_round(T, J, seq, (ncols + JOB_CHUNK - 1) / JOB_CHUNK);
+    ++seq;
+  }
+  job_close(T, J, seq);
+  for (long long c = 0; c < ncols; ++c)
+    for (long long i = T.rank(); i < m; i += T.size()) C[i + c * ldc] = ldcg(C + i + c * ldc);
+  T.sync();
+  return timed_out;
+}
+
 #if defined(__CUDACC__)
-// An idle CTA's warps help the shared Jacobi sweeps of the CTAs still
-// contracting, until every instance of the launch has finished (or after a
-// long stretch with nothing to do).
+// A CTA's warps help the shared jobs of the CTAs still contracting, until
+// every instance of the launch has finished (or after a long stretch with
+// nothing to do).
 __device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, const int* finished, int ninst) {
   const int w = (int)blockIdx.x * T.nwarps() + T.warp();
   long long idle = 0;
@@ -728,9 +913,9 @@ __device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, 
     bool worked = false;
     for (int s2 = 0; s2 < nslots && !worked; ++s2) {
       JacobiJob* J = board + (s2 + w) % nslots;
-      const int npair = ldcg_i(&J->npair);
-      if (npair == 0) continue;
-      if ((long long)(ldcg_u(&J->word) & 0xffffffffULL) >= npair) continue;
+      if (!ldcg_i(&J->open)) continue;
+      const unsigned long long word = ldcg_u(&J->word);
+      if ((word & 0xfffffULL) >= ((word >> 20) & 0xfffffULL)) continue;
       job_work(T, J);
       worked = true;
     }

@@ -39,6 +39,8 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   jl.qhead = &qhead;
   jl.ninst = 1;
   jl.min_n = 2;
+  jl.pool = 0;
+  jl.min_qr = 1;
   const char* je = std::getenv("CATN_HOSTCHECK_JOB");
   run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
                sws_doubles, (je && je[0] == '1') ? &jl : nullptr);
