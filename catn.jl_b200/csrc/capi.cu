@@ -67,7 +67,8 @@ namespace {
 // 512-instance spin-glass batch (ms per launch): no pool 471; pool 24 with
 // threshold 48 / 64 / 96 / 128 / 200 / 256: 459 / 437 / 437 / 417-422 / 417 /
 // 477; threshold 128-160 with pool 16 / 24 / 32: 424-426 / 417-426 / 441.
-// CATN_HELPER_CTAS and CATN_SHARED_JACOBI_MIN_N override the two.
+// CATN_HELPER_CTAS and CATN_SHARED_JACOBI_MIN_N override the two, and
+// CATN_SHARED_HOUSE_MIN the element threshold for Householder work.
 constexpr int kSharedJacobiMinN = 128;
 constexpr int kHelperCtas = 24;
 
@@ -79,7 +80,7 @@ constexpr int kHelperCtas = 24;
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue,
-    JacobiJob* board, int nhelp, int share_min_n) {
+    JacobiJob* board, int nhelp, int share_min_n, long long share_min_qr) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
   jl.ninst = ninst;
   jl.min_n = share_min_n;
   jl.pool = nhelp > 0;
-  jl.min_qr = kSharedHouseMinElems;
+  jl.min_qr = share_min_qr;
   if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
     help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
     return;
@@ -189,15 +190,18 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   return CATN_OK;
 }
 
-void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n) {
+void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n, long long* min_qr) {
   int h = pool ? kHelperCtas : 0;
   if (const char* e = std::getenv("CATN_HELPER_CTAS")) h = std::atoi(e);
   if (!R.d_board || h < 0 || 4 * h > R.nslots || 4 * h > R.ninst) h = 0;
   if (R.d_board && R.ngrid > R.nslots) h = R.ngrid - R.nslots;
   int m = kSharedJacobiMinN;
   if (const char* e = std::getenv("CATN_SHARED_JACOBI_MIN_N")) m = std::max(2, std::atoi(e));
+  long long q = kSharedHouseMinElems;
+  if (const char* e = std::getenv("CATN_SHARED_HOUSE_MIN")) q = std::max(1LL, std::atoll(e));
   *nhelp = h;
   *min_n = m;
+  *min_qr = q;
 }
 
 catn_status upload(DeviceRun& R, cudaStream_t st) {
@@ -232,10 +236,11 @@ catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, 4 * sizeof(int), st));
   if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.ngrid, st));
   int nhelp = 0, min_n = 0;
-  helper_config(R, true, &nhelp, &min_n);
+  long long min_qr = 0;
+  helper_config(R, true, &nhelp, &min_n, &min_qr);
   catn_persistent_kernel<<<R.ngrid, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
                                                                 R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
-                                                                R.d_queue, R.d_board, nhelp, min_n);
+                                                                R.d_queue, R.d_board, nhelp, min_n, min_qr);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

@@ -25,7 +25,7 @@ namespace {
 __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, double* gimg, int* queue,
-    JacobiJob* board, int nhelp, int share_min_n) {
+    JacobiJob* board, int nhelp, int share_min_n, long long share_min_qr) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
   jl.ninst = ninst;
   jl.min_n = share_min_n;
   jl.pool = nhelp > 0;
-  jl.min_qr = kSharedHouseMinElems;
+  jl.min_qr = share_min_qr;
   if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
     help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
     return;
@@ -92,14 +92,15 @@ catn_status grad_launch(GradRun* g, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(g->R.d_queue, 0, 4 * sizeof(int), st));
   if (g->R.d_board) CUDA_TRY(cudaMemsetAsync(g->R.d_board, 0, sizeof(JacobiJob) * g->R.ngrid, st));
   int nhelp = 0, min_n = 0;
+  long long min_qr = 0;
   // batch gradient runs keep no helper pool: measured 780 ms with 24 helper
   // CTAs against 731 ms without on the 512-instance batch (the taped
   // instances are long, so the CTAs are worth more as workers)
-  helper_config(g->R, false, &nhelp, &min_n);
+  helper_config(g->R, false, &nhelp, &min_n, &min_qr);
   catn_grad_kernel<<<g->R.ngrid, kThreads, kSmemBytes, st>>>(g->R.d_desc, g->R.d_order, g->R.ninst, g->R.d_i64,
                                                               g->R.d_i32, g->R.d_dat, g->R.d_slots, g->R.L,
                                                               g->R.d_res, g->d_gimg, g->R.d_queue, g->R.d_board,
-                                                              nhelp, min_n);
+                                                              nhelp, min_n, min_qr);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

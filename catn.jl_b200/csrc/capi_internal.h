@@ -77,7 +77,7 @@ catn_status upload(DeviceRun& R, cudaStream_t st);
 // Dedicated helper CTAs of a launch of R and the smallest column count whose
 // Jacobi sweeps are shared (capi.cu).  `pool`: keep the batch helper pool
 // (one network always gets every other resident CTA as a helper).
-void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n);
+void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n, long long* min_qr);
 // Arena of a single network when the caller passes 0 (capi.cu).
 long long default_arena(long long a, const catn_params& p);
 // Frees a gradient run (capi_grad.cu).
