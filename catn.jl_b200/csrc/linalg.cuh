@@ -975,15 +975,21 @@ __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const bool own = lane < nn;
-  // column norms and pivots (lane j owns column j)
+  // Pivoted QR with LPC lanes per column: lane = col + NN * part handles the
+  // rows i = part (mod LPC) of column col; partial sums meet by xor shuffles
+  // in which every lane takes part.
+  constexpr int LPC = 32 / NN;
+  const int col = lane % NN, part = lane / NN;
+  const bool ocol = col < nn;
   double nrm = 0.0;
-  int piv = lane;
-  if (own)
-    for (int i = 0; i < mm; ++i) nrm = fma(W[i + lane * mm], W[i + lane * mm], nrm);
+  int piv = col;
+  if (ocol)
+    for (int i = part; i < mm; i += LPC) nrm = fma(W[i + col * mm], W[i + col * mm], nrm);
+  for (int o = NN; o < 32; o <<= 1) nrm += __shfl_xor_sync(FULL, nrm, o);
   for (int k = 0; k < nn; ++k) {
     // pivot: largest remaining partial norm, smallest index on ties
-    double bv = (own && lane >= k) ? nrm : -1.0;
-    int bi = (own && lane >= k) ? lane : 64;
+    double bv = (ocol && col >= k) ? nrm : -1.0;
+    int bi = (ocol && col >= k) ? col : 64;
     for (int o = 16; o > 0; o >>= 1) {
       const double ov = __shfl_xor_sync(FULL, bv, o);
       const int oi = __shfl_xor_sync(FULL, bi, o);
@@ -998,8 +1004,8 @@ __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau
       }
       const double nk = __shfl_sync(FULL, nrm, k), np = __shfl_sync(FULL, nrm, p);
       const int qk = __shfl_sync(FULL, piv, k), qp = __shfl_sync(FULL, piv, p);
-      if (lane == k) { nrm = np; piv = qp; }
-      if (lane == p) { nrm = nk; piv = qk; }
+      if (col == k) { nrm = np; piv = qp; }
+      if (col == p) { nrm = nk; piv = qk; }
       __syncwarp();
     }
     // Householder reflector for column k (lanes over rows)
@@ -1018,23 +1024,31 @@ __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau
     }
     if (lane == 0) tau[k] = tk;
     __syncwarp();
-    // apply to the columns right of k (lane j owns column j) and update norms
-    if (own && lane > k) {
-      double* aj = W + lane * mm;
-      const double* ak = W + k * mm;
-      if (tk != 0.0) {
-        double w = aj[k];
-        for (int i = k + 1; i < mm; ++i) w = fma(ak[i], aj[i], w);
-        w *= tk;
-        aj[k] -= w;
-        for (int i = k + 1; i < mm; ++i) aj[i] = fma(-w, ak[i], aj[i]);
+    // apply to the columns right of k and recompute their norms
+    const bool act = ocol && col > k;
+    double* aj = W + col * mm;
+    const double* ak = W + k * mm;
+    if (tk != 0.0) {
+      double w = 0.0;
+      if (act)
+        for (int i = k + 1 + part; i < mm; i += LPC) w = fma(ak[i], aj[i], w);
+      for (int o = NN; o < 32; o <<= 1) w += __shfl_xor_sync(FULL, w, o);
+      if (act) w = (w + aj[k]) * tk;
+      __syncwarp();
+      if (act) {
+        if (part == 0) aj[k] -= w;
+        for (int i = k + 1 + part; i < mm; i += LPC) aj[i] = fma(-w, ak[i], aj[i]);
       }
-      double s = 0.0;
-      for (int i = k + 1; i < mm; ++i) s = fma(aj[i], aj[i], s);
-      nrm = s;
+      __syncwarp();
     }
+    double sn = 0.0;
+    if (act)
+      for (int i = k + 1 + part; i < mm; i += LPC) sn = fma(aj[i], aj[i], sn);
+    for (int o = NN; o < 32; o <<= 1) sn += __shfl_xor_sync(FULL, sn, o);
+    if (act) nrm = sn;
     __syncwarp();
   }
+  // lane j (< NN) holds column j's pivot
   if (own) piv_s[lane] = piv;
   // X = R^T: lane j holds column j of X = row j of R
   double x[NN], v[NN];
