@@ -522,8 +522,7 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     // tiny problem: one warp, warp-level synchronisation only
     int sweeps = 0;
     if (T.warp() == 0)
-      sweeps = nn <= 8 ? svd_warp_tiny<8>(s.W, (int)mm, (int)nn, tau, piv, Ut, Vt, Sout, 60)
-                       : svd_warp_tiny<16>(s.W, (int)mm, (int)nn, tau, piv, Ut, Vt, Sout, 60);
+      sweeps = svd_warp_tiny_any(s.W, (int)mm, (int)nn, tau, piv, Ut, Vt, Sout, 60);
     T.sync();
     if (T.leader()) {
       if (sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;

@@ -960,147 +960,224 @@ namespace catn {
 
 #if CATN_DEVICE_PASS
 // ---------------------------------------------------------------------------
-// Tiny SVD by one warp (nn <= NN <= 32, nn <= mm <= 64): the same method as
-// the team path -- pivoted Householder QR W P = Q R, one-sided Jacobi on
-// X = R^T, W = (Q V') Sigma (P U')^T -- with one lane per column, the Jacobi
-// columns held in registers and exchanged by shuffles, and warp-level
-// synchronisation only.  W (column-major, ld mm) is overwritten by the
-// Householder form; outputs: Ut (mm x nn) = Q V'[:, perm], Vt (nn x nn) =
-// P U'[:, perm], Sout (nn, descending).  Returns the sweep count (-1 when the
-// cap was reached).  Must be called by all 32 lanes of one warp.
+// Tiny SVD by one warp (nn <= NN <= 16, nn <= mm <= ME * 32 / NN <= 64): the
+// same method as the team path -- pivoted Householder QR W P = Q R, one-sided
+// Jacobi on X = R^T, W = (Q V') Sigma (P U')^T -- with the whole problem in
+// registers.  Each column is spread over LPC = 32 / NN lanes (lane = column +
+// NN * part holds the rows part + LPC * e), so every lane works and the
+// reductions are xor shuffles over the parts.  Pivoting tracks positions
+// instead of moving columns; the Jacobi rounds pair column j with j ^ m
+// (m = 1 .. NN-1, every pair once per sweep).  W (column-major, ld mm) is
+// overwritten by the Householder form; outputs: Ut (mm x nn) = Q V'[:, perm],
+// Vt (nn x nn) = P U'[:, perm], Sout (nn, descending).  Returns the sweep
+// count (-1 when the cap was reached).  Must be called by all 32 lanes of one
+// warp.
 // ---------------------------------------------------------------------------
-template <int NN>
-__device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau, int* piv_s, double* Ut,
-                                          double* Vt, double* Sout, int max_sweeps) {
-  const unsigned FULL = 0xffffffffu;
+
+// Jacobi rotation for the pair (alpha, beta, gamma) in half-angle form:
+// cos 2t = |d| / r, sin 2t = 2|g| / r (d = beta - alpha, r^2 = d^2 + 4 g^2),
+// c = sqrt((1 + cos 2t) / 2), s = sign(d g) sin 2t / (2c); two reciprocal
+// square roots and no division on the round's critical path.
+__device__ __forceinline__ bool tiny_rotation(double al, double be, double g, double tol, double* c, double* s) {
+  if (al < 1e-250 || be < 1e-250) return false;
+  if (!(g * g > tol * tol * al * be)) return false;
+  const double d = be - al;
+  const double rr = rsqrt(fma(d, d, 4.0 * g * g));
+  const double q = fma(0.5 * fabs(d), rr, 0.5);
+  const double kq = rsqrt(q);
+  *c = q * kq;
+  const double sv = fabs(g) * rr * kq;
+  *s = ((d < 0.0) != (g < 0.0)) ? -sv : sv;
+  return true;
+}
+
+template <int NN, int ME>
+__device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau, int* piv_s, double* Ut, double* Vt,
+                                          double* Sout, int max_sweeps) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int LPC = 32 / NN;                   // lanes per column
+  static_assert(ME * LPC <= 64 && ME >= 1, "rows per lane");   // this lane: rows part + LPC*e, e < ME (mm <= ME*LPC)
+  constexpr int XE = NN >= LPC ? NN / LPC : 1;   // rows of X per lane
+  constexpr int RP = NN < LPC ? NN : LPC;        // parts holding rows of X
   const int lane = threadIdx.x & 31;
-  const bool own = lane < nn;
-  // Pivoted QR with LPC lanes per column: lane = col + NN * part handles the
-  // rows i = part (mod LPC) of column col; partial sums meet by xor shuffles
-  // in which every lane takes part.
-  constexpr int LPC = 32 / NN;
-  const int col = lane % NN, part = lane / NN;
+  const int col = lane & (NN - 1), part = lane / NN;
   const bool ocol = col < nn;
-  double nrm = 0.0;
-  int piv = col;
-  if (ocol)
-    for (int i = part; i < mm; i += LPC) nrm = fma(W[i + col * mm], W[i + col * mm], nrm);
-  for (int o = NN; o < 32; o <<= 1) nrm += __shfl_xor_sync(FULL, nrm, o);
+  // ---- pivoted Householder QR, this lane's rows i = part + LPC*e of column col
+  double a[ME];
+#pragma unroll
+  for (int e = 0; e < ME; ++e) {
+    const int i = part + LPC * e;
+    a[e] = (ocol && i < mm) ? W[i + col * mm] : 0.0;
+  }
+  // nrm: squared norm of the rows >= k, lo: of the rows > k (k = 0 here)
+  double nrm = 0.0, lo = 0.0;
+#pragma unroll
+  for (int e = 0; e < ME; ++e) {
+    const double t = a[e] * a[e];
+    nrm += t;
+    if (part + LPC * e > 0) lo += t;
+  }
+#pragma unroll
+  for (int o = NN; o < 32; o <<= 1) {
+    nrm += __shfl_xor_sync(FULL, nrm, o);
+    lo += __shfl_xor_sync(FULL, lo, o);
+  }
+  int cur = col;   // position of this column in the pivoted order
+  double tau_k = 0.0;   // lane k keeps tau[k]
   for (int k = 0; k < nn; ++k) {
-    // pivot: largest remaining partial norm, smallest index on ties
-    double bv = (ocol && col >= k) ? nrm : -1.0;
-    int bi = (ocol && col >= k) ? col : 64;
-    for (int o = 16; o > 0; o >>= 1) {
+    // pivot: largest remaining norm, smallest position on ties (a total
+    // order, NaN below every number, so every lane reaches the same answer)
+    const bool cand = ocol && cur >= k;
+    double bv = cand ? (nrm == nrm ? nrm : -0.5) : -1.0;
+    int bc = cand ? (cur << 8) | col : (64 << 8);
+#pragma unroll
+    for (int o = 1; o < NN; o <<= 1) {
       const double ov = __shfl_xor_sync(FULL, bv, o);
-      const int oi = __shfl_xor_sync(FULL, bi, o);
-      if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      const int oc = __shfl_xor_sync(FULL, bc, o);
+      if (ov > bv || (ov == bv && oc < bc)) { bv = ov; bc = oc; }
     }
-    const int p = bi;
-    if (p != k && p < nn) {
-      for (int i = lane; i < mm; i += 32) {
-        const double t = W[i + k * mm];
-        W[i + k * mm] = W[i + p * mm];
-        W[i + p * mm] = t;
-      }
-      const double nk = __shfl_sync(FULL, nrm, k), np = __shfl_sync(FULL, nrm, p);
-      const int qk = __shfl_sync(FULL, piv, k), qp = __shfl_sync(FULL, piv, p);
-      if (col == k) { nrm = np; piv = qp; }
-      if (col == p) { nrm = nk; piv = qk; }
-      __syncwarp();
+    const int pc = bc >> 8;
+    if (ocol && pc != k && pc < nn) {
+      if (cur == pc) cur = k;
+      else if (cur == k) cur = pc;
     }
-    // Householder reflector for column k (lanes over rows)
-    double loc = 0.0;
-    for (int i = k + 1 + lane; i < mm; i += 32) loc = fma(W[i + k * mm], W[i + k * mm], loc);
-    for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(FULL, loc, o);
-    const double alpha = W[k + k * mm];
+    const int gk = pc < nn ? (bc & 255) : 0;   // lane of the column now at position k
+    // (pc >= nn cannot happen for k < nn: some column is always a candidate)
+    double mine = 0.0;
+#pragma unroll
+    for (int e = 0; e < ME; ++e)
+      if (part + LPC * e == k) mine = a[e];
+    const double loc = __shfl_sync(FULL, lo, gk);
+    const double alpha = __shfl_sync(FULL, mine, gk + NN * (k & (LPC - 1)));
     double tk = 0.0;
     if (loc > 0.0) {
-      const double beta = -copysign(sqrt(alpha * alpha + loc), alpha);
-      tk = (beta - alpha) / beta;
+      // |beta| = sqrt(alpha^2 + loc), beta = -sign(alpha) |beta|,
+      // tau = (beta - alpha) / beta = 1 + |alpha| / |beta|, scale = 1 / (alpha - beta)
+      const double q = fma(alpha, alpha, loc);
+      const double rq = rsqrt(q);
+      const double nb = q * rq;
+      const double beta = alpha < 0.0 ? nb : -nb;
+      tk = fma(fabs(alpha), rq, 1.0);
       const double sc = 1.0 / (alpha - beta);
-      for (int i = k + 1 + lane; i < mm; i += 32) W[i + k * mm] *= sc;
-      __syncwarp();
-      if (lane == 0) W[k + k * mm] = beta;
-    }
-    if (lane == 0) tau[k] = tk;
-    __syncwarp();
-    // apply to the columns right of k and recompute their norms
-    const bool act = ocol && col > k;
-    double* aj = W + col * mm;
-    const double* ak = W + k * mm;
-    if (tk != 0.0) {
-      double w = 0.0;
-      if (act)
-        for (int i = k + 1 + part; i < mm; i += LPC) w = fma(ak[i], aj[i], w);
-      for (int o = NN; o < 32; o <<= 1) w += __shfl_xor_sync(FULL, w, o);
-      if (act) w = (w + aj[k]) * tk;
-      __syncwarp();
-      if (act) {
-        if (part == 0) aj[k] -= w;
-        for (int i = k + 1 + part; i < mm; i += LPC) aj[i] = fma(-w, ak[i], aj[i]);
-      }
-      __syncwarp();
-    }
-    double sn = 0.0;
-    if (act)
-      for (int i = k + 1 + part; i < mm; i += LPC) sn = fma(aj[i], aj[i], sn);
-    for (int o = NN; o < 32; o <<= 1) sn += __shfl_xor_sync(FULL, sn, o);
-    if (act) nrm = sn;
-    __syncwarp();
-  }
-  // lane j (< NN) holds column j's pivot
-  if (own) piv_s[lane] = piv;
-  // X = R^T: lane j holds column j of X = row j of R
-  double x[NN], v[NN];
+      if (ocol && cur == k) {
 #pragma unroll
-  for (int i = 0; i < NN; ++i) {
-    x[i] = (own && i < nn && i >= lane) ? W[lane + i * mm] : 0.0;
-    v[i] = (i == lane) ? 1.0 : 0.0;
+        for (int e = 0; e < ME; ++e) {
+          const int i = part + LPC * e;
+          if (i > k) a[e] *= sc;
+          else if (i == k) a[e] = beta;
+        }
+      }
+    }
+    if (lane == k) tau_k = tk;
+    const bool act = ocol && cur > k;
+    if (tk != 0.0) {
+      double vk[ME];
+#pragma unroll
+      for (int e = 0; e < ME; ++e) vk[e] = 0.0;
+      double w = 0.0;
+      double w2 = 0.0;
+#pragma unroll
+      for (int e = 0; e < ME; ++e) {
+        const int i = part + LPC * e;
+        const double t = __shfl_sync(FULL, a[e], gk + NN * part);
+        vk[e] = i > k ? t : (i == k ? 1.0 : 0.0);
+        if (e & 1) w2 = fma(vk[e], a[e], w2);
+        else w = fma(vk[e], a[e], w);
+      }
+      w += w2;
+#pragma unroll
+      for (int o = NN; o < 32; o <<= 1) w += __shfl_xor_sync(FULL, w, o);
+      if (act) {
+        w *= tk;
+#pragma unroll
+        for (int e = 0; e < ME; ++e) {
+          a[e] = fma(-w, vk[e], a[e]);
+        }
+      }
+    }
+    // squared norms of the rows > k and > k+1 of the remaining columns
+    double sn = 0.0, sl = 0.0;
+#pragma unroll
+    for (int e = 0; e < ME; ++e) {
+      const int i = part + LPC * e;
+      const double t = a[e] * a[e];
+      if (i > k) sn += t;
+      if (i > k + 1) sl += t;
+    }
+#pragma unroll
+    for (int o = NN; o < 32; o <<= 1) {
+      sn += __shfl_xor_sync(FULL, sn, o);
+      sl += __shfl_xor_sync(FULL, sl, o);
+    }
+    if (act) { nrm = sn; lo = sl; }
   }
-  // unit max-abs scale (numerically-zero columns below 1e-250 are skipped)
+  // Householder form into W (column order of the pivoted matrix), pivots
+#pragma unroll
+  for (int e = 0; e < ME; ++e) {
+    const int i = part + LPC * e;
+    if (ocol && i < mm) W[i + cur * mm] = a[e];
+  }
+  if (ocol && part == 0) piv_s[cur] = col;
+  if (lane < nn) tau[lane] = tau_k;
+  __syncwarp();
+  // ---- one-sided Jacobi on X = R^T; lane holds rows i = part + LPC*e of column col
+  double x[XE], v[XE];
+#pragma unroll
+  for (int e = 0; e < XE; ++e) {
+    const int i = part + LPC * e;
+    x[e] = (ocol && i < nn && i >= col) ? W[col + i * mm] : 0.0;
+    v[e] = (i == col) ? 1.0 : 0.0;
+  }
   double mx = 0.0;
 #pragma unroll
-  for (int i = 0; i < NN; ++i) mx = fmax(mx, fabs(x[i]));
+  for (int e = 0; e < XE; ++e) mx = fmax(mx, fabs(x[e]));
+#pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
   const double sc = mx > 0.0 ? 1.0 / mx : 1.0;
 #pragma unroll
-  for (int i = 0; i < NN; ++i) x[i] *= sc;
-  const int np = (nn % 2) ? nn + 1 : nn;
+  for (int e = 0; e < XE; ++e) x[e] *= sc;
   const double tol = 2.220446049250313e-16 * 16.0;
   int result = -1;
   for (int sweep = 0; sweep < max_sweeps && nn > 1; ++sweep) {
     int rotated = 0;
-    for (int r = 0; r < np - 1; ++r) {
-      int partner = (lane < np) ? rr_partner(np, r, lane) : -1;
-      if (!own || partner >= nn) partner = -1;
-      const int src = partner >= 0 ? partner : lane;
-      // dot products with the partner column (every lane takes part in every shuffle)
-      double a_own = 0.0, a_par = 0.0, g = 0.0;
+    // round m pairs column j with j ^ m: every pair once per sweep
+    for (int m = 1; m < NN; ++m) {
+      int partner = col ^ m;
+      if (!ocol || partner >= nn) partner = -1;
+      const int src = partner >= 0 ? partner + NN * part : lane;
+      double px[XE];
+      double ao = 0.0, ap = 0.0, g = 0.0;
 #pragma unroll
-      for (int i = 0; i < NN; ++i) {
-        const double pxi = __shfl_sync(FULL, x[i], src);
-        a_own = fma(x[i], x[i], a_own);
-        a_par = fma(pxi, pxi, a_par);
-        g = fma(x[i], pxi, g);
+      for (int e = 0; e < XE; ++e) {
+        px[e] = __shfl_sync(FULL, x[e], src);
+        ao = fma(x[e], x[e], ao);
+        ap = fma(px[e], px[e], ap);
+        g = fma(x[e], px[e], g);
+      }
+#pragma unroll
+      for (int o = NN; o < NN * RP; o <<= 1) {
+        ao += __shfl_xor_sync(FULL, ao, o);
+        ap += __shfl_xor_sync(FULL, ap, o);
+        g += __shfl_xor_sync(FULL, g, o);
       }
       bool doit = false, low = false;
       double c = 1.0, s = 0.0;
       if (partner >= 0) {
-        low = lane < partner;
-        const double al = low ? a_own : a_par, be = low ? a_par : a_own;
-        if (jacobi_rotation(al, be, g, tol, &c, &s)) {
+        low = col < partner;
+        if (tiny_rotation(low ? ao : ap, low ? ap : ao, g, tol, &c, &s)) {
           doit = true;
           rotated = 1;
         }
       }
-      // lower column: c*x_lo - s*x_hi ; higher column: s*x_lo + c*x_hi
+      if (__any_sync(FULL, doit)) {
+        const double sl = low ? -s : s;
 #pragma unroll
-      for (int i = 0; i < NN; ++i) {
-        const double pxi = __shfl_sync(FULL, x[i], src);
-        const double pvi = __shfl_sync(FULL, v[i], src);
-        if (doit) {
-          x[i] = low ? c * x[i] - s * pxi : s * pxi + c * x[i];
-          v[i] = low ? c * v[i] - s * pvi : s * pvi + c * v[i];
+        for (int e = 0; e < XE; ++e) {
+          const double pv = __shfl_sync(FULL, v[e], src);
+          if (doit) {
+            x[e] = fma(sl, px[e], c * x[e]);
+            v[e] = fma(sl, pv, c * v[e]);
+          }
         }
       }
     }
@@ -1110,45 +1187,82 @@ __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau
     }
   }
   if (nn <= 1) result = 0;
-  // singular values and descending order
+  // singular values, descending order
   double sg = 0.0;
 #pragma unroll
-  for (int i = 0; i < NN; ++i) sg = fma(x[i], x[i], sg);
-  sg = own ? sqrt(sg) / sc : -1.0;
+  for (int e = 0; e < XE; ++e) sg = fma(x[e], x[e], sg);
+#pragma unroll
+  for (int o = NN; o < NN * RP; o <<= 1) sg += __shfl_xor_sync(FULL, sg, o);
+  sg = __shfl_sync(FULL, ocol ? sqrt(sg) / sc : -1.0, col);   // lanes outside the RP parts take part 0's
   int rank = 0;
   for (int l = 0; l < nn; ++l) {
     const double sl = __shfl_sync(FULL, sg, l);
-    rank += (sl > sg || (sl == sg && l < lane)) ? 1 : 0;
+    rank += (sl > sg || (sl == sg && l < col)) ? 1 : 0;
   }
-  __syncwarp();
-  if (own) {
-    Sout[rank] = sg;
-    // right vectors of W: Vt[piv[i], rank] = X[i, lane] / sigma
+  if (ocol) {
+    if (part == 0) Sout[rank] = sg;
 #pragma unroll
-    for (int i = 0; i < NN; ++i)
-      if (i < nn) Vt[piv_s[i] + rank * nn] = (sg > 0.0) ? (x[i] / sc) / sg : 0.0;
-    // left vectors before Q: Ut[:, rank] = [v; 0]
-#pragma unroll
-    for (int i = 0; i < NN; ++i)
-      if (i < nn) Ut[i + rank * mm] = v[i];
-    for (int i = nn; i < mm; ++i) Ut[i + rank * mm] = 0.0;
+    for (int e = 0; e < XE; ++e) {
+      const int i = part + LPC * e;
+      if (i < nn) Vt[piv_s[i] + rank * nn] = (sg > 0.0) ? (x[e] / sc) / sg : 0.0;
+    }
   }
-  __syncwarp();
-  // Ut <- Q Ut (reflectors in W's lower part), lane c owns column c
+  // Ut[:, rank] = Q [v; 0], reflectors from W
+  double u[ME];
+#pragma unroll
+  for (int e = 0; e < ME; ++e) u[e] = 0.0;
+#pragma unroll
+  for (int e = 0; e < XE; ++e) u[e] = v[e];
   for (int k = nn - 1; k >= 0; --k) {
     const double tk = tau[k];
-    if (own && tk != 0.0) {
-      double* uc = Ut + lane * mm;
-      const double* ak = W + k * mm;
-      double w = uc[k];
-      for (int i = k + 1; i < mm; ++i) w = fma(ak[i], uc[i], w);
+    if (tk != 0.0) {
+      double vk[ME];
+#pragma unroll
+      for (int e = 0; e < ME; ++e) vk[e] = 0.0;
+      double w = 0.0, w2 = 0.0;
+#pragma unroll
+      for (int e = 0; e < ME; ++e) {
+        const int i = part + LPC * e;
+        vk[e] = i > k ? (i < mm ? W[i + k * mm] : 0.0) : (i == k ? 1.0 : 0.0);
+        if (e & 1) w2 = fma(vk[e], u[e], w2);
+        else w = fma(vk[e], u[e], w);
+      }
+      w += w2;
+#pragma unroll
+      for (int o = NN; o < 32; o <<= 1) w += __shfl_xor_sync(FULL, w, o);
       w *= tk;
-      uc[k] -= w;
-      for (int i = k + 1; i < mm; ++i) uc[i] = fma(-w, ak[i], uc[i]);
+#pragma unroll
+      for (int e = 0; e < ME; ++e) {
+        u[e] = fma(-w, vk[e], u[e]);
+      }
     }
-    __syncwarp();
   }
+  if (ocol) {
+#pragma unroll
+    for (int e = 0; e < ME; ++e) {
+      const int i = part + LPC * e;
+      if (i < mm) Ut[i + rank * mm] = u[e];
+    }
+  }
+  __syncwarp();
   return result;
+}
+
+// Dispatch on the column count (NN = next power of two) and the rows per lane.
+__device__ __forceinline__ int svd_warp_tiny_any(double* W, int mm, int nn, double* tau, int* piv, double* Ut,
+                                                 double* Vt, double* S, int max_sweeps) {
+  if (nn <= 2)
+    return mm <= 16 ? svd_warp_tiny<2, 1>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps)
+                    : svd_warp_tiny<2, 4>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps);
+  if (nn <= 4)
+    return mm <= 8    ? svd_warp_tiny<4, 1>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps)
+           : mm <= 16 ? svd_warp_tiny<4, 2>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps)
+                      : svd_warp_tiny<4, 8>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps);
+  if (nn <= 8)
+    return mm <= 16 ? svd_warp_tiny<8, 4>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps)
+                    : svd_warp_tiny<8, 16>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps);
+  return mm <= 32 ? svd_warp_tiny<16, 16>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps)
+                  : svd_warp_tiny<16, 32>(W, mm, nn, tau, piv, Ut, Vt, S, max_sweeps);
 }
 #endif
 
