@@ -383,6 +383,11 @@ CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const d
   if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
   return C.T.bcast(drained) != 0;
 }
+// Blocked application of Q: panel width and the smallest m x ncols product
+// that takes it (with at least two panels of reflectors; below that the
+// per-reflector passes are faster).
+constexpr long long kQPanel = 32;
+constexpr long long kBlockedQMinElems = 8192;
 // qr_apply_q, shared when large; false when a shared wait ran out.
 CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
                              double* Cm, long long ncols, long long ldc) {
@@ -392,6 +397,18 @@ CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, 
       return false;
     }
     return true;
+  }
+  // large products: reflectors in panels of kQPanel (three GEMMs per panel)
+  // when the scratch stack has room, one reflector at a time otherwise
+  if (n >= 2 * kQPanel && m * ncols >= kBlockedQMinElems) {
+    const long long need = (m + 2 * ncols + 2 * kQPanel) * kQPanel;
+    if (C.sp + 8 * need + 512 <= C.sp_hi) {
+      const long long mark = C.sp;
+      double* work = spush(C, need);
+      qr_apply_q_blocked(C.T, A, m, n, lda, tau, Cm, ncols, ldc, kQPanel, work);
+      C.sp = mark;
+      return true;
+    }
   }
   qr_apply_q(C.T, A, m, n, lda, tau, Cm, ncols, ldc);
   return true;

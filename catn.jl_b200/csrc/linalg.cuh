@@ -66,17 +66,32 @@ CATN_HD MOp transposed(double* p, long long ld) { return mop(p, cols_plain(ld), 
 // GEMM: C(M x N) = A(M x K) * B(K x N), overwrite (or C += A * B with accum).
 // ---------------------------------------------------------------------------
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_BK = 16;
-constexpr int GEMM_STAGE_BYTES = (GEMM_BM + GEMM_BN) * GEMM_BK * 8;
+// Shared tiles are [BK][BM + 1] and [BK][BN + 1]: the padding keeps the
+// k-fastest tile loads (operands whose k index is the unit-stride one) free
+// of bank conflicts.
+constexpr int GEMM_LDA = GEMM_BM + 1, GEMM_LDB = GEMM_BN + 1;
+constexpr int GEMM_STAGE_BYTES = (GEMM_LDA + GEMM_LDB) * GEMM_BK * 8;
+
+// Whether consecutive indices of the map are (mostly) consecutive addresses.
+CATN_HD bool unit_stride(const IMap& m) { return m.n1 == 1 ? m.s2 == 1 : m.s1 == 1; }
 
 CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, const MOp& A,
                           const MOp& B, const MOp& C, bool accum = false) {
   if (M <= 0 || N <= 0) return;
 #if CATN_DEVICE_PASS
   if (T.size() == 256 && T.stage_bytes >= GEMM_STAGE_BYTES && M * N >= 256) {
-    double* sA = (double*)T.stage;            // [BK][BM]
-    double* sB = sA + GEMM_BK * GEMM_BM;      // [BK][BN]
+    double* sA = (double*)T.stage;            // [BK][LDA]
+    double* sB = sA + GEMM_BK * GEMM_LDA;     // [BK][LDB]
     const int tid = T.rank();
-    const int tx = tid & 15, ty = tid >> 4;   // 16 x 16 threads, 4 x 4 outputs each
+    // tile loads: consecutive threads walk the operand's unit-stride index
+    const bool a_kfast = !unit_stride(A.R) && unit_stride(A.C);
+    const bool b_kfast = unit_stride(B.R) && !unit_stride(B.C);
+    // 16 x 16 threads, each with the 4 x 4 outputs (tr + 16 x, tc + 16 y);
+    // with a column-major C the fast thread index walks the rows, so the
+    // stores are coalesced
+    const bool c_rows = unit_stride(C.R);
+    const int tr = c_rows ? (tid & 15) : (tid >> 4);
+    const int tc = c_rows ? (tid >> 4) : (tid & 15);
     for (long long m0 = 0; m0 < M; m0 += GEMM_BM) {
       for (long long n0 = 0; n0 < N; n0 += GEMM_BN) {
         double acc[4][4];
@@ -86,23 +101,27 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
           for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
         for (long long k0 = 0; k0 < K; k0 += GEMM_BK) {
           for (int e = tid; e < GEMM_BK * GEMM_BM; e += 256) {
-            int kk = e / GEMM_BM, mm = e - kk * GEMM_BM;
+            int kk, mm;
+            if (a_kfast) { kk = e & (GEMM_BK - 1); mm = e / GEMM_BK; }
+            else { kk = e / GEMM_BM; mm = e - kk * GEMM_BM; }
             long long r = m0 + mm, k = k0 + kk;
-            sA[e] = (r < M && k < K) ? A.ld(r, k) : 0.0;
+            sA[kk * GEMM_LDA + mm] = (r < M && k < K) ? A.ld(r, k) : 0.0;
           }
           for (int e = tid; e < GEMM_BK * GEMM_BN; e += 256) {
-            int kk = e / GEMM_BN, nn = e - kk * GEMM_BN;
+            int kk, nn;
+            if (b_kfast) { kk = e & (GEMM_BK - 1); nn = e / GEMM_BK; }
+            else { kk = e / GEMM_BN; nn = e - kk * GEMM_BN; }
             long long c = n0 + nn, k = k0 + kk;
-            sB[e] = (c < N && k < K) ? B.ld(k, c) : 0.0;
+            sB[kk * GEMM_LDB + nn] = (c < N && k < K) ? B.ld(k, c) : 0.0;
           }
           __syncthreads();
 #pragma unroll 4
           for (int kk = 0; kk < GEMM_BK; ++kk) {
             double a[4], b[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) a[q] = sA[kk * GEMM_BM + ty * 4 + q];
+            for (int q = 0; q < 4; ++q) a[q] = sA[kk * GEMM_LDA + tr + 16 * q];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) b[q] = sB[kk * GEMM_BN + tx * 4 + q];
+            for (int q = 0; q < 4; ++q) b[q] = sB[kk * GEMM_LDB + tc + 16 * q];
 #pragma unroll
             for (int x = 0; x < 4; ++x)
 #pragma unroll
@@ -112,11 +131,11 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
         }
 #pragma unroll
         for (int x = 0; x < 4; ++x) {
-          long long r = m0 + ty * 4 + x;
+          long long r = m0 + tr + 16 * x;
           if (r >= M) continue;
 #pragma unroll
           for (int y = 0; y < 4; ++y) {
-            long long c = n0 + tx * 4 + y;
+            long long c = n0 + tc + 16 * y;
             if (c < N) C.ref(r, c) = accum ? C.ref(r, c) + acc[x][y] : acc[x][y];
           }
         }
@@ -324,25 +343,79 @@ CATN_HDI inline void qr_apply_q(const Team& T, const double* A, long long m, lon
   }
 }
 
+// qr_apply_q by panels of up to b reflectors (compact WY form): the panel
+// H_k0 ... H_k0+kb-1 equals I - V T V^T with V (rows k0..m-1) unit lower
+// trapezoidal and T upper triangular, T_jj = tau_j and T[0:j, j] =
+// -tau_j T[0:j, 0:j] (V[:, 0:j]^T v_j).  N = -T obeys the same recurrence
+// with N_jj = -tau_j, so C[k0:m] += V (N (V^T C[k0:m])): three GEMMs per
+// panel instead of one pass over C per reflector.  Panels go last to first
+// (Q = H_0 H_1 ... H_{n-1}).  work: (m + 2 ncols + 2 b) b doubles.
+CATN_HDI inline void qr_apply_q_blocked(const Team& T, const double* A, long long m, long long n, long long lda,
+                                        const double* tau, double* C, long long ncols, long long ldc, long long b,
+                                        double* work) {
+  double* Vp = work;           // mp x kb, ld mp
+  double* G = Vp + m * b;      // kb x kb: V^T V
+  double* Nm = G + b * b;      // kb x kb: -T
+  double* Y = Nm + b * b;      // kb x ncols: V^T C, then Y2 = N Y
+  double* Y2 = Y + b * ncols;
+  for (long long p = (n + b - 1) / b - 1; p >= 0; --p) {
+    const long long k0 = p * b, kb = (n - k0 < b) ? n - k0 : b, mp = m - k0;
+    for (long long e = T.rank(); e < mp * kb; e += T.size()) {
+      long long i, j;
+      divmod(e, mp, &i, &j);
+      Vp[e] = (i > j) ? A[k0 + i + (k0 + j) * lda] : (i == j ? 1.0 : 0.0);
+    }
+    for (long long e = T.rank(); e < kb * kb; e += T.size()) Nm[e] = 0.0;
+    T.sync();
+    gemm(T, kb, kb, mp, transposed(Vp, mp), colmajor(Vp, mp), colmajor(G, kb));
+    for (long long j = 0; j < kb; ++j) {
+      const double tj = tau[k0 + j];
+      for (long long i = T.rank(); i <= j; i += T.size()) {
+        double s = 0.0;
+        for (long long l = i; l < j; ++l) s = fma(Nm[i + l * kb], G[l + j * kb], s);
+        Nm[i + j * kb] = -tj * (i == j ? 1.0 : s);
+      }
+      T.sync();
+    }
+    gemm(T, kb, ncols, mp, transposed(Vp, mp), colmajor(C + k0, ldc), colmajor(Y, kb));
+    gemm(T, kb, ncols, kb, colmajor(Nm, kb), colmajor(Y, kb), colmajor(Y2, kb));
+    gemm(T, mp, ncols, kb, colmajor(Vp, mp), colmajor(Y2, kb), colmajor(C + k0, ldc), true);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // One-sided Jacobi on B (m x n, m >= n, col-major ld ldb), accumulating V
 // (n x n, ld n).  Columns of B converge to U * diag(S).  Returns the number
 // of sweeps, or -1 when the sweep cap was reached.
 // ---------------------------------------------------------------------------
+// 1 / sqrt(x) (the host build divides).
+CATN_HD double rsqrt_d(double x) {
+#if CATN_DEVICE_PASS
+  return rsqrt(x);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+
 // Jacobi rotation annihilating the off-diagonal g of the 2x2 Gram block
-// [[al, g], [g, be]] (Rutishauser's formula): returns false when the pair is
-// already orthogonal to tolerance (g^2 <= tol^2 al be) or a column is
-// numerically zero; otherwise c = cos, s = sin with
-// t = sign(d g) 2|g| / (|d| + sqrt(d^2 + 4 g^2)), d = be - al.
-CATN_HD bool jacobi_rotation(double al, double be, double g, double tol, double* c, double* s) {
+// [[al, g], [g, be]]: returns false when the pair is already orthogonal to
+// tolerance (g^2 <= tol^2 al be) or a column is numerically zero; otherwise
+// c = cos, s = sin of the angle with tan = t = sign(d g) 2|g| / (|d| + r),
+// d = be - al, r^2 = d^2 + 4 g^2, in half-angle form: cos 2a = |d| / r,
+// c = sqrt((1 + cos 2a) / 2), s = sign(d g) |g| / (r c), t = s / c -- two
+// reciprocal square roots and no division (d == 0 takes the sign of g).
+CATN_HD bool jacobi_rotation(double al, double be, double g, double tol, double* c, double* s, double* t = nullptr) {
   if (al < 1e-250 || be < 1e-250) return false;
   if (!(g * g > tol * tol * al * be)) return false;
   const double d = be - al;
-  double t = (2.0 * fabs(g)) / (fabs(d) + sqrt(d * d + 4.0 * g * g));
-  if ((d < 0.0) != (g < 0.0)) t = -t;   // sign(d * g); d == 0 takes the sign of g
-  const double cc = 1.0 / sqrt(1.0 + t * t);
-  *c = cc;
-  *s = cc * t;
+  const double rr = rsqrt_d(fma(d, d, 4.0 * g * g));   // 1 / r
+  const double q = fma(0.5 * fabs(d), rr, 0.5);        // c^2
+  const double kq = rsqrt_d(q);                          // 1 / c
+  const double sv = fabs(g) * rr * kq;
+  const double sg = ((d < 0.0) != (g < 0.0)) ? -sv : sv;
+  *c = q * kq;
+  *s = sg;
+  if (t) *t = sg * kq;
   return true;
 }
 
@@ -422,9 +495,9 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
         }
         g0 = T.wsum(g0);
         g1 = T.wsum(g1);
-        double c0 = 1.0, s0 = 0.0, c1 = 1.0, s1 = 0.0;
-        const bool r0 = a0 && jacobi_rotation(nrm[p0], nrm[q0], g0, tol, &c0, &s0);
-        const bool r1 = a1 && jacobi_rotation(nrm[p1], nrm[q1], g1, tol, &c1, &s1);
+        double c0 = 1.0, s0 = 0.0, t0 = 0.0, c1 = 1.0, s1 = 0.0, t1 = 0.0;
+        const bool r0 = a0 && jacobi_rotation(nrm[p0], nrm[q0], g0, tol, &c0, &s0, &t0);
+        const bool r1 = a1 && jacobi_rotation(nrm[p1], nrm[q1], g1, tol, &c1, &s1, &t1);
         if (!r0 && !r1) continue;
         rotated = 1;
         T.wsync();
@@ -459,14 +532,12 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
         T.wsync();
         if (T.lane() == 0) {
           if (r0) {
-            const double t = s0 / c0;
-            nrm[p0] -= t * g0;
-            nrm[q0] += t * g0;
+            nrm[p0] -= t0 * g0;
+            nrm[q0] += t0 * g0;
           }
           if (r1) {
-            const double t = s1 / c1;
-            nrm[p1] -= t * g1;
-            nrm[q1] += t * g1;
+            nrm[p1] -= t1 * g1;
+            nrm[q1] += t1 * g1;
           }
         }
         T.wsync();
@@ -550,8 +621,8 @@ CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double*
   for (long long i = T.lane(); i < m; i += T.wsize()) g = fma(ldcg(bp + i), ldcg(bq + i), g);
   g = T.wsum(g);
   const double al = ldcg(nrm + p), be = ldcg(nrm + q);
-  double c, s;
-  if (!jacobi_rotation(al, be, g, tol, &c, &s)) return false;
+  double c, s, t;
+  if (!jacobi_rotation(al, be, g, tol, &c, &s, &t)) return false;
   for (long long i = T.lane(); i < m; i += T.wsize()) {
     const double x = ldcg(bp + i), y = ldcg(bq + i);
     stcg(bp + i, c * x - s * y);
@@ -566,7 +637,6 @@ CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double*
   }
   T.wsync();
   if (T.lane() == 0) {
-    const double t = s / c;
     stcg(nrm + p, al - t * g);
     stcg(nrm + q, be + t * g);
   }
@@ -905,25 +975,66 @@ CATN_HDI inline int qr_apply_q_shared(const Team& T, JacobiJob* J, const double*
 // A CTA's warps help the shared jobs of the CTAs still contracting, until
 // every instance of the launch has finished (or after a long stretch with
 // nothing to do).
+// Whether J is open with unclaimed items of its current round (warp-uniform:
+// lane 0's view).
+__device__ __forceinline__ bool job_has_items(const JacobiJob* J) {
+  int open = ldcg_i(&J->open);
+  unsigned long long word = ldcg_u(&J->word);
+  open = __shfl_sync(0xffffffffu, open, 0);
+  word = __shfl_sync(0xffffffffu, word, 0);
+  return open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
+}
+
+// Polls (of about 1 us each) that a helper warp keeps watching the job it
+// last worked on for that job's next round before it scans the board again.
+constexpr int kJobStickPolls = 64;
+
 __device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, const int* finished, int ninst) {
+  const unsigned FULL = 0xffffffffu;
   const int w = (int)blockIdx.x * T.nwarps() + T.warp();
+  const int lane = T.lane();
   long long idle = 0;
   while (idle < (1LL << 22)) {
     if (ldcg_i(finished) >= ninst) return;
-    bool worked = false;
-    for (int s2 = 0; s2 < nslots && !worked; ++s2) {
-      JacobiJob* J = board + (s2 + w) % nslots;
-      if (!ldcg_i(&J->open)) continue;
-      const unsigned long long word = ldcg_u(&J->word);
-      if ((word & 0xfffffULL) >= ((word >> 20) & 0xfffffULL)) continue;
-      job_work(T, J);
-      worked = true;
+    // find a job with unclaimed items: the lanes check 32 slots at once
+    // (independent L2 loads), starting at a warp-specific block so that
+    // helpers spread over the open jobs
+    const int nblk = (nslots + 31) / 32;
+    int pick = -1;
+    for (int b = 0; b < nblk && pick < 0; ++b) {
+      const int base = ((b + w) % nblk) * 32;
+      const int s = base + lane;
+      bool ok = false;
+      if (s < nslots) {
+        const JacobiJob* J = board + s;
+        const int open = ldcg_i(&J->open);
+        const unsigned long long word = ldcg_u(&J->word);
+        ok = open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
+      }
+      const unsigned mask = __ballot_sync(FULL, ok);
+      if (mask) {
+        const int r = w & 31;   // first candidate at or after lane r (cyclically)
+        const unsigned hi = mask & (~0u << r);
+        pick = base + __ffs(hi ? hi : mask) - 1;
+      }
     }
-    if (worked) {
-      idle = 0;
-    } else {
+    if (pick < 0) {
       ++idle;
       __nanosleep(256);
+      continue;
+    }
+    idle = 0;
+    JacobiJob* J = board + pick;
+    job_work(T, J);
+    // stay with J: its owner opens the next round within microseconds
+    for (int t = 0; t < kJobStickPolls; ++t) {
+      if (job_has_items(J)) {
+        job_work(T, J);
+        t = -1;
+        continue;
+      }
+      if (!ldcg_i(&J->open)) break;
+      __nanosleep(32);
     }
   }
 }
@@ -973,23 +1084,6 @@ namespace catn {
 // count (-1 when the cap was reached).  Must be called by all 32 lanes of one
 // warp.
 // ---------------------------------------------------------------------------
-
-// Jacobi rotation for the pair (alpha, beta, gamma) in half-angle form:
-// cos 2t = |d| / r, sin 2t = 2|g| / r (d = beta - alpha, r^2 = d^2 + 4 g^2),
-// c = sqrt((1 + cos 2t) / 2), s = sign(d g) sin 2t / (2c); two reciprocal
-// square roots and no division on the round's critical path.
-__device__ __forceinline__ bool tiny_rotation(double al, double be, double g, double tol, double* c, double* s) {
-  if (al < 1e-250 || be < 1e-250) return false;
-  if (!(g * g > tol * tol * al * be)) return false;
-  const double d = be - al;
-  const double rr = rsqrt(fma(d, d, 4.0 * g * g));
-  const double q = fma(0.5 * fabs(d), rr, 0.5);
-  const double kq = rsqrt(q);
-  *c = q * kq;
-  const double sv = fabs(g) * rr * kq;
-  *s = ((d < 0.0) != (g < 0.0)) ? -sv : sv;
-  return true;
-}
 
 template <int NN, int ME>
 __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau, int* piv_s, double* Ut, double* Vt,
@@ -1164,7 +1258,7 @@ __device__ __noinline__ int svd_warp_tiny(double* W, int mm, int nn, double* tau
       double c = 1.0, s = 0.0;
       if (partner >= 0) {
         low = col < partner;
-        if (tiny_rotation(low ? ao : ap, low ? ap : ao, g, tol, &c, &s)) {
+        if (jacobi_rotation(low ? ao : ap, low ? ap : ao, g, tol, &c, &s)) {
           doit = true;
           rotated = 1;
         }
