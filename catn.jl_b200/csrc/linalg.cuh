@@ -198,6 +198,98 @@ CATN_HDI inline double maxabs(const Team& T, const double* x, long long n) {
 }
 
 // ---------------------------------------------------------------------------
+// Householder reflector H = I - tk v v^T (v = [1 at row k; v[k+1:m]]) applied
+// to the columns j0 <= j < j1 of X (ld ldx); with nrm, the squared norm of
+// rows k+1..m-1 of each updated column goes to nrm[j] in the same pass.
+// Each warp takes NC columns at a time, so their loads are in flight together.
+// ---------------------------------------------------------------------------
+template <int NC>
+CATN_HDI inline void house_apply_cols_n(const Team& T, const double* v, long long k, long long m, double tk,
+                                        double* X, long long ldx, long long j0, long long j1, double* nrm) {
+  for (long long jb = j0 + NC * T.warp(); jb < j1; jb += NC * T.nwarps()) {
+    double* c[NC];
+    bool on[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) {
+      on[q] = jb + q < j1;
+      c[q] = X + (on[q] ? jb + q : jb) * ldx;
+    }
+    double w[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) w[q] = 0.0;
+    if (tk != 0.0) {
+      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) {
+        const double vi = v[i];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) w[q] = fma(vi, c[q][i], w[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < NC; ++q) w[q] = (T.wsum(w[q]) + c[q][k]) * tk;
+      T.wsync();
+    }
+    double s[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) s[q] = 0.0;
+    if (tk != 0.0) {
+      // two rows of every column per trip, all loads issued before the
+      // stores (the columns may alias as far as the compiler knows)
+      for (long long i0 = k + 1 + T.lane(); i0 < m; i0 += 2 * T.wsize()) {
+        const long long i1 = i0 + T.wsize();
+        const bool h1 = i1 < m;
+        const double v0 = v[i0], v1 = h1 ? v[i1] : 0.0;
+        double x0[NC], x1[NC];
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          x0[q] = c[q][i0];
+          x1[q] = h1 ? c[q][i1] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          x0[q] = fma(-w[q], v0, x0[q]);
+          x1[q] = fma(-w[q], v1, x1[q]);
+          s[q] = fma(x0[q], x0[q], s[q]);
+          s[q] = fma(x1[q], x1[q], s[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < NC; ++q) {
+          if (!on[q]) continue;
+          c[q][i0] = x0[q];
+          if (h1) c[q][i1] = x1[q];
+        }
+      }
+    } else if (nrm) {
+      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) {
+#pragma unroll
+        for (int q = 0; q < NC; ++q) s[q] = fma(c[q][i], c[q][i], s[q]);
+      }
+    }
+    if (nrm) {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) s[q] = T.wsum(s[q]);
+    }
+    T.wsync();
+    if (T.lane() == 0) {
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        if (!on[q]) continue;
+        if (tk != 0.0) c[q][k] -= w[q];
+        if (nrm) nrm[jb + q] = s[q];
+      }
+    }
+    T.wsync();
+  }
+}
+// Columns per warp: enough columns for every warp first, then up to four.
+CATN_HDI inline void house_apply_cols(const Team& T, const double* v, long long k, long long m, double tk,
+                                      double* X, long long ldx, long long j0, long long j1, double* nrm) {
+  if (tk == 0.0 && !nrm) return;
+  const long long per = (j1 - j0) / T.nwarps();
+  if (per >= 4) house_apply_cols_n<4>(T, v, k, m, tk, X, ldx, j0, j1, nrm);
+  else if (per >= 2) house_apply_cols_n<2>(T, v, k, m, tk, X, ldx, j0, j1, nrm);
+  else house_apply_cols_n<1>(T, v, k, m, tk, X, ldx, j0, j1, nrm);
+}
+
+// ---------------------------------------------------------------------------
 // Householder QR, m >= n, in place (LAPACK dgeqr2 semantics).
 // ---------------------------------------------------------------------------
 CATN_HDI inline void qr_inplace(const Team& T, double* A, long long m, long long n, long long lda,
@@ -219,19 +311,9 @@ CATN_HDI inline void qr_inplace(const Team& T, double* A, long long m, long long
     }
     if (T.leader()) tau[k] = tk;
     T.sync();
-    if (tk != 0.0) {
+    if (tk != 0.0 && k + 1 < n) {
       // A[k:m, j] -= tk * v * (v^T A[k:m, j]),  v = [1; A[k+1:m, k]]
-      for (long long j = k + 1 + T.warp(); j < n; j += T.nwarps()) {
-        double* aj = A + j * lda;
-        double w = 0.0;
-        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], aj[i], w);
-        w = T.wsum(w) + aj[k];
-        w *= tk;
-        T.wsync();
-        if (T.lane() == 0) aj[k] -= w;
-        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) aj[i] -= w * ak[i];
-        T.wsync();
-      }
+      house_apply_cols(T, ak, k, m, tk, A, lda, k + 1, n, nullptr);
       T.sync();
     }
   }
@@ -297,25 +379,10 @@ CATN_HDI inline long long qrcp_inplace(const Team& T, double* A, long long m, lo
     }
     if (T.leader()) tau[k] = tk;
     T.sync();
-    for (long long j = k + 1 + T.warp(); j < n; j += T.nwarps()) {
-      double* aj = A + j * lda;
-      if (tk != 0.0) {
-        double w = 0.0;
-        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], aj[i], w);
-        w = T.wsum(w) + aj[k];
-        w *= tk;
-        T.wsync();
-        if (T.lane() == 0) aj[k] -= w;
-        for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) aj[i] -= w * ak[i];
-        T.wsync();
-      }
-      double s = 0.0;
-      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) s = fma(aj[i], aj[i], s);
-      s = T.wsum(s);
-      if (T.lane() == 0) nrm[j] = s;
-      T.wsync();
+    if (k + 1 < n) {
+      house_apply_cols(T, ak, k, m, tk, A, lda, k + 1, n, nrm);
+      T.sync();
     }
-    T.sync();
   }
   return n;
 }
@@ -327,18 +394,7 @@ CATN_HDI inline void qr_apply_q(const Team& T, const double* A, long long m, lon
   for (long long k = n - 1; k >= 0; --k) {
     double tk = tau[k];
     if (tk == 0.0) continue;
-    const double* ak = A + k * lda;
-    for (long long j = T.warp(); j < ncols; j += T.nwarps()) {
-      double* cj = C + j * ldc;
-      double w = 0.0;
-      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ak[i], cj[i], w);
-      w = T.wsum(w) + cj[k];
-      w *= tk;
-      T.wsync();
-      if (T.lane() == 0) cj[k] -= w;
-      for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) cj[i] -= w * ak[i];
-      T.wsync();
-    }
+    house_apply_cols(T, A + k * lda, k, m, tk, C, ldc, 0, ncols, nullptr);
     T.sync();
   }
 }
