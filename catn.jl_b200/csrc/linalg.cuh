@@ -664,8 +664,15 @@ CATN_HD void job_set_word(JacobiJob* J, unsigned long long w) {
 #endif
 }
 
+// Rows per lane of the register-resident pair rotation (columns up to
+// kPairRows warps long).
+constexpr int kPairRows = 8;
+
 // Pair pi of round r (round-robin order) on B (m x n) and V (n x n) with
-// the squared norms in nrm; warp-level.  Returns whether it rotated.
+// the squared norms in nrm; warp-level.  Returns whether it rotated.  With
+// m, n <= kPairRows * warp size every load (both columns of B and of V, both
+// norms) is issued at once and the columns stay in registers for the
+// rotation, so a pair costs one L2 round trip instead of one per row block.
 CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double* nrm, long long m, long long n,
                                     long long ldb, long long np, long long r, long long pi, double tol) {
   long long p, q;
@@ -673,23 +680,51 @@ CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double*
   if (p >= n || q >= n) return false;
   double* bp = B + p * ldb;
   double* bq = B + q * ldb;
-  double g = 0.0;
-  for (long long i = T.lane(); i < m; i += T.wsize()) g = fma(ldcg(bp + i), ldcg(bq + i), g);
-  g = T.wsum(g);
-  const double al = ldcg(nrm + p), be = ldcg(nrm + q);
-  double c, s, t;
-  if (!jacobi_rotation(al, be, g, tol, &c, &s, &t)) return false;
-  for (long long i = T.lane(); i < m; i += T.wsize()) {
-    const double x = ldcg(bp + i), y = ldcg(bq + i);
-    stcg(bp + i, c * x - s * y);
-    stcg(bq + i, s * x + c * y);
-  }
   double* vp = V + p * n;
   double* vq = V + q * n;
-  for (long long i = T.lane(); i < n; i += T.wsize()) {
-    const double x = ldcg(vp + i), y = ldcg(vq + i);
-    stcg(vp + i, c * x - s * y);
-    stcg(vq + i, s * x + c * y);
+  const double al = ldcg(nrm + p), be = ldcg(nrm + q);
+  double c, s, t, g = 0.0;
+  const long long ws = T.wsize();
+  if (m <= ws * kPairRows && n <= ws * kPairRows) {
+    double xp[kPairRows], xq[kPairRows], yp[kPairRows], yq[kPairRows];
+#pragma unroll
+    for (int e = 0; e < kPairRows; ++e) {
+      const long long i = T.lane() + ws * e;
+      xp[e] = i < m ? ldcg(bp + i) : 0.0;
+      xq[e] = i < m ? ldcg(bq + i) : 0.0;
+      yp[e] = i < n ? ldcg(vp + i) : 0.0;
+      yq[e] = i < n ? ldcg(vq + i) : 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < kPairRows; ++e) g = fma(xp[e], xq[e], g);
+    g = T.wsum(g);
+    if (!jacobi_rotation(al, be, g, tol, &c, &s, &t)) return false;
+#pragma unroll
+    for (int e = 0; e < kPairRows; ++e) {
+      const long long i = T.lane() + ws * e;
+      if (i < m) {
+        stcg(bp + i, c * xp[e] - s * xq[e]);
+        stcg(bq + i, s * xp[e] + c * xq[e]);
+      }
+      if (i < n) {
+        stcg(vp + i, c * yp[e] - s * yq[e]);
+        stcg(vq + i, s * yp[e] + c * yq[e]);
+      }
+    }
+  } else {
+    for (long long i = T.lane(); i < m; i += T.wsize()) g = fma(ldcg(bp + i), ldcg(bq + i), g);
+    g = T.wsum(g);
+    if (!jacobi_rotation(al, be, g, tol, &c, &s, &t)) return false;
+    for (long long i = T.lane(); i < m; i += T.wsize()) {
+      const double x = ldcg(bp + i), y = ldcg(bq + i);
+      stcg(bp + i, c * x - s * y);
+      stcg(bq + i, s * x + c * y);
+    }
+    for (long long i = T.lane(); i < n; i += T.wsize()) {
+      const double x = ldcg(vp + i), y = ldcg(vq + i);
+      stcg(vp + i, c * x - s * y);
+      stcg(vq + i, s * x + c * y);
+    }
   }
   T.wsync();
   if (T.lane() == 0) {
