@@ -62,15 +62,18 @@ namespace {
 
 // Batch launches keep kHelperCtas CTAs that only help the large SVDs of the
 // others, and open the Jacobi sweeps of SVDs with at least kSharedJacobiMinN
-// columns to them: a launch lasts as long as its slowest instance, whose
-// time is mostly the Jacobi sweeps of such SVDs.  Measured on the
-// 512-instance spin-glass batch (ms per launch): no pool 471; pool 24 with
-// threshold 48 / 64 / 96 / 128 / 200 / 256: 459 / 437 / 437 / 417-422 / 417 /
-// 477; threshold 128-160 with pool 16 / 24 / 32: 424-426 / 417-426 / 441.
+// columns to them: a launch lasts as long as its slowest instance (whose
+// largest SVDs dominate it) or as the work left to the other CTAs, whichever
+// is longer.  Measured on the
+// 512-instance spin-glass batch (ms per launch, with shared Jacobi pairs held
+// in registers): pool 8 / 12 / 16 / 20 / 24 at threshold 128: 309 / 306 / 307
+// / 316 / 324; pool 16 at threshold 64 / 96: 312 / 312.  The pool's size
+// trades the slowest instance (320 ms at 8, 290 ms at 24) against the work
+// left to the other CTAs.
 // CATN_HELPER_CTAS and CATN_SHARED_JACOBI_MIN_N override the two, and
 // CATN_SHARED_HOUSE_MIN the element threshold for Householder work.
 constexpr int kSharedJacobiMinN = 128;
-constexpr int kHelperCtas = 24;
+constexpr int kHelperCtas = 16;
 
 // `order` lists instance ids by descending work estimate, so the longest
 // contractions start first (longest-processing-time scheduling).  With a job
