@@ -79,6 +79,32 @@ CATN_HDI inline void gemm(const Team& T, long long M, long long N, long long K, 
                           const MOp& B, const MOp& C, bool accum = false) {
   if (M <= 0 || N <= 0) return;
 #if CATN_DEVICE_PASS
+  if (T.size() == 256 && M * N <= 1024 && 8 * (M * K + K * N) <= T.stage_bytes) {
+    // small products: gather both operands into shared memory at once (one
+    // round trip), then one output per thread (k ascending, as below)
+    double* sA = (double*)T.stage;   // M x K, ld M
+    double* sB = sA + M * K;         // K x N, ld K
+    for (long long e = T.rank(); e < M * K; e += 256) {
+      long long r, k;
+      divmod(e, M, &r, &k);
+      sA[e] = A.ld(r, k);
+    }
+    for (long long e = T.rank(); e < K * N; e += 256) {
+      long long k, c;
+      divmod(e, K, &k, &c);
+      sB[e] = B.ld(k, c);
+    }
+    __syncthreads();
+    for (long long e = T.rank(); e < M * N; e += 256) {
+      long long r, c;
+      divmod(e, M, &r, &c);
+      double s = 0.0;
+      for (long long k = 0; k < K; ++k) s = fma(sA[r + k * M], sB[k + c * K], s);
+      C.ref(r, c) = accum ? C.ref(r, c) + s : s;
+    }
+    __syncthreads();
+    return;
+  }
   if (T.size() == 256 && T.stage_bytes >= GEMM_STAGE_BYTES && M * N >= 256) {
     double* sA = (double*)T.stage;            // [BK][LDA]
     double* sB = sA + GEMM_BK * GEMM_LDA;     // [BK][LDB]
