@@ -9,8 +9,12 @@ Workload (one "step" = one persistent-kernel pass over one batch):
   value  instances/s with the inputs already in HBM (CUDA events around the
          kernel launch; L2 flushed by a 256 MiB write between steps)
   e2e    instances/s through the public batch API per step: pinned
-         host->device copy of the packed inputs, the launch, device->host
-         read of every instance's result (CUDA events on the same stream)
+         host->device copy of the step's inputs (every instance's couplings,
+         fields and beta; the lattices are fixed at batch creation), the
+         device rebuild of the site tensors, the launch, and the
+         device->host read of every instance's result (CUDA events on the
+         same stream).  `e2e.full_image` times the same path with the whole
+         host-built network image uploaded instead.
 
   grad   the other half of the metric: d lnZ / d w and d lnZ / d h (every
          <s_i s_j>, <s_k> of every instance) from one device gradient run
@@ -297,6 +301,7 @@ def main():
         batch.launch(sh)
         batch.fetch(sh)
     res = batch.fetch(sh)
+    res_ref = [catn_lib.Result.from_buffer_copy(x) for x in res]
     flops = sum(r.flops for r in res)
     nbytes = sum(r.bytes for r in res)
     steps_per_inst = [r.nsteps for r in res]
@@ -317,27 +322,47 @@ def main():
             times.append(a.elapsed_time(b) / 1000.0)
         batch.fetch(sh)
         # --- end-to-end timing through the public API ---
-        e2e_times = []
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            if dist:
-                dist.barrier()
-            torch.cuda.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            batch.upload(sh)
-            batch.launch(sh)
-            batch.fetch(sh)
-            b.record(stream)
-            torch.cuda.synchronize()
-            e2e_times.append(a.elapsed_time(b) / 1000.0)
+        # the step's inputs: every instance's couplings, fields and beta in
+        # pinned host memory (the lattices were fixed at batch creation)
+        pw = torch.tensor(np.concatenate([np.asarray(d["weights"], float) for d in insts]),
+                          dtype=torch.float64).pin_memory()
+        ph = torch.tensor(np.concatenate([np.asarray(d["fields"], float) for d in insts]),
+                          dtype=torch.float64).pin_memory()
+        pb = torch.tensor([float(d["beta"]) for d in insts], dtype=torch.float64).pin_memory()
+        pw_np, ph_np, pb_np = pw.numpy(), ph.numpy(), pb.numpy()
+
+        def e2e_run(full_image):
+            ts = []
+            for _ in range(args.steps):
+                flush.fill_(1.0)
+                if dist:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                if full_image:
+                    batch.upload(sh)
+                else:
+                    batch.set_params(pw_np, ph_np, pb_np, sh)
+                batch.launch(sh)
+                batch.fetch(sh)
+                b.record(stream)
+                torch.cuda.synchronize()
+                ts.append(a.elapsed_time(b) / 1000.0)
+            return ts
+
+        e2e_times = e2e_run(False)
+        e2e_res = batch.fetch(sh)
+        e2e_check = max(abs(x.lnZ - y.lnZ) / max(1.0, abs(y.lnZ)) for x, y in zip(e2e_res, res_ref))
+        e2e_full_times = e2e_run(True)   # last: leaves the host-built networks on the device
     total = sum(times)
     total_e2e = sum(e2e_times)
+    total_full = sum(e2e_full_times)
     if dist:
-        t = torch.tensor([total, total_e2e], dtype=torch.float64, device="cuda")
+        t = torch.tensor([total, total_e2e, total_full], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total, total_e2e = float(t[0]), float(t[1])
+        total, total_e2e, total_full = float(t[0]), float(t[1]), float(t[2])
     units = args.instances * world * args.steps
     value = units / total
     e2e_value = units / total_e2e
@@ -359,9 +384,15 @@ def main():
                    "l2": "flushed (256 MiB write) between timed steps", "slots": batch.slots,
                    "contraction_steps_total": int(sum(steps_per_inst))},
         "e2e": {"value": round(e2e_value, 3), "unit": "instances/s",
-                "h2d_bytes_per_step": int(batch.input_bytes),
-                "d2h_bytes_per_step": int(args.instances * ctypes.sizeof(catn_lib.Result))},
-        "gpu_launches": 2 * args.steps,
+                "h2d_bytes_per_step": int(batch.param_bytes),
+                "d2h_bytes_per_step": int(args.instances * ctypes.sizeof(catn_lib.Result)),
+                "inputs": "couplings, fields and beta of every instance (pinned host -> device); site tensors "
+                          "rebuilt on the device (catn_ising_batch_set_params)",
+                "max_rel_dlnZ_vs_host_built": float(e2e_check),
+                "full_image": {"value": round(units / total_full, 3), "unit": "instances/s",
+                               "h2d_bytes_per_step": int(batch.input_bytes),
+                               "inputs": "the whole host-built network image (catn_batch_upload)"}},
+        "gpu_launches": 4 * args.steps,
         "roofline": {"bound": "hbm", "achieved": round(achieved_gbs, 3), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved_gbs / peak, 6), "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",

@@ -63,6 +63,10 @@ SIGNATURES = {
     "catn_batch_slots": ([ct.c_void_p], ct.c_int32),
     "catn_batch_input_bytes": ([ct.c_void_p], ct.c_int64),
     "catn_batch_destroy": ([ct.c_void_p], ct.c_int),
+    "catn_ising_batch_set_params": ([ct.c_void_p, _P, _P, _P, ct.c_void_p], ct.c_int),
+    "catn_ising_batch_randomize": ([ct.c_void_p, ct.c_uint64, ct.c_double, ct.c_double, ct.c_void_p], ct.c_int),
+    "catn_ising_batch_get_params": ([ct.c_void_p, _P, _P, _P], ct.c_int),
+    "catn_ising_batch_param_bytes": ([ct.c_void_p], ct.c_int64),
     "catn_braket_create": ([ct.POINTER(Params), ct.c_int32, _P, _P, _P, _P, ct.c_int64, ct.POINTER(ct.c_void_p)],
                            ct.c_int),
     "catn_ising_grad": ([ct.c_void_p, ct.POINTER(Result), _P, _P, ct.c_int32], ct.c_int),

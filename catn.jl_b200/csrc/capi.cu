@@ -248,6 +248,76 @@ catn_status launch(DeviceRun& R, cudaStream_t st) {
   return CATN_OK;
 }
 
+// Site tensors of an Ising batch rebuilt from the batch's device copies of
+// couplings, fields and betas (ising_build.cuh), one recipe per thread.
+__global__ void catn_ising_fill_kernel(const IsingSiteRecipe* rec, long long nrec, const double* w,
+                                       const double* h, const double* beta, double* dat) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nrec;
+       q += (long long)gridDim.x * blockDim.x) {
+    const IsingSiteRecipe r = rec[q];
+    double v[8];
+    const int c = ising_site_values(r, r.edge >= 0 ? w[r.edge] : 0.0, h[r.node], beta[r.inst], v);
+    for (int k = 0; k < c; ++k) dat[r.dat + k] = v[k];
+  }
+}
+
+// Couplings sigma_w N(0,1) (stream 0) and fields sigma_h N(0,1) (stream 1).
+__global__ void catn_disorder_kernel(unsigned long long seed, double sigma_w, double sigma_h, double* w,
+                                     long long nw, double* h, long long nh) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nw || q < nh;
+       q += (long long)gridDim.x * blockDim.x) {
+    if (q < nw) w[q] = sigma_w * disorder_normal(seed, 0, (unsigned long long)q);
+    if (q < nh) h[q] = sigma_h * disorder_normal(seed, 1, (unsigned long long)q);
+  }
+}
+
+catn_status params_restore(catn_batch* b, cudaStream_t st);
+
+// Device copies of the creation parameters and the site recipes.
+catn_status params_prepare(catn_batch* b, const double* weights, const double* fields, const double* betas,
+                           long long nw, long long nh, long long nb) {
+  IsingParams& P = b->ip;
+  P.nrec = (long long)b->im.recipes.size();
+  P.nw = nw;
+  P.nh = nh;
+  P.nb = nb;
+  if (P.nrec == 0) return CATN_OK;
+  CUDA_TRY(cudaMalloc(&P.d_rec, sizeof(IsingSiteRecipe) * P.nrec));
+  CUDA_TRY(cudaMalloc(&P.d_w, sizeof(double) * std::max(nw, 1LL)));
+  CUDA_TRY(cudaMalloc(&P.d_h, sizeof(double) * std::max(nh, 1LL)));
+  CUDA_TRY(cudaMalloc(&P.d_beta, sizeof(double) * std::max(nb, 1LL)));
+  CUDA_TRY(cudaMemcpy(P.d_rec, b->im.recipes.data(), sizeof(IsingSiteRecipe) * P.nrec, cudaMemcpyHostToDevice));
+  return params_restore(b, nullptr);
+}
+// The device parameter copies back to the creation values (the host image
+// holds the networks built from them).
+catn_status params_restore(catn_batch* b, cudaStream_t st) {
+  IsingParams& P = b->ip;
+  std::vector<double> w, h, be;
+  for (const IsingSpec& sp : b->im.ising) {
+    w.insert(w.end(), sp.w.begin(), sp.w.end());
+    h.insert(h.end(), sp.h.begin(), sp.h.end());
+    be.push_back(sp.beta);
+  }
+  if ((long long)w.size() != P.nw || (long long)h.size() != P.nh || (long long)be.size() != P.nb)
+    return fail(CATN_ESTATE, "batch parameter counts disagree with its instances");
+  if (P.nw > 0) CUDA_TRY(cudaMemcpyAsync(P.d_w, w.data(), sizeof(double) * P.nw, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(P.d_h, h.data(), sizeof(double) * P.nh, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(P.d_beta, be.data(), sizeof(double) * P.nb, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  P.on_device = false;
+  return CATN_OK;
+}
+// Rebuild every site from the device parameters.
+catn_status params_fill(catn_batch* b, cudaStream_t st) {
+  IsingParams& P = b->ip;
+  const int grid = (int)std::min<long long>((P.nrec + 255) / 256, 4096);
+  catn_ising_fill_kernel<<<grid > 0 ? grid : 1, 256, 0, st>>>(P.d_rec, P.nrec, P.d_w, P.d_h, P.d_beta, b->R.d_dat);
+  CUDA_TRY(cudaGetLastError());
+  P.on_device = true;
+  return CATN_OK;
+}
+
 }  // namespace
 
 
@@ -415,12 +485,18 @@ catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const 
     if (pins) { pos1 = pins[4 * q]; val1 = pins[4 * q + 1]; pos2 = pins[4 * q + 2]; val2 = pins[4 * q + 3]; }
     int tc = p->trace ? 2 * ne + 16 : 0;
     std::string e = b->im.add_ising(*p, n_nodes[q], ne, edges + 2 * e0, weights + e0, fields + node_off[q],
-                                    betas[q], pos1, val1, pos2, val2, tc);
+                                    betas[q], pos1, val1, pos2, val2, tc, e0, node_off[q]);
     if (!e.empty()) { delete b; return fail(CATN_EINVAL, "instance " + std::to_string(q) + ": " + e); }
   }
   long long arena = slot_arena_bytes > 0 ? slot_arena_bytes : (128LL << 20);
   b->arena = arena;
   if (catn_status s = prepare(b->im, arena, max_slots, b->R)) {
+    b->R.release();
+    delete b;
+    return s;
+  }
+  if (catn_status s = params_prepare(b, weights, fields, betas, edge_off[n_inst], node_off[n_inst], n_inst)) {
+    b->ip.release();
     b->R.release();
     delete b;
     return s;
@@ -431,7 +507,50 @@ catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const 
 
 catn_status catn_batch_upload(catn_batch* b, void* stream) {
   if (!b) return fail(CATN_EINVAL, "NULL batch");
-  return upload(b->R, (cudaStream_t)stream);
+  if (catn_status s = upload(b->R, (cudaStream_t)stream)) return s;
+  if (b->ip.on_device) {   // back to the networks given at creation
+    if (catn_status s = params_restore(b, (cudaStream_t)stream)) return s;
+  }
+  return CATN_OK;
+}
+
+catn_status catn_ising_batch_set_params(catn_batch* b, const double* weights, const double* fields,
+                                        const double* betas, void* stream) {
+  if (!b || !fields || (!weights && b->ip.nw > 0)) return fail(CATN_EINVAL, "NULL argument");
+  if (!b->ip.d_rec) return fail(CATN_EINVAL, "not an Ising batch");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (b->ip.nw > 0)
+    CUDA_TRY(cudaMemcpyAsync(b->ip.d_w, weights, sizeof(double) * b->ip.nw, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(b->ip.d_h, fields, sizeof(double) * b->ip.nh, cudaMemcpyHostToDevice, st));
+  if (betas) CUDA_TRY(cudaMemcpyAsync(b->ip.d_beta, betas, sizeof(double) * b->ip.nb, cudaMemcpyHostToDevice, st));
+  return params_fill(b, st);
+}
+
+catn_status catn_ising_batch_randomize(catn_batch* b, uint64_t seed, double sigma_w, double sigma_h,
+                                       void* stream) {
+  if (!b) return fail(CATN_EINVAL, "NULL batch");
+  if (!b->ip.d_rec) return fail(CATN_EINVAL, "not an Ising batch");
+  if (!(sigma_w >= 0.0) || !(sigma_h >= 0.0)) return fail(CATN_EINVAL, "sigma_w and sigma_h must be >= 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long n = std::max(b->ip.nw, b->ip.nh);
+  const int grid = (int)std::min<long long>((n + 255) / 256, 4096);
+  catn_disorder_kernel<<<grid > 0 ? grid : 1, 256, 0, st>>>(seed, sigma_w, sigma_h, b->ip.d_w, b->ip.nw, b->ip.d_h,
+                                                            b->ip.nh);
+  CUDA_TRY(cudaGetLastError());
+  return params_fill(b, st);
+}
+
+catn_status catn_ising_batch_get_params(const catn_batch* b, double* weights, double* fields, double* betas) {
+  if (!b || !fields || !betas || (!weights && b->ip.nw > 0)) return fail(CATN_EINVAL, "NULL argument");
+  if (!b->ip.d_rec) return fail(CATN_EINVAL, "not an Ising batch");
+  if (b->ip.nw > 0) CUDA_TRY(cudaMemcpy(weights, b->ip.d_w, sizeof(double) * b->ip.nw, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(fields, b->ip.d_h, sizeof(double) * b->ip.nh, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(betas, b->ip.d_beta, sizeof(double) * b->ip.nb, cudaMemcpyDeviceToHost));
+  return CATN_OK;
+}
+
+int64_t catn_ising_batch_param_bytes(const catn_batch* b) {
+  return b ? (int64_t)(sizeof(double) * (b->ip.nw + b->ip.nh + b->ip.nb)) : 0;
 }
 
 catn_status catn_batch_launch(catn_batch* b, void* stream) {
@@ -462,6 +581,7 @@ int64_t catn_batch_input_bytes(const catn_batch* b) { return b ? b->R.input_byte
 
 catn_status catn_batch_destroy(catn_batch* b) {
   if (!b) return CATN_OK;
+  b->ip.release();
   grad_release(b->grad);
   b->R.release();
   delete b;

@@ -168,6 +168,10 @@ catn_status catn_ising_grad(catn_net* net, catn_result* res, double* dlnZ_dw, do
 catn_status catn_batch_grad_launch(catn_batch* b, void* stream) {
   if (!b) return fail(CATN_EINVAL, "NULL batch");
   if (catn_status s = check_ising_only(b->im)) return s;
+  if (b->ip.on_device)
+    return fail(CATN_ESTATE,
+                "gradients use the parameters given at creation: catn_batch_upload restores them, or create a "
+                "batch from the new parameters");
   if (catn_status s = grad_prepare(b->im, b->grad ? b->grad->arena : grad_arena(b->arena, b->R.nslots), b->R.nslots,
                                       b->grad)) return s;
   return grad_launch(b->grad, (cudaStream_t)stream);

@@ -94,11 +94,31 @@ struct catn_net {
   catn_capi::GradRun* grad = nullptr;
 };
 
+namespace catn_capi {
+// Device-side disorder of an Ising batch (catn_ising_batch_set_params /
+// _randomize): the site recipes recorded at creation, the current couplings,
+// fields and betas, and whether the device image holds values rebuilt from
+// them instead of the ones given at creation.
+struct IsingParams {
+  catn::IsingSiteRecipe* d_rec = nullptr;
+  double* d_w = nullptr;
+  double* d_h = nullptr;
+  double* d_beta = nullptr;
+  long long nrec = 0, nw = 0, nh = 0, nb = 0;
+  bool on_device = false;
+  void release() {
+    cudaFree(d_rec); cudaFree(d_w); cudaFree(d_h); cudaFree(d_beta);
+    d_rec = nullptr; d_w = d_h = d_beta = nullptr;
+  }
+};
+}  // namespace catn_capi
+
 struct catn_batch {
   catn::Image im;
   catn_capi::DeviceRun R;
   long long arena = 0;
   catn_capi::GradRun* grad = nullptr;
+  catn_capi::IsingParams ip;
 };
 
 #define CUDA_TRY(expr)                                                \

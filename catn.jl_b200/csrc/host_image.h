@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 #include "catn_layout.h"
+#include "ising_build.cuh"
 
 namespace catn {
 
@@ -32,6 +33,9 @@ struct Image {
   int smax = 0;       // largest per-node site / neighbour count at load
   long long trace_total = 0;
   std::vector<IsingSpec> ising;   // Ising instances, in the order added
+  // Site recipes of the Ising instances added with recording on
+  // (ising_build.cuh), in image order.
+  std::vector<IsingSiteRecipe> recipes;
 
   // Network in MPS form.  Returns an error message or "".
   std::string add_mps(const catn_params& P, int n, const int* site_counts, const int* nbr_counts,
@@ -278,9 +282,12 @@ struct Image {
   // ising_network (src/ising.jl:20-227): one site per incident edge, B =
   // exp(beta w s_i s_j) on the first endpoint, identity on the second, field
   // folded into the first (or leaf) site, degree-0 spins as 2cosh(beta h).
+  // With rec_edge_base >= 0 one recipe per site goes to `recipes`, its
+  // coupling and field indices offset by rec_edge_base and rec_node_base
+  // (the instance's place in the batch's weights and fields).
   std::string add_ising(const catn_params& P, int n, int n_edges, const int* edges, const double* w,
                         const double* h, double beta, int pos1, int val1, int pos2, int val2,
-                        int trace_cap) {
+                        int trace_cap, long long rec_edge_base = -1, long long rec_node_base = -1) {
     if (n < 1) return "ising_network: n must be >= 1";
     std::vector<int> degree(n + 1, 0);
     for (int e = 0; e < n_edges; ++e) {
@@ -294,6 +301,27 @@ struct Image {
     struct Site { int dl, d, dr; double v[8]; };
     std::vector<std::vector<Site>> mps(n + 1);
     std::vector<std::vector<int>> nbr(n + 1);
+    const bool record = rec_edge_base >= 0;
+    std::vector<std::vector<IsingSiteRecipe>> rec(record ? n + 1 : 0);
+    // the site layout build_site picks for `node` (leaf / first / last / interior)
+    auto layout_of = [&](int node) -> int {
+      if (degree[node] == 1) return 0;
+      if (nbr[node].empty()) return 1;
+      if ((int)nbr[node].size() == degree[node] - 1) return 2;
+      return 3;
+    };
+    auto recipe = [&](int e, int node, int role, const double* own, const double* other) {
+      IsingSiteRecipe r;
+      std::memset(&r, 0, sizeof(r));
+      r.edge = e < 0 ? -1 : (int)(rec_edge_base + e);
+      r.node = (int)(rec_node_base + node - 1);
+      r.inst = (int)desc.size();
+      r.role = (signed char)role;
+      r.layout = (signed char)(role == 2 ? 0 : layout_of(node));
+      if (own) { r.s_own[0] = (signed char)own[0]; r.s_own[1] = (signed char)own[1]; }
+      if (other) { r.s_other[0] = (signed char)other[0]; r.s_other[1] = (signed char)other[1]; }
+      rec[node].push_back(r);
+    };
     auto build_site = [&](int node, double field_diag[2], const double Q[2][2]) -> Site {
       Site s;
       std::memset(&s, 0, sizeof(s));
@@ -335,9 +363,11 @@ struct Image {
       for (int a = 0; a < 2; ++a)
         for (int b = 0; b < 2; ++b) B[a][b] = std::exp(beta * w[e] * (si[a] * sj[b]));
       double fi[2] = {std::exp(beta * h[i - 1] * si[0]), std::exp(beta * h[i - 1] * si[1])};
+      if (record) recipe(e, i, 0, si, sj);
       mps[i].push_back(build_site(i, fi, B));
       nbr[i].push_back(j);
       double fj[2] = {std::exp(beta * h[j - 1] * sj[0]), std::exp(beta * h[j - 1] * sj[1])};
+      if (record) recipe(e, j, 1, sj, si);
       mps[j].push_back(build_site(j, fj, I2));
       nbr[j].push_back(i);
     }
@@ -352,11 +382,14 @@ struct Image {
         s.dl = s.d = s.dr = 1;
         s.v[0] = std::exp(beta * h[k - 1]) + std::exp(-beta * h[k - 1]);
         mps[k].push_back(s);
+        if (record) recipe(-1, k, 2, nullptr, nullptr);
       }
       sc[k - 1] = (int)mps[k].size();
       nc[k - 1] = (int)nbr[k].size();
       cn[k - 1] = (int)mps[k].size();
-      for (const Site& s : mps[k]) {
+      for (size_t q0 = 0; q0 < mps[k].size(); ++q0) {
+        const Site& s = mps[k][q0];
+        if (record) rec[k][q0].dat = (long long)data.size();   // made absolute below
         dims.push_back(s.dl);
         dims.push_back(s.d);
         dims.push_back(s.dr);
@@ -365,6 +398,14 @@ struct Image {
       for (int v : nbr[k]) nb.push_back(v);
     }
     std::string err = add_mps(P, n, sc.data(), nc.data(), cn.data(), dims.data(), data.data(), nb.data(), trace_cap);
+    if (err.empty() && record) {
+      const long long base = desc.back().data_off;
+      for (int k = 1; k <= n; ++k)
+        for (IsingSiteRecipe r : rec[k]) {
+          r.dat += base;
+          recipes.push_back(r);
+        }
+    }
     if (err.empty()) {
       IsingSpec sp;
       sp.n = n;

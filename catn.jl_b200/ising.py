@@ -155,6 +155,47 @@ class IsingBatch:
         L.check(self.lib, self.lib.catn_batch_run(self.handle, self.results))
         return self.results
 
+    def set_params(self, weights, fields, betas=None, stream=None):
+        """New couplings, fields (and betas) for every instance, same lattices
+        and pins: concatenated in instance order like the constructor's
+        input.  Only these arrays go to the device, where the site tensors are
+        rebuilt; ``launch`` then contracts the new networks (``upload``
+        restores the networks given at construction)."""
+        a = self._arrays
+        w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1)
+        h = np.ascontiguousarray(fields, dtype=np.float64).reshape(-1)
+        if w.size != int(a[2][-1]) or h.size != int(a[1][-1]):
+            raise ValueError(f"set_params: expected {int(a[2][-1])} weights and {int(a[1][-1])} fields, "
+                             f"got {w.size} and {h.size}")
+        b = None
+        if betas is not None:
+            b = np.ascontiguousarray(betas, dtype=np.float64).reshape(-1)
+            if b.size != self.size:
+                raise ValueError(f"set_params: expected {self.size} betas, got {b.size}")
+        self._params_keep = (w, h, b)   # alive until the asynchronous copy has run
+        L.check(self.lib, self.lib.catn_ising_batch_set_params(self.handle, L.ptr(w) if w.size else None, L.ptr(h),
+                                                               L.ptr(b) if b is not None else None, stream))
+
+    def randomize(self, seed, sigma_w=1.0, sigma_h=0.0, stream=None):
+        """Disorder generated on the device: weights ~ sigma_w N(0,1), fields ~
+        sigma_h N(0,1) (counter-based generator keyed by ``seed``), site
+        tensors rebuilt there."""
+        L.check(self.lib, self.lib.catn_ising_batch_randomize(self.handle, int(seed) & (2 ** 64 - 1),
+                                                              float(sigma_w), float(sigma_h), stream))
+
+    def params(self):
+        """The device's current (weights, fields, betas), concatenated."""
+        a = self._arrays
+        w = np.zeros(max(int(a[2][-1]), 1))
+        h = np.zeros(int(a[1][-1]))
+        b = np.zeros(self.size)
+        L.check(self.lib, self.lib.catn_ising_batch_get_params(self.handle, L.ptr(w), L.ptr(h), L.ptr(b)))
+        return w[:int(a[2][-1])], h, b
+
+    @property
+    def param_bytes(self):
+        return self.lib.catn_ising_batch_param_bytes(self.handle)
+
     def grad_launch(self, stream=None):
         """Upload and start the gradient run of every instance (one launch)."""
         L.check(self.lib, self.lib.catn_batch_grad_launch(self.handle, stream))

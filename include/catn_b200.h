@@ -181,6 +181,34 @@ catn_status catn_ising_batch_create(const catn_params* p, int32_t n_inst, const 
                                     const int32_t* pins, int64_t slot_arena_bytes,
                                     int32_t max_slots, catn_batch** out);
 
+/* No counterpart in the reference, which rebuilds every network on the host
+ * (ising_network, src/ising.jl:20-227).  New couplings, fields and inverse
+ * temperatures for the instances of a batch made by catn_ising_batch_create,
+ * with the same lattices and pins: weights in the order of the edges at
+ * creation (all instances), fields likewise, betas one per instance (NULL =
+ * keep).  Only these arrays cross to the device; a kernel rebuilds every site
+ * tensor there (the builder's values, src/ising.jl:95-183), and the next
+ * catn_batch_launch contracts the new networks.  catn_batch_upload restores
+ * the networks given at creation; gradient launches need those
+ * (CATN_ESTATE otherwise).  `stream` is a cudaStream_t (NULL = default). */
+catn_status catn_ising_batch_set_params(catn_batch* b, const double* weights, const double* fields,
+                                        const double* betas, void* stream);
+
+/* No counterpart in the reference.  Disorder generated on the device:
+ * weights sigma_w * N(0,1), fields sigma_h * N(0,1) (betas kept), from a
+ * counter-based generator keyed by `seed` (SplitMix64 mixing, Box-Muller),
+ * then the site tensors rebuilt as by catn_ising_batch_set_params. */
+catn_status catn_ising_batch_randomize(catn_batch* b, uint64_t seed, double sigma_w, double sigma_h,
+                                       void* stream);
+
+/* The batch's current couplings, fields and betas (device copies; sizes as
+ * in catn_ising_batch_set_params).  Synchronous. */
+catn_status catn_ising_batch_get_params(const catn_batch* b, double* weights, double* fields, double* betas);
+
+/* Bytes that catn_ising_batch_set_params copies host->device (all three
+ * arrays). */
+int64_t catn_ising_batch_param_bytes(const catn_batch* b);
+
 /* Upload the inputs of the batch (host -> HBM), run the persistent kernel,
  * read back the per-instance results.  Timing-friendly split below. */
 catn_status catn_batch_run(catn_batch* b, catn_result* results);

@@ -121,4 +121,53 @@ int catn_hostcheck_dense(const catn_params* p, int n, const int* ndims, const lo
   return run_image(im, arena_bytes, res, trace);
 }
 
+// Ising site recipes (ising_build.cuh) checked on the host: the batch is
+// built from (w, h, betas) with recipes recorded, the recipes are evaluated
+// with (w2, h2, betas2), and the values are compared with a batch built
+// directly from (w2, h2, betas2).  Returns the recipe count (-1 on a build
+// error); *maxdiff is the largest absolute difference, *covered the number
+// of distinct image values the recipes wrote, *total the image size.
+long long catn_hostcheck_ising_recipes(const catn_params* p, int n_inst, const int* n_nodes,
+                                       const long long* node_off, const long long* edge_off, const int* edges,
+                                       const double* w, const double* h, const double* betas, const double* w2,
+                                       const double* h2, const double* betas2, const int* pins, double* maxdiff,
+                                       long long* covered, long long* total) {
+  Image A, B;
+  for (int q = 0; q < n_inst; ++q) {
+    const long long e0 = edge_off[q], ne = edge_off[q + 1] - e0;
+    const int* pq = pins + 4 * q;
+    if (!A.add_ising(*p, n_nodes[q], (int)ne, edges + 2 * e0, w + e0, h + node_off[q], betas[q], pq[0], pq[1],
+                     pq[2], pq[3], 0, e0, node_off[q]).empty())
+      return -1;
+    if (!B.add_ising(*p, n_nodes[q], (int)ne, edges + 2 * e0, w2 + e0, h2 + node_off[q], betas2[q], pq[0], pq[1],
+                     pq[2], pq[3], 0).empty())
+      return -1;
+  }
+  if (A.dat.size() != B.dat.size()) return -1;
+  std::vector<char> hit(A.dat.size(), 0);
+  double md = 0.0;
+  long long cov = 0;
+  for (const IsingSiteRecipe& r : A.recipes) {
+    double v[8];
+    const int c = ising_site_values(r, r.edge >= 0 ? w2[r.edge] : 0.0, h2[r.node], betas2[r.inst], v);
+    for (int k = 0; k < c; ++k) {
+      const double d = std::fabs(v[k] - B.dat[r.dat + k]);
+      if (!(d <= md)) md = d;
+      if (!hit[r.dat + k]) {
+        hit[r.dat + k] = 1;
+        ++cov;
+      }
+    }
+  }
+  *maxdiff = md;
+  *covered = cov;
+  *total = (long long)A.dat.size();
+  return (long long)A.recipes.size();
+}
+
+// The device disorder generator's formula evaluated on the host.
+double catn_hostcheck_disorder_normal(unsigned long long seed, unsigned long long stream, unsigned long long index) {
+  return disorder_normal(seed, stream, index);
+}
+
 }
