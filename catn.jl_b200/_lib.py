@@ -28,7 +28,7 @@ class Params(ct.Structure):
     _fields_ = [("Dmax", ct.c_int32), ("chi", ct.c_int32), ("cutoff", ct.c_double),
                 ("norm_method", ct.c_int32), ("select", ct.c_int32), ("reverse", ct.c_int32),
                 ("svdopt", ct.c_int32), ("swapopt", ct.c_int32), ("compress", ct.c_int32),
-                ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32)]
+                ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32), ("rsvd", ct.c_int32)]
 
 
 class Result(ct.Structure):
@@ -116,7 +116,7 @@ def ptr(a):
 
 
 def make_params(Dmax=32, chi=32, cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True,
-                swapopt=True, compress=False, cut_bond=False, seed=1, trace=False):
+                swapopt=True, compress=False, cut_bond=False, seed=1, trace=False, rsvd=0):
     return Params(int(Dmax), int(chi), float(cutoff), int(norm_method), int(select), int(bool(reverse)),
                   int(bool(svdopt)), int(bool(swapopt)), int(bool(compress)), int(bool(cut_bond)),
-                  int(seed), int(bool(trace)))
+                  int(seed), int(bool(trace)), int(rsvd))

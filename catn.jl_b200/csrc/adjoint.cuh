@@ -411,6 +411,7 @@ CATN_HDI inline void run_instance_grad(const Team& T, char* slot, const SlotLayo
                                        const JobLink* jl = nullptr) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
   C.multigraph = D.multigraph;
+  C.rsvd_min = D.rsvd_min;
   if (jl) {
     C.job = jl->job;
     C.qhead = jl->qhead;

@@ -296,6 +296,7 @@ CATN_HDI inline void run_instance_braket(const Team& T, char* slot, const SlotLa
                                          const long long* i64, const int* i32, const double* dat, catn_result* res,
                                          int* trace_base, double* sws, long long sws_doubles) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
+  C.rsvd_min = D.rsvd_min;
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {
     C.trace = trace_base + D.trace_off;

@@ -53,6 +53,7 @@ catn_status check_params(const catn_params* p) {
   if (p->norm_method < 0 || p->norm_method > 2) return fail(CATN_EINVAL, "norm_method must be 0, 1 or 2");
   if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
   if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
+  if (p->rsvd < 0 || p->rsvd > 1) return fail(CATN_EINVAL, "rsvd must be 0 or 1");
   return CATN_OK;
 }
 
@@ -337,6 +338,7 @@ void catn_params_default(catn_params* p) {
   p->cut_bond = 0;
   p->seed = 1;
   p->trace = 0;
+  p->rsvd = 0;
 }
 
 static catn_status net_finish(catn_net* net, long long arena_bytes, catn_net** out) {

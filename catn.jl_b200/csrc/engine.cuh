@@ -25,6 +25,7 @@
 //   contraction! .............. tensor_network.jl:556-717   -> contract
 #pragma once
 #include "linalg.cuh"
+#include "ising_build.cuh"
 #include "catn_layout.h"
 
 namespace catn {
@@ -88,6 +89,8 @@ struct Ctx {
   double* ldc;    // per-node logdim cache [n+1]
   long long* ldv; // cache validity [n+1]
   int status;     // uniform copy of the instance status
+  int rsvd_min;   // randomized-SVD route threshold override (0: 7000 / 20000)
+  int rsvd_calls; // randomized SVDs so far (selects each sketch's generator stream)
   int multigraph; // the input lists some neighbour twice
   int* trace;
   int trace_cap;
@@ -745,6 +748,76 @@ CATN_HDI inline void cano_to(Ctx& C, int k, int idx) {
 }
 
 // ---------------------------------------------------------------------------
+// Thin Q (m x min(m, c)) of the Householder QR of A (m x c, m >= c,
+// overwritten by the factorisation).
+CATN_HDI inline bool thin_q(Ctx& C, double* A, long long m, long long c, double* tau, double* Q) {
+  const Team& T = C.T;
+  qr_inplace(T, A, m, c, m, tau);
+  for (long long e = T.rank(); e < m * c; e += T.size()) {
+    long long r, j;
+    divmod(e, m, &r, &j);
+    Q[e] = (r == j) ? 1.0 : 0.0;
+  }
+  T.sync();
+  return apply_q(C, A, m, c, m, tau, Q, c, m);
+}
+
+// The reference's randomized SVD (linalg_utils.jl:44-58) of the swap
+// matrix M (m x n, the oriented input `in`), with its Gaussian sketch from
+// the counter-based generator keyed by (P.seed, this instance's call
+// count): G (n x p, p = min(n, 10 k)), Y = M G, ten rounds of Y <- thin Q
+// of M (M^T Y), Q = thin Q of Y, B = Q^T M = Ub S Vb^T (exact), U = Q Ub;
+// the first min(k, rank B) triplets.  Needs m >= p (the thin Q of a wide
+// sketch is not formed; the caller takes the exact route then).
+CATN_HDI inline Svd rsvd_swap(Ctx& C, const SvdIn& in, long long m, long long n, long long k) {
+  const Team& T = C.T;
+  Svd R;
+  R.m = m; R.n = n; R.p = 0; R.U = R.S = R.V = nullptr;
+  // M out of the shared-memory workspace, which the SVD of B reuses
+  double* Wm = in.W;
+  if (in.smem) {
+    Wm = spush(C, m * n);
+    if (failed(C)) return R;
+    copy(T, Wm, in.W, m * n);
+  }
+  const MOp M = in.wide ? transposed(Wm, in.mm) : colmajor(Wm, in.mm);
+  const MOp Mt = in.wide ? colmajor(Wm, in.mm) : transposed(Wm, in.mm);
+  const long long p = n < 10 * k ? n : 10 * k;
+  double* G = spush(C, n * p);
+  double* Y = spush(C, m * p);
+  double* Z = spush(C, n * p);
+  double* Qm = spush(C, m * p);
+  double* tau = spush(C, p);
+  if (failed(C)) return R;
+  const unsigned long long key = (unsigned long long)(unsigned)C.P.seed;
+  const unsigned long long stream = 16ULL + (unsigned long long)C.rsvd_calls;
+  C.rsvd_calls += 1;   // every thread keeps the same count
+  for (long long e = T.rank(); e < n * p; e += T.size()) G[e] = disorder_normal(key, stream, (unsigned long long)e);
+  T.sync();
+  gemm(T, m, p, n, M, colmajor(G, n), colmajor(Y, m));
+  for (int it = 0; it < 10; ++it) {
+    gemm(T, n, p, m, Mt, colmajor(Y, m), colmajor(Z, n));   // Z = M^T Y
+    gemm(T, m, p, n, M, colmajor(Z, n), colmajor(Y, m));    // Y = M Z
+    if (!thin_q(C, Y, m, p, tau, Qm)) return R;
+    copy(T, Y, Qm, m * p);
+  }
+  if (!thin_q(C, Y, m, p, tau, Qm)) return R;              // Q (m x p)
+  SvdIn bin = svd_begin(C, p, n, 0.0);
+  if (failed(C)) return R;
+  gemm(T, p, n, m, transposed(Qm, m), M, svd_target(bin));  // B = Q^T M
+  Svd F = svd_finish(C, bin);
+  if (failed(C) || !F.U) return R;
+  const long long kk = F.p < k ? F.p : k;
+  double* U = spush(C, m * kk);
+  if (failed(C)) return R;
+  gemm(T, m, kk, p, colmajor(Qm, m), colmajor(F.U, p), colmajor(U, m));
+  R.p = kk;
+  R.U = U;
+  R.S = F.S;
+  R.V = F.V;
+  return R;
+}
+
 // swap! (mps_node.jl:126-178)
 // ---------------------------------------------------------------------------
 CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
@@ -767,7 +840,11 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   SiteRef tl = sref(C, k, lo), tr = sref(C, k, hi);
   const long long d0 = tl.dl, d1 = tr.d, d2 = tl.d, d3 = tr.dr, kk = tl.dr;
   const long long m = d0 * d1, n = d2 * d3;
-  const bool rsvd_route = C.P.swapopt && ((m > 7000 && n > 7000) || m > 20000 || n > 20000);
+  const long long rmin = C.rsvd_min > 0 ? C.rsvd_min : 7000, rbig = C.rsvd_min > 0 ? 3LL * C.rsvd_min : 20000;
+  const bool rsvd_route = C.P.swapopt && ((m > rmin && n > rmin) || m > rbig || n > rbig);
+  // the reference's randomized algorithm on request (forward runs, sketch no
+  // wider than M); otherwise the exact top-chi subspace it approximates
+  const bool randomized = rsvd_route && C.P.rsvd == 1 && !C.tape && m >= (n < 10LL * C.P.chi ? n : 10LL * C.P.chi);
   SvdIn in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);
   if (failed(C)) return 0.0;
   // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
@@ -779,15 +856,16 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
     gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
     prof_add(C, PROF_SWAP_GEMM, (double)(clk() - tg));
   }
-  Svd R = svd_finish(C, in);
+  Svd R = randomized ? rsvd_swap(C, in, m, n, C.P.chi) : svd_finish(C, in);
   if (failed(C)) return 0.0;
   const long long te = clk();
   double err = 0.0;
   int myd;
   if (rsvd_route) {
     // The reference's randomized route keeps min(chi, rank) vectors with no
-    // cutoff and reports zero error (mps_node.jl:154-156); the exact top-chi
-    // subspace it approximates is used here.
+    // cutoff and reports zero error (mps_node.jl:154-156): its randomized
+    // algorithm with P.rsvd = 1 (rsvd_swap), else the exact top-chi subspace
+    // it approximates.
     myd = (int)(R.p < C.P.chi ? R.p : C.P.chi);
   } else {
     myd = keep_rule(C, R, C.P.cutoff, C.P.chi, &err);
@@ -1932,6 +2010,8 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.sws = sws;
   C.sws_doubles = sws_doubles;
   C.status = 0;
+  C.rsvd_min = 0;
+  C.rsvd_calls = 0;
   C.multigraph = 1;
   C.trace = nullptr;
   C.trace_cap = 0;
@@ -2047,6 +2127,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
                                   const JobLink* jl = nullptr) {
   Ctx C = make_ctx(T, slot, L, D.P, D.n, sws, sws_doubles);
   C.multigraph = D.multigraph;
+  C.rsvd_min = D.rsvd_min;
   if (jl) {
     C.job = jl->job;
     C.qhead = jl->qhead;

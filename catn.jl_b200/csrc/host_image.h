@@ -3,6 +3,7 @@
 // the Ising / spin-glass builder of the reference (src/ising.jl:20-227).
 #pragma once
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <set>
 #include <string>
@@ -422,6 +423,9 @@ struct Image {
 
  private:
   void finish(InstDesc& D, int n, int edges, int trace_cap) {
+    // CATN_RSVD_MIN_DIM lowers the randomized-SVD route's size threshold so
+    // that tests reach it with small networks (0 / unset: the reference's)
+    if (const char* e = std::getenv("CATN_RSVD_MIN_DIM")) D.rsvd_min = std::atoi(e);
     D.trace_cap = trace_cap;
     D.cost = edges;
     D.trace_off = trace_total;

@@ -51,8 +51,16 @@ typedef struct {
   int32_t swapopt;
   int32_t compress;
   int32_t cut_bond;
-  int32_t seed;        /* kept for API parity; the reference never reads it */
+  int32_t seed;        /* key of the rsvd sketch generator (rsvd = 1)       */
   int32_t trace;       /* record the per-step integer trace                 */
+  int32_t rsvd;        /* swap! matrices on the reference's randomized-SVD
+                        * route (swapopt, both sides > 7000 or one > 20000,
+                        * mps_node.jl:154-156): 0 = the exact top-chi
+                        * subspace; 1 = the reference's randomized algorithm
+                        * (linalg_utils.jl:44-58: sketch of min(n, 10 chi)
+                        * columns, 10 power iterations), its Gaussian sketch
+                        * drawn from the counter-based generator keyed by
+                        * seed (forward runs; gradient runs use 0)          */
 } catn_params;
 
 /* Default values of the reference's keyword arguments. */

@@ -49,21 +49,49 @@ def thin_qr(A):
     return Q, R
 
 
-def rsvd(A, k, oversample=10, power=10, rng=None):
+def _splitmix64(x):
+    """SplitMix64 mixing function (Steele, Lea and Flood, 2014) on uint64
+    arrays (wrapping arithmetic)."""
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def counter_normal(seed, stream, index):
+    """Standard normals from (seed, stream, index): SplitMix64 on a Weyl
+    sequence of the counter and the Box-Muller transform of two 53-bit
+    uniforms -- the generator the engine draws its rsvd sketch and device
+    disorder from (csrc/ising_build.cuh, disorder_normal)."""
+    index = np.asarray(index, dtype=np.uint64)
+    key = _splitmix64(np.array([seed], dtype=np.uint64) ^ (np.array([stream], dtype=np.uint64)
+                                                           * np.uint64(0xD1B54A32D192ED03)))[0]
+    a = _splitmix64(key + np.uint64(2) * index)
+    b = _splitmix64(key + np.uint64(2) * index + np.uint64(1))
+    u1 = ((a >> np.uint64(11)) + np.uint64(1)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    u2 = (b >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    return np.sqrt(-2.0 * np.log(u1)) * np.cos(6.283185307179586 * u2)
+
+
+def rsvd(A, k, oversample=10, power=10, rng=None, sketch=None):
     """Randomized SVD (linalg_utils.jl:44-58).
 
     ``p = min(n, oversample*k)`` -- the oversampling is multiplicative in the
     reference; ``power`` rounds of ``Y <- thinQ(A (A^H Y))``.  The reference
     draws the sketch from Julia's global RNG (unseeded from ``contraction!``),
-    so this restatement can only match it in distribution, not bit for bit.
+    so this restatement can only match it in distribution, not bit for bit;
+    ``sketch`` (n x p) supplies the Gaussian matrix instead.
     """
     if rng is None:
         rng = np.random.default_rng(0)
     n = A.shape[1]
     p = min(n, oversample * k)
-    G = rng.standard_normal((n, p))
-    if np.iscomplexobj(A):
-        G = G + 1j * rng.standard_normal((n, p))
+    if sketch is not None:
+        G = sketch
+    else:
+        G = rng.standard_normal((n, p))
+        if np.iscomplexobj(A):
+            G = G + 1j * rng.standard_normal((n, p))
     Y = A @ G
     for _ in range(power):
         M = A @ (A.conj().T @ Y)

@@ -9,7 +9,24 @@ import math
 
 import numpy as np
 
-from .linalg import tsvd, rsvd, thin_qr
+from .linalg import tsvd, rsvd, thin_qr, counter_normal, _svd_full
+
+# Randomized-SVD route of swap! (test infrastructure).  RSVD_MIN overrides
+# the reference's size thresholds (7000 / 20000 become RSVD_MIN / 3 RSVD_MIN,
+# as the engine's CATN_RSVD_MIN_DIM does).  RSVD_SKETCH_SEED, when set,
+# draws the sketch from the engine's counter-based generator (that seed,
+# stream 16 + RSVD_CALLS), which pins the engine's rsvd = 1 mode; callers
+# reset RSVD_CALLS to 0 before each network.
+RSVD_MIN = None
+RSVD_SKETCH_SEED = None
+RSVD_CALLS = 0
+
+
+def svd_full_topk(M, k):
+    """The exact top-k singular triplets (all of them when fewer)."""
+    U, S, V = _svd_full(M)
+    kk = min(k, S.shape[0])
+    return U[:, :kk], S[:kk], V[:, :kk]
 
 # Optional step log: list of tuples (op, d0, d1, d2, d3, kept).
 STEP_LOG = None
@@ -161,8 +178,18 @@ def swap(node, i, j):
     W = np.einsum("ijk,kab->iajb", tl, tr)
     M = rs(W, d0 * d1, d2 * d3)
     rows, cols = M.shape
-    if node.swapopt and ((rows > 7000 and cols > 7000) or rows > 20000 or cols > 20000):
-        U, S, V = rsvd(M, node.chi, 10, 10)
+    rmin, rbig = (7000, 20000) if RSVD_MIN is None else (RSVD_MIN, 3 * RSVD_MIN)
+    if node.swapopt and ((rows > rmin and cols > rmin) or rows > rbig or cols > rbig):
+        p = min(cols, 10 * node.chi)
+        if RSVD_SKETCH_SEED is None:
+            U, S, V = rsvd(M, node.chi, 10, 10)
+        elif rows >= p:
+            global RSVD_CALLS
+            G = counter_normal(RSVD_SKETCH_SEED, 16 + RSVD_CALLS, np.arange(cols * p)).reshape(p, cols).T
+            RSVD_CALLS += 1
+            U, S, V = rsvd(M, node.chi, 10, 10, sketch=G)
+        else:   # the engine takes the exact top-chi subspace for a sketch wider than M
+            U, S, V = svd_full_topk(M, node.chi)
         err = 0.0
     else:
         U, S, V, err = tsvd(M, cutoff=node.cutoff, maxdim=node.chi, tag="swap")
