@@ -194,8 +194,8 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   return CATN_OK;
 }
 
-void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n, long long* min_qr) {
-  int h = pool ? kHelperCtas : 0;
+void helper_config(const DeviceRun& R, int pool, int* nhelp, int* min_n, long long* min_qr) {
+  int h = pool;
   if (const char* e = std::getenv("CATN_HELPER_CTAS")) h = std::atoi(e);
   if (!R.d_board || h < 0 || 4 * h > R.nslots || 4 * h > R.ninst) h = 0;
   if (R.d_board && R.ngrid > R.nslots) h = R.ngrid - R.nslots;
@@ -241,7 +241,7 @@ catn_status launch(DeviceRun& R, cudaStream_t st) {
   if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.ngrid, st));
   int nhelp = 0, min_n = 0;
   long long min_qr = 0;
-  helper_config(R, true, &nhelp, &min_n, &min_qr);
+  helper_config(R, kHelperCtas, &nhelp, &min_n, &min_qr);
   catn_persistent_kernel<<<R.ngrid, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
                                                                 R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
                                                                 R.d_queue, R.d_board, nhelp, min_n, min_qr);

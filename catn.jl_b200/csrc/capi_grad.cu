@@ -93,10 +93,7 @@ catn_status grad_launch(GradRun* g, cudaStream_t st) {
   if (g->R.d_board) CUDA_TRY(cudaMemsetAsync(g->R.d_board, 0, sizeof(JacobiJob) * g->R.ngrid, st));
   int nhelp = 0, min_n = 0;
   long long min_qr = 0;
-  // batch gradient runs keep no helper pool: measured 780 ms with 24 helper
-  // CTAs against 731 ms without on the 512-instance batch (the taped
-  // instances are long, so the CTAs are worth more as workers)
-  helper_config(g->R, false, &nhelp, &min_n, &min_qr);
+  helper_config(g->R, kGradHelperCtas, &nhelp, &min_n, &min_qr);
   catn_grad_kernel<<<g->R.ngrid, kThreads, kSmemBytes, st>>>(g->R.d_desc, g->R.d_order, g->R.ninst, g->R.d_i64,
                                                               g->R.d_i32, g->R.d_dat, g->R.d_slots, g->R.L,
                                                               g->R.d_res, g->d_gimg, g->R.d_queue, g->R.d_board,

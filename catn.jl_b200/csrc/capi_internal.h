@@ -77,7 +77,13 @@ catn_status upload(DeviceRun& R, cudaStream_t st);
 // Dedicated helper CTAs of a launch of R and the smallest column count whose
 // Jacobi sweeps are shared (capi.cu).  `pool`: keep the batch helper pool
 // (one network always gets every other resident CTA as a helper).
-void helper_config(const DeviceRun& R, bool pool, int* nhelp, int* min_n, long long* min_qr);
+// Dedicated helper CTAs of a launch (`pool`, or CATN_HELPER_CTAS) and the
+// sharing thresholds.
+void helper_config(const DeviceRun& R, int pool, int* nhelp, int* min_n, long long* min_qr);
+// Helper pool of batch gradient launches: 0 / 8 / 16 / 24 CTAs measured 592-598
+// / 547 / 578 / 610 ms on the 512-instance spin-glass batch (taped instances
+// are long, so most CTAs are worth more as workers).
+constexpr int kGradHelperCtas = 8;
 // Arena of a single network when the caller passes 0 (capi.cu).
 long long default_arena(long long a, const catn_params& p);
 // Frees a gradient run (capi_grad.cu).
