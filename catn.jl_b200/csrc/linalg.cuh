@@ -761,13 +761,55 @@ CATN_HDI inline bool jacobi_pair_l2(const Team& T, double* B, double* V, double*
   return true;
 }
 
+// Rows per lane of the register-resident reflector application (columns up
+// to kHouseRows warps long below the reflector's row).
+constexpr int kHouseRows = 32;
+
 // Reflector k (v = A[k+1:m, k] with an implicit 1 at k, factor tk) applied to
 // column j of C; with nrm, the squared norm of C[k+1:m, j] goes to nrm[j].
-// Warp-level, through L2.
+// Warp-level, through L2.  When the rows below k fit kHouseRows per lane,
+// the reflector and the column are loaded at once and kept in registers for
+// the dot product, the update and the norm: one L2 round trip instead of
+// one per row block and pass.
 CATN_HDI inline void house_col_l2(const Team& T, const double* A, long long m, long long lda, long long k, double tk,
                                   double* C, long long ldc, long long j, double* nrm) {
   const double* ak = A + k * lda;
   double* cj = C + j * ldc;
+  const long long ws = T.wsize();
+  if (m - (k + 1) <= ws * kHouseRows) {
+    double vr[kHouseRows], cr[kHouseRows];
+#pragma unroll
+    for (int e = 0; e < kHouseRows; ++e) {
+      const long long i = k + 1 + T.lane() + ws * e;
+      vr[e] = (i < m && tk != 0.0) ? ldcg(ak + i) : 0.0;
+      cr[e] = i < m ? ldcg(cj + i) : 0.0;
+    }
+    double w = 0.0;
+    if (tk != 0.0) {
+      const double ck = ldcg(cj + k);
+#pragma unroll
+      for (int e = 0; e < kHouseRows; ++e) w = fma(vr[e], cr[e], w);
+      w = (T.wsum(w) + ck) * tk;
+      T.wsync();
+      if (T.lane() == 0) stcg(cj + k, ck - w);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int e = 0; e < kHouseRows; ++e) {
+      const long long i = k + 1 + T.lane() + ws * e;
+      if (tk != 0.0) {
+        cr[e] = fma(-w, vr[e], cr[e]);
+        if (i < m) stcg(cj + i, cr[e]);
+      }
+      s = fma(cr[e], cr[e], s);
+    }
+    if (nrm) {
+      s = T.wsum(s);
+      if (T.lane() == 0) stcg(nrm + j, s);
+    }
+    T.wsync();
+    return;
+  }
   if (tk != 0.0) {
     double w = 0.0;
     for (long long i = k + 1 + T.lane(); i < m; i += T.wsize()) w = fma(ldcg(ak + i), ldcg(cj + i), w);
