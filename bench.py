@@ -19,8 +19,9 @@ Workload (one "step" = one persistent-kernel pass over one batch):
   grad   the other half of the metric: d lnZ / d w and d lnZ / d h (every
          <s_i s_j>, <s_k> of every instance) from one device gradient run
          of the whole batch, against the reference's pinning definition,
-         which needs 1 + 2n + 4|E| contractions per instance (priced at the
-         measured forward rate, and timed directly on one sample instance)
+         which needs 1 + 2n + 4|E| contractions per instance: the pinned
+         networks of the first instances are contracted in one launch and
+         timed, and their measured rate prices the batch's pinned set
 
   plain_gpu_form  the same instances through the plain GPU form
          (baseline/plain_gpu_form.py: PyTorch FP64, one library call per
@@ -202,38 +203,56 @@ def load_peaks():
 
 
 # ----------------------------------------------------------------------------
+def lpt_order(instances):
+    """Largest instances first (by edge count), as the device work queue
+    takes them, so that a pass over the batch on the host cores does not end
+    on one large instance started last."""
+    return sorted(range(len(instances)), key=lambda q: -len(instances[q]["edges"]))
+
+
+def config_of(args, world):
+    """The workload description shared by both arms (same keys, same values)."""
+    return {"workload": WORKLOAD, "instances_per_gpu": args.instances, "seed": args.seed,
+            "Dmax": PARAMS["Dmax"], "chi": PARAMS["chi"],
+            "parallelism": f"replicas x{world} (independent instances)",
+            "l2": "flushed between timed steps by a 256 MiB device write (the host-core reference arm has "
+                  "no device L2)"}
+
+
 def run_reference(args):
     """--impl reference: the oracle port (CPU restatement of the reference
-    algorithm; Julia is unavailable) on the host cores, rank 0 only."""
+    algorithm; Julia is unavailable) on all host cores, rank 0 only.  One
+    step contracts the whole batch: every instance once, one single-threaded
+    process per core pulling instances in LPT order (imap, no per-chunk
+    barrier), like the device arm's work queue."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     cores = host_cores()
     insts = make_instances(args.instances, args.seed)
+    order = [insts[q] for q in lpt_order(insts)]
     pool = _cpu_pool(cores)
-    per_step = max(cores, 8)
-    rates = []
-    pos = 0
+    times = []
     for s in range(args.warmup + args.steps):
-        chunk = [insts[(pos + q) % len(insts)] for q in range(per_step)]
-        pos += per_step
         t0 = time.perf_counter()
-        pool.map(_oracle_one, chunk, chunksize=1)
+        for _ in pool.imap_unordered(_oracle_one, order, chunksize=1):
+            pass
         dt = time.perf_counter() - t0
         if s >= args.warmup:
-            rates.append((per_step, dt))
+            times.append(dt)
     pool.terminate()
-    n = sum(r[0] for r in rates)
-    t = sum(r[1] for r in rates)
-    v = n / t
+    t = sum(times)
+    v = args.instances * args.steps / t
     out = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "instances/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(1000 * t / args.steps, 3), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "instances_per_step": per_step, "l2": "n/a (CPU)"},
+           "config": config_of(args, world),
            "cpu_baseline": {"value": round(v, 3), "unit": "instances/s", "cores": cores, "kind": "port",
-                            "sample": f"{per_step} instances per step (instances in workload order, "
-                                      f"one single-threaded process per core)"},
+                            "sample": f"the whole {args.instances}-instance batch per step, oracle port "
+                                      f"(numpy/OpenBLAS FP64), {cores} single-threaded processes pulling "
+                                      f"instances largest first"},
            "e2e": {"value": round(v, 3), "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -265,12 +284,15 @@ def main():
 
     # CPU baseline first (spawned pool, before any CUDA call), rank 0 at N=1 only
     cpu = None
+    cpu_lz = {}
     if rank == 0 and world == 1 and not args.no_cpu:
         cores = host_cores()
         sample = make_instances(args.instances, args.seed)
-        rate, cnt, _ = cpu_sample_rate(sample, args.cpu_seconds, cores)
+        order = lpt_order(sample)
+        rate, cnt, lz = cpu_sample_rate([sample[q] for q in order], args.cpu_seconds, cores)
+        cpu_lz = {order[k]: v for k, v in enumerate(lz)}
         cpu = {"value": round(rate, 3), "unit": "instances/s", "cores": cores, "kind": "port",
-               "sample": f"first {cnt} of the {args.instances} workload instances in order, "
+               "sample": f"{cnt} of the {args.instances} workload instances, largest first, "
                          f"oracle port (numpy/OpenBLAS FP64), {cores} single-threaded processes, "
                          f"~{args.cpu_seconds:.0f} s"}
 
@@ -372,6 +394,16 @@ def main():
             dist.destroy_process_group()
         return
     peak, peak_kind = load_peaks()
+    # error against the FP64 oracle on the instances the CPU leg contracted
+    accuracy = {"vs": "FP64 oracle (numpy/OpenBLAS restatement of the reference algorithm)",
+                "instances_compared": len(cpu_lz)}
+    if cpu_lz:
+        d_or = [abs(res_ref[q].lnZ - v) / insts[q]["n"] for q, v in cpu_lz.items()]
+        accuracy["max_abs_dlnZ_per_spin"] = float(max(d_or))
+        accuracy["median_abs_dlnZ_per_spin"] = float(statistics.median(d_or))
+        accuracy["bar"] = 1e-6
+        accuracy["within_bar"] = bool(max(d_or) <= 1e-6)
+    fp64_peak = measure_dgemm_tflops()
     avg = total / args.steps
     achieved_gbs = nbytes / avg / 1e9
     traffic = read_traffic()
@@ -379,10 +411,10 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": "instances/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * avg, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "instances_per_gpu": args.instances, "seed": args.seed,
-                   "Dmax": 32, "chi": 128, "parallelism": f"replicas x{world} (independent instances)",
-                   "l2": "flushed (256 MiB write) between timed steps", "slots": batch.slots,
-                   "contraction_steps_total": int(sum(steps_per_inst))},
+        "config": config_of(args, world),
+        "engine": {"slots": batch.slots, "contraction_steps_total": int(sum(steps_per_inst)),
+                   "statuses_nonzero": int(sum(1 for r in res_ref if r.status != 0))},
+        "accuracy": accuracy,
         "e2e": {"value": round(e2e_value, 3), "unit": "instances/s",
                 "h2d_bytes_per_step": int(batch.param_bytes),
                 "d2h_bytes_per_step": int(args.instances * ctypes.sizeof(catn_lib.Result)),
@@ -398,7 +430,11 @@ def main():
                      "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)",
                      "algorithmic_bytes_per_launch": nbytes,
                      "algorithmic_fp64_flops_per_launch": flops,
-                     "achieved_fp64_tflops": round(flops / avg / 1e12, 4)},
+                     "achieved_fp64_tflops": round(flops / avg / 1e12, 4),
+                     "fp64": {"achieved": round(flops / avg / 1e12, 4), "peak": fp64_peak, "unit": "TFLOP/s",
+                              "frac": round(flops / avg / 1e12 / fp64_peak, 5) if fp64_peak else None,
+                              "peak_source": "cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5, "
+                                             "measured in this run on this GPU"}},
         "clocks": clk.summary(),
     }
     if cpu:
@@ -419,54 +455,117 @@ def main():
         dist.destroy_process_group()
 
 
-def grad_leg(catn, batch, insts, forward_rate, stream, sh):
-    """Adjoint of the whole batch (one launch) against pinning."""
+def _pin_sets(d):
+    """The reference's pinned networks of one instance: the unpinned one,
+    both values of every spin (ising.jl:263-290) and the four value pairs of
+    every edge (ising.jl:309-339)."""
+    pins = [(0, 0, 0, 0)] + [(k, v, 0, 0) for k in range(1, d["n"] + 1) for v in (1, 2)]
+    for (m, nn) in d["edges"]:
+        for v1 in (1, 2):
+            for v2 in (1, 2):
+                pins.append((int(m), v1, int(nn), v2))
+    return pins
+
+
+def grad_leg(catn, batch, insts, forward_rate, stream, sh, sample=4):
+    """Adjoint of the whole batch (one launch) against pinning, both measured."""
     import torch
     batch.grad_launch(sh)   # first call allocates the gradient slots
     batch.grad_fetch(sh)
     times = []
-    for _ in range(2):
+    for _ in range(3):
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
         batch.grad_launch(sh)
+        res, dw, dh = batch.grad_fetch(sh)
         b.record(stream)
         torch.cuda.synchronize()
         times.append(a.elapsed_time(b) / 1000.0)
-    res, dw, dh = batch.grad_fetch(sh)
     t_grad = sum(times) / len(times)
     pin = [1 + 2 * d["n"] + 4 * len(d["edges"]) for d in insts]
-    t_pin = sum(pin) / forward_rate
-    # one instance timed both ways: its pinned set in one batch launch, and
-    # its gradient run alone; observables compared
-    d = min(insts, key=lambda x: x["n"])
+    # measured pinning: every pinned network of the first `sample` instances
+    # in ONE batch launch (upload, launch and read-back inside CUDA events)
     kw = dict(PARAMS)
-    t0 = time.perf_counter()
-    m_pin = catn.magnetization(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
-    c_pin = catn.correlation(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
-    t_pin1 = time.perf_counter() - t0
-    tn = catn.ising_network(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **kw)
-    catn.gradient(tn)   # allocation of its gradient slot
-    t0 = time.perf_counter()
-    _, gw, gh = catn.gradient(tn)
-    t_adj1 = time.perf_counter() - t0
-    dev = max(float(np.max(np.abs(gh / d["beta"] - m_pin))), float(np.max(np.abs(gw / d["beta"] - c_pin))))
+    pinned, owner = [], []
+    for q in range(sample):
+        d = insts[q]
+        for p in _pin_sets(d):
+            pinned.append(dict(n=d["n"], edges=d["edges"], weights=d["weights"], fields=d["fields"], beta=d["beta"],
+                               pos1=p[0], val1=p[1], pos2=p[2], val2=p[3]))
+            owner.append(q)
+    pb = catn.IsingBatch(pinned, **kw)
+    pb.upload(sh)
+    pb.launch(sh)
+    pb.fetch(sh)
+    torch.cuda.synchronize()
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    pb.upload(sh)
+    pb.launch(sh)
+    pres = pb.fetch(sh)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_pin_sample = a.elapsed_time(b) / 1000.0
+    lz = np.array([r.lnZ for r in pres])
+    pin_rate = len(pinned) / t_pin_sample
+    # observables of the sample from pinning vs from the batch's adjoint run
+    arr = batch._arrays
+    dev, pos = 0.0, 0
+    for q in range(sample):
+        d = insts[q]
+        n, ne = d["n"], len(d["edges"])
+        z0 = lz[pos]
+        pm = np.exp(lz[pos + 1:pos + 1 + 2 * n] - z0).reshape(n, 2)
+        pc = np.exp(lz[pos + 1 + 2 * n:pos + 1 + 2 * n + 4 * ne] - z0).reshape(ne, 2, 2)
+        pos += 1 + 2 * n + 4 * ne
+        m_pin = pm[:, 1] - pm[:, 0]
+        c_pin = pc[:, 0, 0] - pc[:, 0, 1] - pc[:, 1, 0] + pc[:, 1, 1]
+        gh = dh[arr[1][q]:arr[1][q + 1]] / d["beta"]
+        gw = dw[arr[2][q]:arr[2][q + 1]] / d["beta"]
+        dev = max(dev, float(np.max(np.abs(gh - m_pin))), float(np.max(np.abs(gw - c_pin))))
+    t_pin_batch = sum(pin) / pin_rate
     return {
         "what": "d lnZ/d w_e = beta <s_i s_j> for every edge and d lnZ/d h_k = beta <s_k> for every spin of "
-                "every instance, one device gradient run (taped forward + backward) of the whole batch",
+                "every instance, one device gradient run (taped forward + backward) of the whole batch, against "
+                "the reference's pinning definition (1 + 2n + 4|E| contractions per instance)",
         "adjoint_ms_per_batch": round(1000 * t_grad, 3),
         "adjoint_instances_per_s": round(len(insts) / t_grad, 3),
         "pinning_contractions_per_batch": int(sum(pin)),
-        "pinning_ms_per_batch_at_forward_rate": round(1000 * t_pin, 3),
-        "speedup_vs_pinning": round(t_pin / t_grad, 1),
-        "sample_instance": {"n": d["n"], "edges": len(d["edges"]), "pinned_contractions": pin[insts.index(d)],
-                            "pinning_s_wall": round(t_pin1, 4), "adjoint_s_wall": round(t_adj1, 4),
-                            "speedup_wall": round(t_pin1 / t_adj1, 1),
-                            "max_abs_observable_diff_vs_pinning": dev},
-        "timing": "CUDA events around catn_batch_grad_launch (input upload + one launch), mean of 2; "
-                  "sample instance: host wall clock around the public calls",
+        "pinning_measured": {"instances": sample, "contractions": len(pinned),
+                             "ms": round(1000 * t_pin_sample, 3),
+                             "contractions_per_s": round(pin_rate, 3),
+                             "max_abs_observable_diff_vs_adjoint": dev},
+        "pinning_ms_per_batch_at_measured_rate": round(1000 * t_pin_batch, 3),
+        "speedup_vs_pinning": round(t_pin_batch / t_grad, 1),
+        "timing": "CUDA events: adjoint = catn_batch_grad_launch (input upload + one launch) + read-back of "
+                  "results and gradients, mean of 3; pinning = upload + one launch + read-back of every pinned "
+                  "network of the first instances of the batch, whose measured rate prices the batch's pinned set",
     }
+
+
+def measure_dgemm_tflops():
+    """FP64 denominator: cuBLAS DGEMM 8192^3 on this GPU, best of 5 (CUDA
+    events).  The measured-peaks file holds no FP64 figure."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    best = None
+    for _ in range(6):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1000.0
+        best = t if best is None else min(best, t)
+    del a, b
+    torch.cuda.empty_cache()
+    return round(2.0 * n ** 3 / best / 1e12, 3)
 
 
 def ct_stream(stream):

@@ -28,7 +28,15 @@ class Params(ct.Structure):
     _fields_ = [("Dmax", ct.c_int32), ("chi", ct.c_int32), ("cutoff", ct.c_double),
                 ("norm_method", ct.c_int32), ("select", ct.c_int32), ("reverse", ct.c_int32),
                 ("svdopt", ct.c_int32), ("swapopt", ct.c_int32), ("compress", ct.c_int32),
-                ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32), ("rsvd", ct.c_int32)]
+                ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32), ("rsvd", ct.c_int32),
+                ("rsvd_min_dim", ct.c_int32), ("precision", ct.c_int32), ("svd_route", ct.c_int32)]
+
+
+class Tuning(ct.Structure):
+    """``catn_tuning``: the process-wide launch-shape and route table."""
+    _fields_ = [("helper_ctas", ct.c_int32), ("grad_helper_ctas", ct.c_int32),
+                ("shared_jacobi_min_n", ct.c_int32), ("block_min_n", ct.c_int32),
+                ("shared_house_min", ct.c_int64)]
 
 
 class Result(ct.Structure):
@@ -75,6 +83,9 @@ SIGNATURES = {
     "catn_ising_contract_static": ([ct.POINTER(Params), ct.c_int32, ct.c_int32, _P, _P, _P, ct.c_double,
                                     ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_void_p,
                                     ct.POINTER(Result)], ct.c_int),
+    "catn_tc_matmul": ([ct.c_int32, ct.c_int32, ct.c_int32, _P, _P, _P], ct.c_int),
+    "catn_tuning_get": ([ct.POINTER(Tuning)], ct.c_int),
+    "catn_tuning_set": ([ct.POINTER(Tuning)], ct.c_int),
     "catn_last_error": ([ct.c_char_p, ct.c_size_t], ct.c_size_t),
     "catn_version": ([], ct.c_char_p),
 }
@@ -115,8 +126,18 @@ def ptr(a):
     return a.ctypes.data_as(ct.c_void_p) if a is not None else None
 
 
+PRECISIONS = {"fp64": 0, "split": 1}
+SVD_ROUTES = {"auto": 0, "scalar": 1, "block": 2}
+
+
 def make_params(Dmax=32, chi=32, cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True,
-                swapopt=True, compress=False, cut_bond=False, seed=1, trace=False, rsvd=0):
+                swapopt=True, compress=False, cut_bond=False, seed=1, trace=False, rsvd=0, rsvd_min_dim=0,
+                precision="fp64", svd_route="auto"):
+    """``catn_params`` from the reference's keywords plus the engine's own:
+    ``rsvd`` / ``rsvd_min_dim`` (randomized swap route), ``precision``
+    ("fp64" or "split") and ``svd_route`` ("auto", "scalar", "block")."""
+    prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    route = SVD_ROUTES[svd_route] if isinstance(svd_route, str) else int(svd_route)
     return Params(int(Dmax), int(chi), float(cutoff), int(norm_method), int(select), int(bool(reverse)),
                   int(bool(svdopt)), int(bool(swapopt)), int(bool(compress)), int(bool(cut_bond)),
-                  int(seed), int(bool(trace)), int(rsvd))
+                  int(seed), int(bool(trace)), int(rsvd), int(rsvd_min_dim), prec, route)

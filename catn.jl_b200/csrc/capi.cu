@@ -54,6 +54,9 @@ catn_status check_params(const catn_params* p) {
   if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
   if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
   if (p->rsvd < 0 || p->rsvd > 1) return fail(CATN_EINVAL, "rsvd must be 0 or 1");
+  if (p->rsvd_min_dim < 0) return fail(CATN_EINVAL, "rsvd_min_dim must be >= 0");
+  if (p->precision < 0 || p->precision > 1) return fail(CATN_EINVAL, "precision must be 0 (FP64) or 1 (split)");
+  if (p->svd_route < 0 || p->svd_route > 2) return fail(CATN_EINVAL, "svd_route must be 0, 1 or 2");
   return CATN_OK;
 }
 
@@ -71,39 +74,36 @@ namespace {
 // / 316 / 324; pool 16 at threshold 64 / 96: 312 / 312.  The pool's size
 // trades the slowest instance (320 ms at 8, 290 ms at 24) against the work
 // left to the other CTAs.
-// CATN_HELPER_CTAS and CATN_SHARED_JACOBI_MIN_N override the two, and
-// CATN_SHARED_HOUSE_MIN the element threshold for Householder work.
+// The process-wide tuning table (catn_tuning_set) overrides both, and the
+// element threshold for Householder work.
 constexpr int kSharedJacobiMinN = 128;
 constexpr int kHelperCtas = 16;
 
 // `order` lists instance ids by descending work estimate, so the longest
 // contractions start first (longest-processing-time scheduling).  With a job
 // board, the last `nhelp` CTAs and every CTA that finds the queue drained
-// lend their warps to the large SVDs of the CTAs still contracting
-// (help_jacobi) until all are finished.
+// help the large SVDs of the CTAs still contracting (help_jobs) until all are
+// finished.  With split-precision instances every CTA holds TMEM columns and
+// the tensor-core staging area for the block route's products.
 __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue,
-    JacobiJob* board, int nhelp, int share_min_n, long long share_min_qr) {
+    JacobiJob* board, int nhelp, JobLink jl, int use_tc) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  T.tcs = nullptr;
+  T.tmem = 0;
+  if (use_tc) tc_setup(T, tc_region(smem));
   double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
-  JobLink jl;
   jl.job = board ? board + blockIdx.x : nullptr;
   jl.qhead = queue;
-  jl.ninst = ninst;
-  jl.min_n = share_min_n;
-  jl.pool = nhelp > 0;
-  jl.min_qr = share_min_qr;
-  if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
-    help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
-    return;
-  }
+  const bool helper = board && (int)blockIdx.x >= (int)gridDim.x - nhelp;
   for (;;) {
+    if (helper) break;
     long long inst = 0;
     if (threadIdx.x == 0) {
       const int q = atomicAdd(queue, 1);
@@ -114,8 +114,13 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles,
                  board ? &jl : nullptr);
     if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
+    // A shared wait that ran out leaves a helper warp that may still write
+    // into this slot's arena: the slot takes no further instance (the other
+    // CTAs drain the queue).
+    if (T.bcast(threadIdx.x == 0 ? res[inst].status : 0) == CATN_ETIMEOUT) break;
   }
-  if (board) help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
+  if (board) help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+  tc_teardown(T);
 }
 
 __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
@@ -125,6 +130,8 @@ __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  T.tcs = nullptr;
+  T.tmem = 0;
   Ctx C = make_ctx(T, slot, L, P, n, (double*)(T.stage + GEMM_STAGE_BYTES), kSwsDoubles);
   int nd = 0;
   long long dims[64];
@@ -144,11 +151,14 @@ namespace catn_capi {
 catn_status prepare(const Image& im, long long arena_bytes, int max_slots, DeviceRun& R) {
   R.ninst = (int)im.desc.size();
   if (R.ninst == 0) return fail(CATN_EINVAL, "no instances");
+  R.use_tc = 0;
+  for (const InstDesc& d : im.desc)
+    if (d.P.precision == 1) R.use_tc = 1;
   R.L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
   int dev = 0, nsm = 0, per_sm = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CUDA_TRY(cudaFuncSetAttribute(catn_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  CUDA_TRY(cudaFuncSetAttribute(catn_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesTc));
   CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, catn_persistent_kernel, kThreads, kSmemBytes));
   if (per_sm < 1) per_sm = 1;
   long long resident = (long long)nsm * per_sm;
@@ -194,18 +204,34 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   return CATN_OK;
 }
 
-void helper_config(const DeviceRun& R, int pool, int* nhelp, int* min_n, long long* min_qr) {
-  int h = pool;
-  if (const char* e = std::getenv("CATN_HELPER_CTAS")) h = std::atoi(e);
+// The tuning table in force (entries < 0: built-in defaults).
+std::mutex g_tuning_mu;
+catn_tuning g_tuning = {-1, -1, -1, -1, -1};
+
+catn_tuning tuning_now() {
+  std::lock_guard<std::mutex> lock(g_tuning_mu);
+  catn_tuning t = g_tuning;
+  if (t.helper_ctas < 0) t.helper_ctas = kHelperCtas;
+  if (t.grad_helper_ctas < 0) t.grad_helper_ctas = kGradHelperCtas;
+  if (t.shared_jacobi_min_n < 0) t.shared_jacobi_min_n = kSharedJacobiMinN;
+  if (t.block_min_n < 0) t.block_min_n = (int32_t)catn::kBlockMinN;
+  if (t.shared_house_min < 0) t.shared_house_min = kSharedHouseMinElems;
+  return t;
+}
+
+void helper_config(const DeviceRun& R, bool grad, JobLink* jl, int* nhelp) {
+  const catn_tuning t = tuning_now();
+  int h = grad ? t.grad_helper_ctas : t.helper_ctas;
   if (!R.d_board || h < 0 || 4 * h > R.nslots || 4 * h > R.ninst) h = 0;
   if (R.d_board && R.ngrid > R.nslots) h = R.ngrid - R.nslots;
-  int m = kSharedJacobiMinN;
-  if (const char* e = std::getenv("CATN_SHARED_JACOBI_MIN_N")) m = std::max(2, std::atoi(e));
-  long long q = kSharedHouseMinElems;
-  if (const char* e = std::getenv("CATN_SHARED_HOUSE_MIN")) q = std::max(1LL, std::atoll(e));
   *nhelp = h;
-  *min_n = m;
-  *min_qr = q;
+  jl->job = nullptr;
+  jl->qhead = nullptr;
+  jl->ninst = R.ninst;
+  jl->min_n = std::max(2, (int)t.shared_jacobi_min_n);
+  jl->pool = h > 0;
+  jl->min_qr = std::max(1LL, (long long)t.shared_house_min);
+  jl->block_min_n = std::max(4, (int)t.block_min_n);
 }
 
 catn_status upload(DeviceRun& R, cudaStream_t st) {
@@ -239,12 +265,12 @@ namespace {
 catn_status launch(DeviceRun& R, cudaStream_t st) {
   CUDA_TRY(cudaMemsetAsync(R.d_queue, 0, 4 * sizeof(int), st));
   if (R.d_board) CUDA_TRY(cudaMemsetAsync(R.d_board, 0, sizeof(JacobiJob) * R.ngrid, st));
-  int nhelp = 0, min_n = 0;
-  long long min_qr = 0;
-  helper_config(R, kHelperCtas, &nhelp, &min_n, &min_qr);
-  catn_persistent_kernel<<<R.ngrid, kThreads, kSmemBytes, st>>>(R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32,
-                                                                R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace,
-                                                                R.d_queue, R.d_board, nhelp, min_n, min_qr);
+  int nhelp = 0;
+  JobLink jl;
+  helper_config(R, false, &jl, &nhelp);
+  catn_persistent_kernel<<<R.ngrid, kThreads, R.use_tc ? kSmemBytesTc : kSmemBytes, st>>>(
+      R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32, R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace, R.d_queue,
+      R.d_board, nhelp, jl, R.use_tc);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }
@@ -339,6 +365,24 @@ void catn_params_default(catn_params* p) {
   p->seed = 1;
   p->trace = 0;
   p->rsvd = 0;
+  p->rsvd_min_dim = 0;
+  p->precision = 0;
+  p->svd_route = 0;
+}
+
+catn_status catn_tuning_get(catn_tuning* t) {
+  if (!t) return fail(CATN_EINVAL, "NULL argument");
+  *t = tuning_now();
+  return CATN_OK;
+}
+
+catn_status catn_tuning_set(const catn_tuning* t) {
+  if (!t) return fail(CATN_EINVAL, "NULL argument");
+  if (t->helper_ctas > 4096 || t->grad_helper_ctas > 4096) return fail(CATN_EINVAL, "helper pool above 4096 CTAs");
+  if (t->block_min_n >= 0 && t->block_min_n < 4) return fail(CATN_EINVAL, "block_min_n must be >= 4 (or < 0)");
+  std::lock_guard<std::mutex> lock(g_tuning_mu);
+  g_tuning = *t;
+  return CATN_OK;
 }
 
 static catn_status net_finish(catn_net* net, long long arena_bytes, catn_net** out) {

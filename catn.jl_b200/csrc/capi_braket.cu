@@ -20,6 +20,8 @@ __global__ void __launch_bounds__(kThreads) catn_braket_kernel(
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  T.tcs = nullptr;
+  T.tmem = 0;
   double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
   for (;;) {

@@ -25,26 +25,22 @@ namespace {
 __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, double* gimg, int* queue,
-    JacobiJob* board, int nhelp, int share_min_n, long long share_min_qr) {
+    JacobiJob* board, int nhelp, JobLink jl, int use_tc) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  T.tcs = nullptr;
+  T.tmem = 0;
+  if (use_tc) tc_setup(T, tc_region(smem));
   double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
-  JobLink jl;
   jl.job = board ? board + blockIdx.x : nullptr;
   jl.qhead = queue;
-  jl.ninst = ninst;
-  jl.min_n = share_min_n;
-  jl.pool = nhelp > 0;
-  jl.min_qr = share_min_qr;
-  if (board && (int)blockIdx.x >= (int)gridDim.x - nhelp) {
-    help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
-    return;
-  }
+  const bool helper = board && (int)blockIdx.x >= (int)gridDim.x - nhelp;
   for (;;) {
+    if (helper) break;
     long long inst = 0;
     if (threadIdx.x == 0) {
       const int q = atomicAdd(queue, 1);
@@ -55,8 +51,13 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     run_instance_grad(T, slot, L, descs[inst], i64, i32, dat, res + inst, gimg, sws, kSwsDoubles,
                       board ? &jl : nullptr);
     if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
+    // A shared wait that ran out leaves a helper warp that may still write
+    // into this slot's arena: the slot takes no further instance (the other
+    // CTAs drain the queue).
+    if (T.bcast(threadIdx.x == 0 ? res[inst].status : 0) == CATN_ETIMEOUT) break;
   }
-  if (board) help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
+  if (board) help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+  tc_teardown(T);
 }
 
 // A gradient run holds the scratch stack, the tape, the append-only heap and
@@ -83,7 +84,7 @@ catn_status grad_prepare(const Image& im, long long arena, int max_slots, GradRu
   const size_t gbytes = sizeof(double) * (im.dat.size() + 1);
   CUDA_TRY(cudaMalloc(&g->d_gimg, gbytes));
   CUDA_TRY(cudaMallocHost(&g->h_gimg, gbytes));
-  CUDA_TRY(cudaFuncSetAttribute(catn_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  CUDA_TRY(cudaFuncSetAttribute(catn_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesTc));
   return CATN_OK;
 }
 
@@ -91,13 +92,12 @@ catn_status grad_launch(GradRun* g, cudaStream_t st) {
   if (catn_status s = upload(g->R, st)) return s;
   CUDA_TRY(cudaMemsetAsync(g->R.d_queue, 0, 4 * sizeof(int), st));
   if (g->R.d_board) CUDA_TRY(cudaMemsetAsync(g->R.d_board, 0, sizeof(JacobiJob) * g->R.ngrid, st));
-  int nhelp = 0, min_n = 0;
-  long long min_qr = 0;
-  helper_config(g->R, kGradHelperCtas, &nhelp, &min_n, &min_qr);
-  catn_grad_kernel<<<g->R.ngrid, kThreads, kSmemBytes, st>>>(g->R.d_desc, g->R.d_order, g->R.ninst, g->R.d_i64,
-                                                              g->R.d_i32, g->R.d_dat, g->R.d_slots, g->R.L,
-                                                              g->R.d_res, g->d_gimg, g->R.d_queue, g->R.d_board,
-                                                              nhelp, min_n, min_qr);
+  int nhelp = 0;
+  JobLink jl;
+  helper_config(g->R, true, &jl, &nhelp);
+  catn_grad_kernel<<<g->R.ngrid, kThreads, g->R.use_tc ? kSmemBytesTc : kSmemBytes, st>>>(
+      g->R.d_desc, g->R.d_order, g->R.ninst, g->R.d_i64, g->R.d_i32, g->R.d_dat, g->R.d_slots, g->R.L, g->R.d_res,
+      g->d_gimg, g->R.d_queue, g->R.d_board, nhelp, jl, g->R.use_tc);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }

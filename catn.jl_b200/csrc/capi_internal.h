@@ -10,15 +10,30 @@
 #include <string>
 #include "catn_b200.h"
 #include "linalg.cuh"
+#include "blockjac.cuh"
 #include "host_image.h"
+
+namespace catn {
+struct JobLink;
+}
 
 namespace catn_capi {
 
 constexpr int kThreads = 256;
 // Dynamic shared memory per CTA: reduction area, GEMM tile staging, and the
-// small-SVD workspace (two CTAs fit on one SM).
+// small-SVD workspace.  The persistent kernel's 255 registers per thread
+// limit an SM to one 256-thread CTA; the 100 KiB would fit twice.
 constexpr int kSmemBytes = 100 * 1024;
 constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - catn::GEMM_STAGE_BYTES) / 8;
+static_assert(kSwsDoubles >= catn::kBlockWsDoubles, "block-route items need their workspace in shared memory");
+// Launches with split-precision instances add the tensor-core staging area
+// (blockjac_tc.cuh) after the small-SVD workspace.
+constexpr int kSmemBytesTc = kSmemBytes + catn::kTcRegionBytes + 1024;
+static_assert(kSmemBytesTc <= 227 * 1024, "shared memory per CTA");
+// The staging area of a kernel's dynamic shared memory (1024-aligned).
+__device__ inline unsigned char* tc_region(double* smem) {
+  return (unsigned char*)((((uintptr_t)smem + kSmemBytes) + 1023) & ~(uintptr_t)1023);
+}
 // Smallest rows x columns whose Householder steps (pivoted QR, applying Q)
 // are shared with helper warps: one publish/claim/wait per reflector must be
 // outweighed.  On the 512-instance spin-glass batch 2^20 / 2^18 / 2^17 / 2^16
@@ -53,6 +68,7 @@ struct DeviceRun {
   int nslots = 0;
   int ngrid = 0;   // CTAs per launch: nslots, or every resident CTA for one network (the rest help)
   int ninst = 0;
+  int use_tc = 0;  // some instance runs in split precision: TMEM and the staging area per CTA
   long long input_bytes = 0;
 
   void release() {
@@ -76,12 +92,11 @@ struct GradRun {
 // Sizes slots and packs the image (capi.cu).
 catn_status prepare(const catn::Image& im, long long arena_bytes, int max_slots, DeviceRun& R);
 catn_status upload(DeviceRun& R, cudaStream_t st);
-// Dedicated helper CTAs of a launch of R and the smallest column count whose
-// Jacobi sweeps are shared (capi.cu).  `pool`: keep the batch helper pool
-// (one network always gets every other resident CTA as a helper).
-// Dedicated helper CTAs of a launch (`pool`, or CATN_HELPER_CTAS) and the
-// sharing thresholds.
-void helper_config(const DeviceRun& R, int pool, int* nhelp, int* min_n, long long* min_qr);
+// Helper pool and sharing thresholds of a launch of R from the tuning table
+// in force (capi.cu); `grad` selects the gradient launches' pool.  One
+// network always gets every other resident CTA as a helper.  The launch's
+// CTAs fill in their own job and queue pointers.
+void helper_config(const DeviceRun& R, bool grad, catn::JobLink* jl, int* nhelp);
 // Helper pool of batch gradient launches: 0 / 8 / 16 / 24 CTAs measured 592-598
 // / 547 / 578 / 610 ms on the 512-instance spin-glass batch (taped instances
 // are long, so most CTAs are worth more as workers).

@@ -6,7 +6,6 @@
 // persistent kernel's register allocation (capi.cu) is unaffected by this
 // kernel sharing the engine's out-of-line routines.
 #include <cuda_runtime.h>
-#include <mutex>
 #include <string>
 #include "engine.cuh"
 #include "host_image.h"
@@ -28,28 +27,23 @@ __global__ void __launch_bounds__(kThreads) catn_static_kernel(char* base, long 
   T.red = smem;
   T.stage = (char*)(smem + 64);
   T.stage_bytes = GEMM_STAGE_BYTES;
+  T.tcs = nullptr;
+  T.tmem = 0;
   double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
   const InstDesc D = *(const InstDesc*)(base + off_desc);
   run_instance(T, base + off_slot, L, D, (const long long*)(base + off_i64), (const int*)(base + off_i32),
                (const double*)(base + off_dat), (catn_result*)(base + off_res), nullptr, sws, kSwsDoubles);
 }
 
-// Device address of g_static_scratch, looked up once per device (with that
-// device current) on the first call there.
+// Device address of g_static_scratch on the current device.  It is looked up
+// on every call, with that device current: the lookup allocates nothing, and
+// an address kept from an earlier call would be stale after cudaDeviceReset
+// (the module, and with it the array, is loaded again).
 catn_status static_scratch_address(char** out) {
-  static std::mutex mu;
-  static char* addr[256] = {nullptr};
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) return fail(CATN_EINVAL, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* ptr = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress(&ptr, g_static_scratch));
-    CUDA_TRY(cudaFuncSetAttribute(catn_static_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
-    addr[dev] = (char*)ptr;
-  }
-  *out = addr[dev];
+  void* ptr = nullptr;
+  CUDA_TRY(cudaGetSymbolAddress(&ptr, g_static_scratch));
+  CUDA_TRY(cudaFuncSetAttribute(catn_static_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+  *out = (char*)ptr;
   return CATN_OK;
 }
 

@@ -58,8 +58,8 @@ struct InstDesc {
   int trace_cap;       // records of 8 int32 (0 = no trace)
   int cost;            // work estimate (real edges) used to order the queue
   int multigraph;      // some node lists the same neighbour twice
-  int rsvd_min;        // randomized-SVD route threshold override for tests
-                       // (CATN_RSVD_MIN_DIM; 0 = the reference's 7000 / 20000)
+  int rsvd_min;        // randomized-SVD route threshold (catn_params.rsvd_min_dim;
+                       // 0 = the reference's 7000 / 20000)
   long long trace_off; // int32 offset into the trace buffer
   long long edge_off;  // BraKet (kind 2): int32 image, edge pairs in processing order
   int n_edges;

@@ -25,6 +25,7 @@
 //   contraction! .............. tensor_network.jl:556-717   -> contract
 #pragma once
 #include "linalg.cuh"
+#include "blockjac.cuh"
 #include "ising_build.cuh"
 #include "catn_layout.h"
 
@@ -109,6 +110,7 @@ struct Ctx {
   int ninst, job_min_n;
   int job_pool;        // CTAs of the launch do nothing but help: share from the start
   long long job_min_qr;   // smallest rows x columns whose Householder work is shared
+  int block_min_n;     // smallest Jacobi factor (columns) on the block route
 };
 
 // Where a batch CTA publishes its shared Jacobi sweeps (null: never).
@@ -118,6 +120,7 @@ struct JobLink {
   int ninst, min_n;
   int pool;   // the launch has dedicated helper CTAs
   long long min_qr;
+  int block_min_n;   // smallest Jacobi factor (columns) on the block route
 };
 
 // ---------------------------------------------------------------------------
@@ -386,6 +389,37 @@ CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const d
   if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
   return C.T.bcast(drained) != 0;
 }
+// Whether the one-sided Jacobi on an n-column factor X takes the block route
+// (blockjac.cuh): svd_route 2, or svd_route 0 with precision 1, for factors
+// of at least block_min_n columns held in global memory.  The factor and its
+// rotations must lie outside the shared-memory workspace, which the block
+// items use (the SVD routines place both there when 2 n^2 doubles fit).
+CATN_HD bool use_block(const Ctx& C, long long n, const double* X) {
+  if (X == C.sws || 2 * n * n <= C.sws_doubles || n < C.block_min_n) return false;
+  return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
+}
+// The shared job for a block-route Jacobi (null: the owner's team alone):
+// always with dedicated helper CTAs, otherwise once the queue is drained.
+CATN_HDI inline JacobiJob* block_job(Ctx& C) {
+  if (!C.job) return nullptr;
+  if (C.job_pool) return C.job;
+  long long drained = 0;
+  if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
+  return C.T.bcast(drained) != 0 ? C.job : nullptr;
+}
+// One-sided Jacobi of X (rows x n, ld) with V accumulated, on the route the
+// parameters select.  Returns jacobi_sweeps' codes.
+CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, long long ld, double* V,
+                               double* nrm) {
+  if (use_block(C, n, X)) {
+    // precision 1: rotations stop at the rounding level of FP32 products
+    const double floor_rel = C.P.precision == 1 ? 4e-7 : 0.0;
+    return jacobi_block(C.T, block_job(C), X, rows, n, ld, V, 60, C.sws, floor_rel, C.P.precision == 1);
+  }
+  return share_jacobi(C, n, X) ? jacobi_sweeps_shared(C.T, C.job, X, rows, n, ld, V, 60, nrm)
+                               : jacobi_sweeps(C.T, X, rows, n, ld, V, 60, nrm);
+}
+
 // Blocked application of Q: panel width and the smallest m x ncols product
 // that takes it (with at least two panels of reflectors; below that the
 // per-reflector passes are faster).
@@ -465,8 +499,7 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
     X2[e] = (j <= i) ? Tt[j + i * nn] : 0.0;
   }
   T.sync();
-  int sweeps = share_jacobi(C, r, X2) ? jacobi_sweeps_shared(T, C.job, X2, r, r, r, Vb2, 60, nrm2)
-                                     : jacobi_sweeps(T, X2, r, r, r, Vb2, 60, nrm2);
+  int sweeps = jacobi_any(C, X2, r, r, r, Vb2, nrm2);
   if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X2, r, r, r, sig2, S2, perm2);
@@ -589,8 +622,7 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
     X[e] = (j <= i) ? s.W[j + i * mm] : 0.0;   // X = R^T
   }
   T.sync();
-  int sweeps = share_jacobi(C, nn, X) ? jacobi_sweeps_shared(T, C.job, X, nn, nn, nn, Vb, 60, nrm)
-                                      : jacobi_sweeps(T, X, nn, nn, nn, Vb, 60, nrm);
+  int sweeps = jacobi_any(C, X, nn, nn, nn, Vb, nrm);
   if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X, nn, nn, nn, sig, Sout, perm);
@@ -2025,6 +2057,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.job_min_n = 1 << 30;
   C.job_pool = 0;
   C.job_min_qr = 1LL << 62;
+  C.block_min_n = kBlockMinN;
   return C;
 }
 
@@ -2135,6 +2168,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     C.job_min_n = jl->min_n;
     C.job_pool = jl->pool;
     C.job_min_qr = jl->min_qr;
+    C.block_min_n = jl->block_min_n;
   }
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {

@@ -423,9 +423,8 @@ struct Image {
 
  private:
   void finish(InstDesc& D, int n, int edges, int trace_cap) {
-    // CATN_RSVD_MIN_DIM lowers the randomized-SVD route's size threshold so
-    // that tests reach it with small networks (0 / unset: the reference's)
-    if (const char* e = std::getenv("CATN_RSVD_MIN_DIM")) D.rsvd_min = std::atoi(e);
+    // the randomized-SVD route's size threshold (0: the reference's)
+    D.rsvd_min = D.P.rsvd_min_dim;
     D.trace_cap = trace_cap;
     D.cost = edges;
     D.trace_off = trace_total;

@@ -648,13 +648,15 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
 // valid claim may read it.  Kinds: Jacobi column pairs of one round-robin
 // round (B, V, nrm); Householder reflector k applied to 4-column chunks of C
 // from column c0 (reflector in column k of A), with the trailing squared
-// norms recomputed into nrm when nrm is set (pivoted QR).
-enum { JOB_JACOBI = 0, JOB_HOUSE = 1 };
+// norms recomputed into nrm when nrm is set (pivoted QR); block pairs of the
+// block Jacobi route (blockjac.cuh), claimed by whole CTAs.
+enum { JOB_JACOBI = 0, JOB_HOUSE = 1, JOB_BLOCK = 2 };
 constexpr int JOB_CHUNK = 4;   // columns per Householder claim
 struct JacobiJob {
   unsigned long long word;
   int done, rotated, round, open;
   int kind, m, n, ldb, np, k, c0, ldc;
+  int tc, pad;   // block items: products on the tensor cores (split precision)
   double tol, tk;
   double* B;     // Jacobi columns / Householder reflectors (A)
   double* V;     // Jacobi rotations / Householder target (C)
@@ -682,6 +684,19 @@ inline void fence_gpu() {}
 CATN_HD unsigned long long job_word(unsigned long long seq, long long count) {
   return (seq << 40) | ((unsigned long long)count << 20);
 }
+
+// Poll limit of the owner's wait for claimed items (a claimed item is a few
+// microseconds of work; 2^24 polls of >= 64 ns is over a second).  The test
+// build of the host harness sets it small.
+#ifndef CATN_JOB_SPIN_CAP
+#define CATN_JOB_SPIN_CAP (1LL << 24)
+#endif
+// Claims already counted when a round is published: always 0 in the library.
+// The host harness's timeout test sets it to 1, which models a helper warp
+// that claimed an item and never reported it done.
+#ifndef CATN_JOB_PHANTOM_CLAIMS
+#define CATN_JOB_PHANTOM_CLAIMS 0
+#endif
 CATN_HD void job_set_word(JacobiJob* J, unsigned long long w) {
 #if CATN_DEVICE_PASS
   atomicExch(&J->word, w);
@@ -895,22 +910,14 @@ CATN_HDI inline unsigned long long job_open(const Team& T, JacobiJob* J) {
   }
   return seq + 1;
 }
-// Publish one round of `count` items (the leader has written its payload),
-// do the team's share, wait (bounded) until every item is done.  Returns 1
-// when the wait ran out.
-CATN_HDI inline int job_round(const Team& T, JacobiJob* J, unsigned long long seq, long long count) {
-  if (T.leader()) {
-    J->done = 0;
-    fence_gpu();
-    job_set_word(J, job_word(seq, count));
-  }
-  T.sync();
-  job_work(T, J);
+// Owner side: wait (bounded) until every item of the round is reported done.
+// Returns 1 when the wait ran out.
+CATN_HDI inline int job_wait_done(const Team& T, JacobiJob* J, long long count) {
   int timed_out = 0;
   if (T.leader()) {
     long long spins = 0;
     while (ldcg_i(&J->done) < count) {
-      if (++spins > (1LL << 24)) {   // claimed items never take this long
+      if (++spins > CATN_JOB_SPIN_CAP) {   // claimed items never take this long
         timed_out = 1;
         break;
       }
@@ -925,6 +932,19 @@ CATN_HDI inline int job_round(const Team& T, JacobiJob* J, unsigned long long se
   timed_out = T.red[0] > 0.5;
   T.sync();
   return timed_out;
+}
+// Publish one round of `count` items (the leader has written its payload),
+// do the team's share, wait (bounded) until every item is done.  Returns 1
+// when the wait ran out.
+CATN_HDI inline int job_round(const Team& T, JacobiJob* J, unsigned long long seq, long long count) {
+  if (T.leader()) {
+    J->done = 0;
+    fence_gpu();
+    job_set_word(J, job_word(seq, count) + (count > 0 ? CATN_JOB_PHANTOM_CLAIMS : 0));
+  }
+  T.sync();
+  job_work(T, J);
+  return job_wait_done(T, J, count);
 }
 CATN_HDI inline void job_close(const Team& T, JacobiJob* J, unsigned long long seq) {
   if (T.leader()) {
@@ -1130,74 +1150,9 @@ CATN_HDI inline int qr_apply_q_shared(const Team& T, JacobiJob* J, const double*
   return timed_out;
 }
 
-#if defined(__CUDACC__)
-// A CTA's warps help the shared jobs of the CTAs still contracting, until
-// every instance of the launch has finished (or after a long stretch with
-// nothing to do).
-// Whether J is open with unclaimed items of its current round (warp-uniform:
-// lane 0's view).
-__device__ __forceinline__ bool job_has_items(const JacobiJob* J) {
-  int open = ldcg_i(&J->open);
-  unsigned long long word = ldcg_u(&J->word);
-  open = __shfl_sync(0xffffffffu, open, 0);
-  word = __shfl_sync(0xffffffffu, word, 0);
-  return open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
-}
-
-// Polls (of about 1 us each) that a helper warp keeps watching the job it
-// last worked on for that job's next round before it scans the board again.
+// Polls (of about 1 us each) that a helper keeps watching the job it last
+// worked on for that job's next round before it scans the board again.
 constexpr int kJobStickPolls = 64;
-
-__device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, const int* finished, int ninst) {
-  const unsigned FULL = 0xffffffffu;
-  const int w = (int)blockIdx.x * T.nwarps() + T.warp();
-  const int lane = T.lane();
-  long long idle = 0;
-  while (idle < (1LL << 22)) {
-    if (ldcg_i(finished) >= ninst) return;
-    // find a job with unclaimed items: the lanes check 32 slots at once
-    // (independent L2 loads), starting at a warp-specific block so that
-    // helpers spread over the open jobs
-    const int nblk = (nslots + 31) / 32;
-    int pick = -1;
-    for (int b = 0; b < nblk && pick < 0; ++b) {
-      const int base = ((b + w) % nblk) * 32;
-      const int s = base + lane;
-      bool ok = false;
-      if (s < nslots) {
-        const JacobiJob* J = board + s;
-        const int open = ldcg_i(&J->open);
-        const unsigned long long word = ldcg_u(&J->word);
-        ok = open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
-      }
-      const unsigned mask = __ballot_sync(FULL, ok);
-      if (mask) {
-        const int r = w & 31;   // first candidate at or after lane r (cyclically)
-        const unsigned hi = mask & (~0u << r);
-        pick = base + __ffs(hi ? hi : mask) - 1;
-      }
-    }
-    if (pick < 0) {
-      ++idle;
-      __nanosleep(256);
-      continue;
-    }
-    idle = 0;
-    JacobiJob* J = board + pick;
-    job_work(T, J);
-    // stay with J: its owner opens the next round within microseconds
-    for (int t = 0; t < kJobStickPolls; ++t) {
-      if (job_has_items(J)) {
-        job_work(T, J);
-        t = -1;
-        continue;
-      }
-      if (!ldcg_i(&J->open)) break;
-      __nanosleep(32);
-    }
-  }
-}
-#endif
 
 // Column norms of B (n columns), then stable descending order.
 // S_out[r] = sigma of the r-th largest column, perm[r] = its column index.

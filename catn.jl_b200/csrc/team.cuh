@@ -34,6 +34,11 @@ struct Team {
   double* red;
   char* stage;
   int stage_bytes;
+  // Tensor-core staging area in shared memory and the CTA's TMEM columns
+  // for the split-precision products (null / 0: none; set by the kernels
+  // that allocate them, never in the host build).
+  unsigned char* tcs;
+  unsigned tmem;
 
 #if CATN_DEVICE_PASS
   __device__ __forceinline__ int rank() const { return threadIdx.x; }

@@ -29,7 +29,8 @@ class IsingNetwork(TensorNetwork):
 
     def __init__(self, n, edges, weights, fields, beta, pos1=0, val1=0, pos2=0, val2=0, Dmax=32, chi=32,
                  cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True, swapopt=True,
-                 compress=False, cut_bond=False, seed=1, rsvd=0):
+                 compress=False, cut_bond=False, seed=1, rsvd=0, rsvd_min_dim=0,
+                 precision="fp64", svd_route="auto"):
         self.kind = "ising"
         self.n = int(n)
         self.edges = np.asarray(edges, dtype=np.int32).reshape(-1, 2) if len(edges) else np.zeros((0, 2), np.int32)
@@ -43,7 +44,8 @@ class IsingNetwork(TensorNetwork):
         self.pins = (int(pos1), int(val1), int(pos2), int(val2))
         self.params = dict(Dmax=Dmax, chi=chi, cutoff=cutoff, norm_method=norm_method, select=select,
                            reverse=reverse, svdopt=svdopt, swapopt=swapopt, compress=compress,
-                           cut_bond=cut_bond, seed=seed, rsvd=rsvd)
+                           cut_bond=cut_bond, seed=seed, rsvd=rsvd,
+                           rsvd_min_dim=rsvd_min_dim, precision=precision, svd_route=svd_route)
         self.neighbors = [[0, 0] for _ in range(self.edges.shape[0])]   # trace sizing only
         deg = np.zeros(self.n + 1, int)
         for i, j in self.edges:

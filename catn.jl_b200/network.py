@@ -44,7 +44,8 @@ class TensorNetwork:
     """
 
     def __init__(self, tensors, ixs, Dmax=32, chi=32, cutoff=1e-15, norm_method=1, select=1,
-                 reverse=True, svdopt=True, swapopt=True, compress=False, cut_bond=False, seed=1, rsvd=0):
+                 reverse=True, svdopt=True, swapopt=True, compress=False, cut_bond=False, seed=1, rsvd=0, rsvd_min_dim=0,
+                 precision="fp64", svd_route="auto"):
         n = len(tensors)
         if len(ixs) != n:
             raise ValueError("tensors and ixs must have the same length")
@@ -83,7 +84,8 @@ class TensorNetwork:
         self.beta = 1.0
         self.params = dict(Dmax=Dmax, chi=chi, cutoff=cutoff, norm_method=norm_method, select=select,
                            reverse=reverse, svdopt=svdopt, swapopt=swapopt, compress=compress,
-                           cut_bond=cut_bond, seed=seed, rsvd=rsvd)
+                           cut_bond=cut_bond, seed=seed, rsvd=rsvd,
+                           rsvd_min_dim=rsvd_min_dim, precision=precision, svd_route=svd_route)
         self.num_isolated = sum(1 for v in nbr if all(x < 0 for x in v))
         self._reset_outputs()
         self._dev = None

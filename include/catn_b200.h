@@ -5,8 +5,9 @@
  * Julia dispatch on the array type `AT` of `TensorNetwork{T,AT}` /
  * `MPSNode{T,AT}` (src/tensor_network.jl:1, src/mps_node.jl:1) entered
  * through `Adapt.adapt_structure` (src/adapt.jl:6-24).  Each entry point
- * below replaces the reference function named beside it; a Julia `ccall`
- * binding for each is given in INTEGRATION.md.
+ * below replaces the reference function named beside it (a Julia `ccall`
+ * binding for each is one line per function: the argument types below map
+ * to Cint, Cdouble, Ptr{...} one to one).
  *
  * Conventions
  *   - Node ids are 1-based, neighbour ids of open legs are negative
@@ -61,7 +62,47 @@ typedef struct {
                         * columns, 10 power iterations), its Gaussian sketch
                         * drawn from the counter-based generator keyed by
                         * seed (forward runs; gradient runs use 0)          */
+  /* Fields below have no counterpart in the reference's keywords. */
+  int32_t rsvd_min_dim; /* > 0: the randomized route above takes swap!
+                        * matrices with both sides >= rsvd_min_dim or one
+                        * side >= 3 rsvd_min_dim (tests reach it with small
+                        * networks); 0 = the reference's 7000 / 20000      */
+  int32_t precision;   /* 0 = FP64 throughout; 1 = split: the products of
+                        * large swap merges and of the block-Jacobi SVD
+                        * route (pair Grams, pair rotations) in 3xTF32 on
+                        * the tensor cores with FP32 accumulation, while the
+                        * Jacobi eigen cores, every singular-value cutoff
+                        * test, the Dmax cut and lnZ stay FP64            */
+  int32_t svd_route;   /* large SVDs (not held in shared memory):
+                        * 0 = auto (precision 0: scalar Jacobi; precision 1:
+                        *     block Jacobi from the tuning table's size on),
+                        * 1 = scalar one-sided Jacobi on the pivoted-QR
+                        *     factor (the FP64 route of earlier releases,
+                        *     bit for bit),
+                        * 2 = block one-sided Jacobi on the pivoted-QR
+                        *     factor from the tuning table's size on      */
 } catn_params;
+
+/* Launch-shape and route thresholds, one process-wide table (no reference
+ * counterpart).  catn_tuning_get returns the table in force (the built-in
+ * defaults until catn_tuning_set is called); the autotuner
+ * (catn_b200.tune) measures candidates on the GPU and installs the winners
+ * with catn_tuning_set.  A value < 0 selects the built-in default.  The
+ * table is read when a launch starts; results never depend on the helper
+ * and sharing entries, only the block-route entries change arithmetic. */
+typedef struct {
+  int32_t helper_ctas;         /* dedicated helper CTAs of a batch launch   */
+  int32_t grad_helper_ctas;    /* the same for batch gradient launches      */
+  int32_t shared_jacobi_min_n; /* smallest column count whose Jacobi rounds
+                                * are opened to helper CTAs                 */
+  int32_t block_min_n;         /* smallest column count of the Jacobi factor
+                                * that takes the block route (svd_route 0
+                                * with precision 1, and svd_route 2)        */
+  int64_t shared_house_min;    /* smallest rows x columns whose Householder
+                                * steps are opened to helper CTAs           */
+} catn_tuning;
+catn_status catn_tuning_get(catn_tuning* t);
+catn_status catn_tuning_set(const catn_tuning* t);
 
 /* Default values of the reference's keyword arguments. */
 void catn_params_default(catn_params* p);
@@ -162,9 +203,10 @@ catn_status catn_ising_create(const catn_params* p, int32_t n, int32_t n_edges,
  * latency and fragmentation are not acceptable.
  *   - Networks whose working memory does not fit return CATN_ENOMEM with
  *     the required and available sizes in catn_last_error().
- *   - The first call on a device looks up the array's device address (once
- *     per device, with that device current); make that first call before
- *     any stream capture.
+ *   - Every call looks up the array's device address on the current device
+ *     (cudaGetSymbolAddress, which allocates nothing) and sets the kernel's
+ *     shared-memory attribute; make the first call on a device before any
+ *     stream capture.
  *   - Every call reuses the same array, so calls that overlap on the GPU
  *     (different streams, threads or processes sharing a context) race;
  *     serialise them.  The call synchronises `stream` before returning.
@@ -175,6 +217,15 @@ catn_status catn_ising_contract_static(const catn_params* p, int32_t n, int32_t 
                                        const double* fields, double beta, int32_t pos1,
                                        int32_t val1, int32_t pos2, int32_t val2, void* stream,
                                        catn_result* res);
+
+/* No counterpart in the reference.  C (M x N) = A (M x K) * B (K x N), all
+ * column-major FP64 host buffers, computed on the tensor cores in the
+ * split-precision form of catn_params.precision = 1: the operands rounded
+ * to FP32 and split into TF32 hi / lo parts, three tcgen05 TF32 products per
+ * pair (hi hi + hi lo + lo hi) accumulated in FP32.  Relative error about
+ * 1e-6 of |A| |B|.  It exposes the tensor-core primitive the split mode's
+ * large products use, so that it can be checked on its own. */
+catn_status catn_tc_matmul(int32_t M, int32_t N, int32_t K, const double* A, const double* B, double* C);
 
 /* Batched Ising instances contracted in ONE persistent kernel launch with a
  * device work queue (no reference counterpart: the reference loops on the

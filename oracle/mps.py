@@ -13,7 +13,7 @@ from .linalg import tsvd, rsvd, thin_qr, counter_normal, _svd_full
 
 # Randomized-SVD route of swap! (test infrastructure).  RSVD_MIN overrides
 # the reference's size thresholds (7000 / 20000 become RSVD_MIN / 3 RSVD_MIN,
-# as the engine's CATN_RSVD_MIN_DIM does).  RSVD_SKETCH_SEED, when set,
+# as the engine's catn_params.rsvd_min_dim does).  RSVD_SKETCH_SEED, when set,
 # draws the sketch from the engine's counter-based generator (that seed,
 # stream 16 + RSVD_CALLS), which pins the engine's rsvd = 1 mode; callers
 # reset RSVD_CALLS to 0 before each network.

@@ -2,6 +2,7 @@
 // CPU test-suite to check the engine's integer bookkeeping and memory safety
 // (under AddressSanitizer) against the oracle.  It is not part of
 // libcatn_b200 and is never loaded by the product path.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -22,28 +23,35 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   T.red = red.data();
   T.stage = nullptr;
   T.stage_bytes = 0;
+  T.tcs = nullptr;
+  T.tmem = 0;
   std::vector<int> tr((size_t)im.trace_total + 8);
   // stand-in for the GPU's shared-memory SVD workspace (same capacity)
   long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   // CATN_HOSTCHECK_SWS overrides the capacity (0 sends every SVD through the
   // large-matrix path, including its rank-revealing truncation)
   if (const char* e = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(e);
-  std::vector<double> sws((size_t)(sws_doubles > 0 ? sws_doubles : 1));
+  // at least the block route's item workspace, whatever capacity is reported
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
   // CATN_HOSTCHECK_JOB=1 sends the Jacobi sweeps of every SVD on the global
-  // path through the shared-job protocol (no helpers: the team claims all)
+  // path through the shared-job protocol (no helpers: the team claims all);
+  // CATN_HOSTCHECK_BLOCK_MIN sets the smallest factor on the block route
   JacobiJob job;
   std::memset(&job, 0, sizeof(job));
   const int qhead = 1;
+  const char* je = std::getenv("CATN_HOSTCHECK_JOB");
+  const bool shared = je && je[0] == '1';
   JobLink jl;
-  jl.job = &job;
+  jl.job = shared ? &job : nullptr;
   jl.qhead = &qhead;
   jl.ninst = 1;
-  jl.min_n = 2;
+  jl.min_n = shared ? 2 : (1 << 30);
   jl.pool = 0;
-  jl.min_qr = 1;
-  const char* je = std::getenv("CATN_HOSTCHECK_JOB");
+  jl.min_qr = shared ? 1 : (1LL << 62);
+  jl.block_min_n = kBlockMinN;
+  if (const char* eb = std::getenv("CATN_HOSTCHECK_BLOCK_MIN")) jl.block_min_n = std::atoi(eb);
   run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
-               sws_doubles, (je && je[0] == '1') ? &jl : nullptr);
+               sws_doubles, &jl);
   if (trace && im.desc[0].trace_cap > 0)
     std::memcpy(trace, tr.data(), sizeof(int) * 8 * (size_t)im.desc[0].trace_cap);
   return res->status;
@@ -76,9 +84,12 @@ int catn_hostcheck_ising_grad(const catn_params* p, int n, int n_edges, const in
   T.red = red.data();
   T.stage = nullptr;
   T.stage_bytes = 0;
+  T.tcs = nullptr;
+  T.tmem = 0;
   long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   if (const char* ev = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(ev);
-  std::vector<double> sws((size_t)(sws_doubles > 0 ? sws_doubles : 1));
+  // at least the block route's item workspace, whatever capacity is reported
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
   std::vector<double> gimg(im.dat.size() + 1, 0.0);
   run_instance_grad(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, gimg.data(),
                     sws.data(), sws_doubles);
@@ -102,8 +113,10 @@ int catn_hostcheck_braket(const catn_params* p, int n, const int* ndims, const l
   T.red = red.data();
   T.stage = nullptr;
   T.stage_bytes = 0;
+  T.tcs = nullptr;
+  T.tmem = 0;
   long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
-  std::vector<double> sws((size_t)sws_doubles);
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
   std::vector<int> tr((size_t)im.trace_total + 8);
   run_instance_braket(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
                       sws_doubles);

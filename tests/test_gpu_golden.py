@@ -88,3 +88,21 @@ def test_spinglass_sample_as_one_batch_golden(catn):
         assert r.maxdim == o["maxdim"]
         assert abs(r.lnZ - o["lnZ"]) / inst["n"] <= 1e-10
         assert abs(r.err - o["err"]) <= 1e-12 + 1e-6 * abs(o["err"])
+
+
+@pytest.mark.parametrize("precision,bar", [("fp64", 1e-10), ("split", 1e-6)])
+def test_random_regular_spin_glass_block_route_golden(catn, precision, bar):
+    """The n=200 configuration on the block Jacobi route for its large SVDs
+    (svd_route = block): FP64 holds the fixture's trace and 1e-10 per spin;
+    the split-precision form holds the trace and 1e-6 per spin against the
+    FP64 oracle."""
+    d = _load("rrg200.json")
+    for k, beta in enumerate(d["betas"]):
+        params = dict(d["params"], svd_route="block", precision=precision)
+        lnZ, err, psi, maxdim, rows = _contract(catn, d, beta, params)
+        ref = d["oracle"][k]
+        assert rows == ref["trace"]
+        assert abs(lnZ - ref["lnZ"]) / d["n"] <= bar
+        assert psi == ref["psi"]
+        assert maxdim == ref["maxdim"]
+        assert abs(err - ref["err"]) <= 1e-6 + (1e-6 if precision == "fp64" else 1e-3) * abs(ref["err"])

@@ -207,3 +207,86 @@ def test_shared_jacobi_protocol(host, name, L, beta, kw, monkeypatch):
     (lz, err, psi), orows, tn = oracle_ising(L * L, e, w, h, beta, **kw)
     assert st == 0 and rows == orows
     assert abs(res.lnZ - lz) / (L * L) < 1e-12
+
+
+def test_shared_wait_timeout_reports_etimeout(host, monkeypatch):
+    """The owner's bounded wait for claimed items of a shared round
+    (linalg.cuh job_round) runs out: the timeout build of the harness
+    publishes every round with one claim that is never reported done (a
+    helper that stopped) and polls at most 2000 times.  The instance must end
+    with CATN_ETIMEOUT instead of waiting, and a following network on the
+    regular build must still complete."""
+    stall = ct.CDLL(hostbuild.build(stall=True))
+    r = np.random.default_rng(3)
+    L_ = 8
+    e = X.square_edges(L_)
+    w, h = r.normal(size=len(e)), r.normal(0, 0.1, L_ * L_)
+    kw = dict(Dmax=8, chi=32)
+    # without the shared path the timeout build contracts normally
+    st, res, _ = run_ising(stall, L_ * L_, e, w, h, 1.0, **kw)
+    assert st == 0 and res.status == 0
+    # every large SVD through the shared protocol: the first round times out
+    monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
+    monkeypatch.setenv("CATN_HOSTCHECK_SWS", "0")
+    st, res, _ = run_ising(stall, L_ * L_, e, w, h, 1.0, **kw)
+    assert st == L.CATN_ETIMEOUT and res.status == L.CATN_ETIMEOUT
+    # the regular build on the same shared path completes and matches the oracle
+    st, res, rows = run_ising(host, L_ * L_, e, w, h, 1.0, **kw)
+    (lz, _, _), orows, _ = oracle_ising(L_ * L_, e, w, h, 1.0, **kw)
+    assert st == 0 and res.status == 0 and rows == orows
+    assert abs(res.lnZ - lz) / (L_ * L_) < 1e-12
+
+
+BLOCK_CASES = [
+    ("block_l12_d32", 12, 1.5, dict(Dmax=32, chi=128), False),
+    ("block_l14_d32_shared", 14, 1.5, dict(Dmax=32, chi=128), True),
+    ("block_l12_d16_select0", 12, 1.3, dict(Dmax=16, chi=96, select=0), True),
+]
+
+
+def _lattice(name, L_):
+    r = np.random.default_rng(zlib.crc32(name.encode()) % 1000)
+    e = X.square_edges(L_)
+    return e, r.normal(size=len(e)), r.normal(0, 0.1, L_ * L_)
+
+
+@pytest.mark.parametrize("name,L_,beta,kw,shared", BLOCK_CASES, ids=[c[0] for c in BLOCK_CASES])
+def test_block_route_matches_oracle(host, monkeypatch, name, L_, beta, kw, shared):
+    """Every SVD on the global path (workspace capacity 0), Jacobi factors of
+    >= 16 columns on the block route (svd_route = 2), alone or through the
+    shared-job protocol: the integer trace identical to the oracle's, lnZ
+    within 1e-12 per spin (the route's singular values carry absolute error
+    ~ eps sigma_1, like LAPACK's), and a different rounding history than the
+    scalar route (the block route was taken)."""
+    monkeypatch.setenv("CATN_HOSTCHECK_SWS", "0")
+    monkeypatch.setenv("CATN_HOSTCHECK_BLOCK_MIN", "16")
+    if shared:
+        monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
+    e, w, h = _lattice(name, L_)
+    st, res, rows = run_ising(host, L_ * L_, e, w, h, beta, svd_route="block", **kw)
+    (lz, err, psi), orows, tn = oracle_ising(L_ * L_, e, w, h, beta, **kw)
+    assert st == 0 and res.status == 0
+    assert rows == orows
+    assert abs(res.lnZ - lz) / (L_ * L_) < 1e-12
+    assert res.maxdim == tn.maxdim_intermediate
+    assert abs(res.err - err) <= 1e-10 + 1e-8 * abs(err)
+    st, res_s, _ = run_ising(host, L_ * L_, e, w, h, beta, svd_route="scalar", **kw)
+    assert st == 0 and (res_s.lnZ, res_s.err) != (res.lnZ, res.err)
+
+
+def test_block_route_random_regular_graph(host, monkeypatch):
+    """A random 3-regular +-1 glass (n = 110, Dmax 32, chi 128) whose swaps
+    reach 512-column factors, through the shared-job protocol on the
+    default block threshold's side of the route."""
+    monkeypatch.setenv("CATN_HOSTCHECK_SWS", "0")
+    monkeypatch.setenv("CATN_HOSTCHECK_BLOCK_MIN", "80")
+    monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
+    r = np.random.default_rng(110)
+    e = X.random_regular_graph(110, 3, r)
+    w, h = r.choice([-1.0, 1.0], size=len(e)), r.normal(0, 0.1, 110)
+    kw = dict(Dmax=32, chi=128)
+    st, res, rows = run_ising(host, 110, e, w, h, 1.0, svd_route="block", **kw)
+    (lz, err, psi), orows, _ = oracle_ising(110, e, w, h, 1.0, **kw)
+    assert st == 0 and rows == orows
+    assert abs(res.lnZ - lz) / 110 < 1e-12
+    assert abs(res.err - err) <= 1e-10 + 1e-8 * abs(err)

@@ -3,8 +3,8 @@ linalg_utils.jl:44-58) with a reproducible sketch (catn_params.rsvd = 1):
 the engine draws the Gaussian sketch from its counter-based generator
 keyed by (seed, call index), and the oracle, given the same sketch, runs the
 reference's algorithm.  The route's size threshold is lowered through
-CATN_RSVD_MIN_DIM (engine) and RSVD_MIN (oracle) so that small networks
-reach it; the default thresholds are the reference's 7000 / 20000.
+catn_params.rsvd_min_dim (engine) and RSVD_MIN (oracle) so that small
+networks reach it; the default thresholds are the reference's 7000 / 20000.
 
 Bars: the per-step integer trace identical to the oracle's and
 |dlnZ|/n <= 1e-10; the oracle's sketch generator equal to the engine's
@@ -34,7 +34,6 @@ CASES = [("full_sketch", 6, dict(Dmax=8, chi=4), 4), ("narrow_sketch", 8, dict(D
 
 
 def route(monkeypatch, rmin):
-    monkeypatch.setenv("CATN_RSVD_MIN_DIM", str(rmin))
     monkeypatch.setattr(OM, "RSVD_MIN", rmin)
     monkeypatch.setattr(OM, "RSVD_SKETCH_SEED", 3)
     monkeypatch.setattr(OM, "RSVD_CALLS", 0)
@@ -78,7 +77,7 @@ def test_host_engine_matches_oracle(monkeypatch, name, L, kw, rmin):
     n, e, w, h, beta = instance(L, 7)
     lz, rows, calls = oracle_run(n, e, w, h, beta, kw)
     assert calls > 0   # the route was taken
-    st, res, drows = run_ising(lib, n, e, w, h, beta, rsvd=1, seed=3, **kw)
+    st, res, drows = run_ising(lib, n, e, w, h, beta, rsvd=1, rsvd_min_dim=rmin, seed=3, **kw)
     assert st == 0
     assert drows == rows
     assert abs(res.lnZ - lz) / n <= 1e-10
@@ -91,13 +90,13 @@ def test_gpu_matches_oracle(monkeypatch, catn, name, L, kw, rmin):
     n, e, w, h, beta = instance(L, 7)
     lz, rows, calls = oracle_run(n, e, w, h, beta, kw)
     assert calls > 0
-    tn = catn.ising_network(n, e, w, h, beta, rsvd=1, seed=3, **kw)
+    tn = catn.ising_network(n, e, w, h, beta, rsvd=1, rsvd_min_dim=rmin, seed=3, **kw)
     dlz, err, psi = catn.contraction(tn, trace=True)
     drows = [tuple(int(x) for x in r[:7]) for r in tn.trace]
     assert drows == rows
     assert abs(dlz - lz) / n <= 1e-10
     assert err == 0.0 or err >= 0.0
     # rsvd = 0 on the same route: the exact top-chi subspace
-    tn0 = catn.ising_network(n, e, w, h, beta, rsvd=0, seed=3, **kw)
+    tn0 = catn.ising_network(n, e, w, h, beta, rsvd=0, rsvd_min_dim=rmin, seed=3, **kw)
     lz0 = catn.contraction(tn0)[0]
     assert np.isfinite(lz0)
