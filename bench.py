@@ -271,6 +271,9 @@ def main():
     ap.add_argument("--plain-seconds", type=float, default=15.0,
                     help="time budget of the plain GPU form sample (0 = skip)")
     ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
+    ap.add_argument("--no-c2", action="store_true", help="skip the n=200 random-regular leg")
+    ap.add_argument("--c2-oracle", action="store_true",
+                    help="also time the FP64 oracle on one beta of the n=200 random-regular leg (~40 s)")
     ap.add_argument("--arena-mb", type=int, default=64, help="device arena per slot, MiB")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -449,10 +452,65 @@ def main():
             "sample": f"first {cnt} of the {args.instances} workload instances in order, one at a time, "
                       f"PyTorch FP64 on cuda:{local} (torch.linalg.svd/qr + einsum per op, host loop), "
                       f"~{args.plain_seconds:.0f} s wall clock"}
+    if world == 1 and not args.no_c2:
+        out["rrg200"] = c2_leg(catn, args)
     print(json.dumps(out))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _oracle_rrg200(beta):
+    """FP64 oracle on the n=200 random-regular configuration (spawned
+    process, all host cores to BLAS); returns (lnZ, seconds)."""
+    from oracle import ising as OI, network as ON
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "rrg200.json")))
+    t0 = time.perf_counter()
+    tn = OI.ising_network(d["n"], d["edges"], d["weights"], d["fields"], beta, **d["params"])
+    lnZ, _, _ = ON.contraction(tn)
+    return lnZ, time.perf_counter() - t0
+
+
+def c2_leg(catn, args):
+    """The n=200 random 3-regular +-1 spin glass (300 edges, h ~ N(0, 0.1^2),
+    beta in {0.5, 1, 1.5}, Dmax 32, chi 128), one network per beta through
+    the public API (host image in, results out), in three forms: FP64 on the
+    scalar Jacobi route, FP64 on the block Jacobi route, and the split
+    precision form (3xTF32 tensor-core products, block route).  Errors are
+    against the FP64 oracle's values frozen in tests/golden/rrg200.json (made
+    by tests/golden/make_golden.py); the trace must equal the oracle's."""
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "rrg200.json")))
+    edges = [tuple(e) for e in d["edges"]]
+    res = {"workload": "random 3-regular +-1 spin glass, n=200 (300 edges), h~N(0,0.1^2), beta in {0.5,1,1.5}, "
+                       "Dmax=32, chi=128, seed 200 (tests/golden/rrg200.json)",
+           "timing": "host wall clock around catn.contraction (device move done before; the launch and the "
+                     "result read-back inside)",
+           "forms": {}}
+    forms = [("fp64_scalar", dict(svd_route="scalar"), [1.0]),
+             ("fp64_block", dict(svd_route="block"), d["betas"]),
+             ("split", dict(svd_route="block", precision="split"), d["betas"])]
+    for name, kw, betas in forms:
+        per = []
+        for beta in betas:
+            k = d["betas"].index(beta)
+            ref = d["oracle"][k]
+            tn = catn.ising_network(d["n"], edges, d["weights"], d["fields"], beta, **d["params"], **kw)
+            catn.adapt(catn.B200, tn, trace=True)
+            t0 = time.perf_counter()
+            lnZ, err, psi = catn.contraction(tn, trace=True)
+            dt = time.perf_counter() - t0
+            rows = [[int(x) for x in r[:7]] for r in tn.trace]
+            per.append({"beta": beta, "s": round(dt, 3), "abs_dlnZ_per_spin": abs(lnZ - ref["lnZ"]) / d["n"],
+                        "trace_identical": rows == ref["trace"], "err": err, "oracle_err": ref["err"]})
+        res["forms"][name] = {"s_per_beta": round(sum(p["s"] for p in per) / len(per), 3),
+                              "max_abs_dlnZ_per_spin": max(p["abs_dlnZ_per_spin"] for p in per),
+                              "traces_identical": all(p["trace_identical"] for p in per), "runs": per}
+    if args.c2_oracle:
+        with mp.get_context("spawn").Pool(1) as pool:
+            lz, secs = pool.apply(_oracle_rrg200, (1.0,))
+        res["oracle_fp64_cpu"] = {"beta": 1.0, "s": round(secs, 3), "cores": host_cores(),
+                                  "what": "the oracle port (numpy/OpenBLAS, all cores to BLAS)"}
+    return res
 
 
 def _pin_sets(d):

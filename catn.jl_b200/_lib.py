@@ -44,7 +44,7 @@ class Result(ct.Structure):
     _fields_ = [("lnZ", ct.c_double), ("err", ct.c_double), ("psi", ct.c_double),
                 ("sign", ct.c_double), ("maxdim", ct.c_int32), ("status", ct.c_int32),
                 ("nsteps", ct.c_int32), ("jacobi_max", ct.c_int32), ("arena_peak", ct.c_int64),
-                ("flops", ct.c_double), ("bytes", ct.c_double), ("prof", ct.c_double * 16)]
+                ("flops", ct.c_double), ("bytes", ct.c_double), ("prof", ct.c_double * 24)]
 
 
 # Every exported symbol with its ctypes signature (argtypes, restype).
@@ -108,7 +108,27 @@ def load(path=None):
         fn.restype = res
     if path is None:
         _lib = lib
+        _apply_committed_tuning(lib)
     return lib
+
+
+TUNING_PATH = os.path.join(_HERE, "tuning_b200.json")
+
+
+def _apply_committed_tuning(lib):
+    """Install the autotuner's table (tune.py) if one is saved beside the
+    package; entries absent from it keep the built-in defaults."""
+    if not os.path.exists(TUNING_PATH):
+        return
+    import json
+    with open(TUNING_PATH) as f:
+        table = json.load(f).get("table", {})
+    t = Tuning()
+    check(lib, lib.catn_tuning_get(ct.byref(t)))
+    for name, _ in Tuning._fields_:
+        if name in table:
+            setattr(t, name, int(table[name]))
+    check(lib, lib.catn_tuning_set(ct.byref(t)))
 
 
 def last_error(lib):

@@ -30,7 +30,7 @@ constexpr int kTcOffQhi = 64 * 1024;         // 32 x 32, K-major
 constexpr int kTcOffQlo = 68 * 1024;
 constexpr int kTcOffCtl = 72 * 1024;         // mbarrier, TMEM slot, counters
 constexpr int kTcRegionBytes = 72 * 1024 + 64;
-constexpr int kTcTmemCols = 32;
+constexpr int kTcTmemCols = 128;   // block items use columns 0-31, merges 0-127
 constexpr long long kTcWaitPolls = 1LL << 22;
 
 #if defined(__CUDACC__)
@@ -272,6 +272,99 @@ __device__ inline bool tc_rotate(const Team& T, double* Y, long long m, long lon
   if (nch > 0) {
     if (!tc_wait(T, &commits)) return false;
     store(nch - 1);
+  }
+  tc_finish(T, commits, 0);
+  return true;
+}
+// C (M x N, written through the operand map `out`) = A (M x K, column-major,
+// lda) * B (K x N, column-major, ldb) on the tensor cores, for the large
+// two-site merges of swap! in split precision.  Tiles of 128 x 128 of C, K
+// in chunks of 32; the next chunk's operands are loaded into registers while
+// the MMAs of the current one run.  Loads of A and B are plain (the CTA's
+// own sites).  Returns false when a wait ran out.
+__device__ inline bool tc_gemm_mop(const Team& T, long long M, long long N, long long K, const double* A,
+                                   long long lda, const double* B, long long ldb, const MOp& out) {
+  constexpr int BM = 128, BN = 128, KC = 32;
+  float* ahi = (float*)(T.tcs + kTcOffAhi);
+  float* bhi = (float*)(T.tcs + kTcOffAhi + 16 * 1024);
+  float* alo = (float*)(T.tcs + kTcOffAlo);
+  float* blo = (float*)(T.tcs + kTcOffAlo + 16 * 1024);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned commits = tc_ctl(T)->commits;
+  __syncthreads();
+  const long long mt = (M + BM - 1) / BM, nt = (N + BN - 1) / BN, kc = (K + KC - 1) / KC;
+  const long long iters = mt * nt * kc;
+  double va[16], vb[16];
+  auto load = [&](long long it) {
+    const long long tile = it / kc, c = it - tile * kc;
+    const long long m0 = (tile / nt) * BM, n0 = (tile % nt) * BN, k0 = c * KC;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + 256 * j;
+      const int r = e & 127, k = e >> 7;   // A: consecutive rows
+      const long long gr = m0 + r, gk = k0 + k;
+      va[j] = (gr < M && gk < K) ? A[gr + gk * lda] : 0.0;
+      const int kb = e & 31, n = e >> 5;   // B: consecutive k
+      const long long gn = n0 + n, gkb = k0 + kb;
+      vb[j] = (gn < N && gkb < K) ? B[gkb + gn * ldb] : 0.0;
+    }
+  };
+  const uint32_t idesc = tc::idesc_tf32(BM, BN);
+  const uint32_t sbo = KC / 4 * 128;
+  const uint32_t sa_hi = tc::smem_u32(ahi), sa_lo = tc::smem_u32(alo);
+  const uint32_t sb_hi = tc::smem_u32(bhi), sb_lo = tc::smem_u32(blo);
+  if (iters > 0) load(0);
+  for (long long it = 0; it < iters; ++it) {
+    const long long tile = it / kc, c = it - tile * kc;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + 256 * j;
+      float h, l;
+      tc::split_tf32(va[j], &h, &l);
+      uint32_t o = tc::kmajor_off(e & 127, e >> 7, KC) / 4;
+      ahi[o] = h;
+      alo[o] = l;
+      tc::split_tf32(vb[j], &h, &l);
+      o = tc::kmajor_off(e >> 5, e & 31, KC) / 4;
+      bhi[o] = h;
+      blo[o] = l;
+    }
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int s = 0; s < KC / 8; ++s) {
+        const uint32_t off = (uint32_t)s * 2 * tc::kLBO;
+        const uint64_t ah = tc::smem_desc(sa_hi + off, tc::kLBO, sbo), al = tc::smem_desc(sa_lo + off, tc::kLBO, sbo);
+        const uint64_t bh = tc::smem_desc(sb_hi + off, tc::kLBO, sbo), bl = tc::smem_desc(sb_lo + off, tc::kLBO, sbo);
+        tc::mma_tf32(T.tmem, ah, bh, idesc, (c > 0 || s > 0) ? 1u : 0u);
+        tc::mma_tf32(T.tmem, ah, bl, idesc, 1u);
+        tc::mma_tf32(T.tmem, al, bh, idesc, 1u);
+      }
+      tc_issue_commit(T);
+    }
+    if (it + 1 < iters) load(it + 1);
+    if (!tc_wait(T, &commits)) return false;
+    if (c == kc - 1) {
+      // epilogue: warp w reads lanes 32 (w % 4) (rows), columns 64 (w / 4) .. + 63
+      const long long m0 = (tile / nt) * BM, n0 = (tile % nt) * BN;
+      const int q = warp & 3, half = warp >> 2;
+      const long long row = m0 + q * 32 + lane;
+      for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
+        float y[32];
+        tc::tmem_ld32(T.tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, y);
+        if (row < M) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const long long col = n0 + c0 + j;
+            if (col < N) out.ref(row, col) = (double)y[j];
+          }
+        }
+      }
+      tc::fence_before_sync();
+      __syncthreads();
+    }
   }
   tc_finish(T, commits, 0);
   return true;

@@ -157,7 +157,8 @@ CATN_HD long long clk() {
 }
 enum { PROF_TOTAL = 0, PROF_SVD_TINY, PROF_SVD_SMALL, PROF_SVD_LARGE, PROF_BOOK, PROF_N_TINY, PROF_N_SMALL,
        PROF_N_LARGE, PROF_SWAP_GEMM, PROF_SWAP_EPI, PROF_CANO_EPI, PROF_EAT, PROF_MERGE, PROF_CUT, PROF_REVERSE,
-       PROF_CONTROL, PROF_SLOTS, PROF_COMPACT = PROF_SLOTS, PROF_N_COMPACT = PROF_SLOTS + 1 };
+       PROF_CONTROL, PROF_LQR, PROF_LJAC, PROF_LAPPLY, PROF_N_BLOCK, PROF_BLOCK_SWEEPS, PROF_LJAC_COLS,
+       PROF_RESERVED1, PROF_RESERVED2, PROF_SLOTS, PROF_COMPACT = PROF_SLOTS, PROF_N_COMPACT = PROF_SLOTS + 1 };
 CATN_HD void prof_add(Ctx& C, int slot, double v) {
   if (C.T.leader()) C.acct[2 + slot] += v;
 }
@@ -326,7 +327,8 @@ struct SvdIn {
   double* W;
   long long m, n, mm, nn;
   bool wide, smem;
-  double tol;   // rank-revealing stop tolerance for large inputs (0 = none)
+  double tol;      // rank-revealing stop tolerance for large inputs (0 = none)
+  long long need;  // singular vectors the caller can use (the first `need`; S is always complete)
 };
 
 CATN_HD long long svd_ws_doubles(long long mm, long long nn) {
@@ -344,6 +346,7 @@ CATN_HDI inline SvdIn svd_begin(Ctx& C, long long m, long long n, double cutoff 
   s.wide = m < n;
   s.mm = s.wide ? n : m;
   s.nn = s.wide ? m : n;
+  s.need = 1LL << 40;
   if (s.mm * s.nn >= (1LL << 31)) {   // index arithmetic is 32-bit per operation
     fail_all(C, CATN_ENOMEM);
     s.smem = false;
@@ -398,6 +401,16 @@ CATN_HD bool use_block(const Ctx& C, long long n, const double* X) {
   if (X == C.sws || 2 * n * n <= C.sws_doubles || n < C.block_min_n) return false;
   return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
 }
+// Whether the large-SVD routes of this release are selected (block route
+// available, singular vectors formed only as far as the caller uses them);
+// svd_route 1, and svd_route 0 in FP64, keep the earlier arithmetic bit for bit.
+CATN_HD bool new_routes(const Ctx& C) {
+  return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
+}
+// Columns of U and V an SVD of nn values forms for its caller.
+CATN_HD long long vec_cols(const Ctx& C, const SvdIn& s, long long nn) {
+  return (new_routes(C) && s.need < nn) ? (s.need > 0 ? s.need : 1) : nn;
+}
 // The shared job for a block-route Jacobi (null: the owner's team alone):
 // always with dedicated helper CTAs, otherwise once the queue is drained.
 CATN_HDI inline JacobiJob* block_job(Ctx& C) {
@@ -411,13 +424,41 @@ CATN_HDI inline JacobiJob* block_job(Ctx& C) {
 // parameters select.  Returns jacobi_sweeps' codes.
 CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, long long ld, double* V,
                                double* nrm) {
+  const long long t0 = clk();
+  int sweeps;
   if (use_block(C, n, X)) {
     // precision 1: rotations stop at the rounding level of FP32 products
     const double floor_rel = C.P.precision == 1 ? 4e-7 : 0.0;
-    return jacobi_block(C.T, block_job(C), X, rows, n, ld, V, 60, C.sws, floor_rel, C.P.precision == 1);
+    sweeps = jacobi_block(C.T, block_job(C), X, rows, n, ld, V, 60, C.sws, floor_rel, C.P.precision == 1);
+    prof_add(C, PROF_N_BLOCK, 1.0);
+    prof_add(C, PROF_BLOCK_SWEEPS, (double)sweeps);
+  } else {
+    sweeps = share_jacobi(C, n, X) ? jacobi_sweeps_shared(C.T, C.job, X, rows, n, ld, V, 60, nrm)
+                                   : jacobi_sweeps(C.T, X, rows, n, ld, V, 60, nrm);
   }
-  return share_jacobi(C, n, X) ? jacobi_sweeps_shared(C.T, C.job, X, rows, n, ld, V, 60, nrm)
-                               : jacobi_sweeps(C.T, X, rows, n, ld, V, 60, nrm);
+  if (X != C.sws) {
+    prof_add(C, PROF_LJAC, (double)(clk() - t0));
+    prof_add(C, PROF_LJAC_COLS, (double)n);
+  }
+  return sweeps;
+}
+
+// Split precision: the two-site merge of a large swap (M x N >= 2^18 outputs)
+// as a 3xTF32 tensor-core product (tc_gemm_mop).  Returns false when the
+// caller should take the FP64 GEMM (FP64 mode, small merges, no tensor-core
+// area in this kernel); a tensor-core wait that ran out fails the instance.
+constexpr long long kTcMergeMinElems = 1LL << 18;
+CATN_HDI inline bool merge_on_tc(Ctx& C, long long M, long long N, long long K, const double* A, const double* B,
+                                 const MOp& out) {
+#if CATN_DEVICE_PASS
+  if (C.P.precision != 1 || M * N < kTcMergeMinElems || !tc_ready(C.T)) return false;
+  if (!tc_gemm_mop(C.T, M, N, K, A, M, B, K, out)) fail_all(C, CATN_ETIMEOUT);
+  C.T.sync();
+  return true;
+#else
+  (void)C; (void)M; (void)N; (void)K; (void)A; (void)B; (void)out;
+  return false;
+#endif
 }
 
 // Blocked application of Q: panel width and the smallest m x ncols product
@@ -426,8 +467,8 @@ CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, l
 constexpr long long kQPanel = 32;
 constexpr long long kBlockedQMinElems = 8192;
 // qr_apply_q, shared when large; false when a shared wait ran out.
-CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
-                             double* Cm, long long ncols, long long ldc) {
+CATN_HDI inline bool apply_q_any(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
+                                 double* Cm, long long ncols, long long ldc) {
   if (share_house(C, m, ncols, Cm)) {
     if (qr_apply_q_shared(C.T, C.job, A, m, n, lda, tau, Cm, ncols, ldc)) {
       fail_all(C, CATN_ETIMEOUT);
@@ -450,15 +491,27 @@ CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, 
   qr_apply_q(C.T, A, m, n, lda, tau, Cm, ncols, ldc);
   return true;
 }
+// apply_q_any with its cycles counted (large SVDs).
+CATN_HDI inline bool apply_q(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
+                             double* Cm, long long ncols, long long ldc) {
+  const long long t0 = clk();
+  const bool ok = apply_q_any(C, A, m, n, lda, tau, Cm, ncols, ldc);
+  prof_add(C, PROF_LAPPLY, (double)(clk() - t0));
+  return ok;
+}
 // qrcp_inplace, shared when large; -2 when a shared wait ran out.
 CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long long lda, double* tau, int* piv,
                                double* nrm, double stop_tol) {
+  const long long t0 = clk();
+  long long r;
   if (share_house(C, m, n, A)) {
-    const long long r = qrcp_shared(C.T, C.job, A, m, n, lda, tau, piv, nrm, stop_tol);
+    r = qrcp_shared(C.T, C.job, A, m, n, lda, tau, piv, nrm, stop_tol);
     if (r == -2) fail_all(C, CATN_ETIMEOUT);
-    return r;
+  } else {
+    r = qrcp_inplace(C.T, A, m, n, lda, tau, piv, nrm, stop_tol);
   }
-  return qrcp_inplace(C.T, A, m, n, lda, tau, piv, nrm, stop_tol);
+  if (A != C.sws) prof_add(C, PROF_LQR, (double)(clk() - t0));
+  return r;
 }
 
 // Large input whose pivoted QR W P = Q R stopped at rank r (trailing block
@@ -503,26 +556,27 @@ CATN_HDI inline Svd svd_truncated(Ctx& C, const SvdIn& s, long long r, const dou
   if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X2, r, r, r, sig2, S2, perm2);
-  for (long long e = T.rank(); e < nn * r; e += T.size()) {
+  const long long nv = vec_cols(C, s, r);   // singular vectors formed
+  for (long long e = T.rank(); e < nn * nv; e += T.size()) {
     long long rr, c;
     divmod(e, nn, &rr, &c);
     Uin[e] = (rr < r) ? Vb2[rr + (long long)perm2[c] * r] : 0.0;
   }
-  for (long long e = T.rank(); e < r * r; e += T.size()) {
+  for (long long e = T.rank(); e < r * nv; e += T.size()) {
     long long i, c;
     divmod(e, r, &i, &c);
     double sv = S2[c];
     Vin[(long long)piv2[i] + c * r] = (sv > 0.0) ? X2[i + (long long)perm2[c] * r] / sv : 0.0;
   }
   T.sync();
-  if (!apply_q(C, Tt, nn, r, nn, tau2, Uin, r, nn)) return R;
-  for (long long e = T.rank(); e < mm * r; e += T.size()) {
+  if (!apply_q(C, Tt, nn, r, nn, tau2, Uin, nv, nn)) return R;
+  for (long long e = T.rank(); e < mm * nv; e += T.size()) {
     long long rr, c;
     divmod(e, mm, &rr, &c);
     Uw[e] = (rr < r) ? Vin[rr + c * r] : 0.0;
   }
   T.sync();
-  if (!apply_q(C, s.W, mm, r, mm, tau, Uw, r, mm)) return R;
+  if (!apply_q(C, s.W, mm, r, mm, tau, Uw, nv, mm)) return R;
   prof_add(C, PROF_SVD_LARGE, (double)(clk() - t0));
   prof_add(C, PROF_N_LARGE, 1.0);
   R.p = r;
@@ -626,19 +680,20 @@ CATN_HDI inline Svd svd_finish(Ctx& C, const SvdIn& s) {
   if (sweeps < 0) fail_all(C, sweeps == -2 ? CATN_ETIMEOUT : CATN_ENOCONV);
   if (T.leader() && sweeps > C.ctl[CTL_JACMAX]) C.ctl[CTL_JACMAX] = sweeps;
   sort_columns(T, X, nn, nn, nn, sig, Sout, perm);
-  for (long long e = T.rank(); e < mm * nn; e += T.size()) {
+  const long long nv = vec_cols(C, s, nn);   // singular vectors formed
+  for (long long e = T.rank(); e < mm * nv; e += T.size()) {
     long long r, c;
     divmod(e, mm, &r, &c);
     Ut[e] = (r < nn) ? Vb[r + (long long)perm[c] * nn] : 0.0;
   }
-  for (long long e = T.rank(); e < nn * nn; e += T.size()) {
+  for (long long e = T.rank(); e < nn * nv; e += T.size()) {
     long long i, c;
     divmod(e, nn, &i, &c);
     double sv = Sout[c];
     Vt[(long long)piv[i] + c * nn] = (sv > 0.0) ? X[i + (long long)perm[c] * nn] / sv : 0.0;
   }
   T.sync();
-  if (!apply_q(C, s.W, mm, nn, mm, tau, Ut, nn, mm)) return R;
+  if (!apply_q(C, s.W, mm, nn, mm, tau, Ut, nv, mm)) return R;
   prof_add(C, s.smem ? PROF_SVD_SMALL : PROF_SVD_LARGE, (double)(clk() - t0));
   prof_add(C, s.smem ? PROF_N_SMALL : PROF_N_LARGE, 1.0);
   R.p = nn;
@@ -879,13 +934,15 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   const bool randomized = rsvd_route && C.P.rsvd == 1 && !C.tape && m >= (n < 10LL * C.P.chi ? n : 10LL * C.P.chi);
   SvdIn in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);
   if (failed(C)) return 0.0;
+  in.need = C.P.chi;   // keep_rule and the randomized route keep at most chi
   // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
   // straight into the SVD's oriented input.
   {
     const long long tg = clk();
     MOp out = in.wide ? mop(in.W, imap((int)d0, n, 1), imap((int)d1, n * d0, d2))
                       : mop(in.W, imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2));
-    gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
+    if (!merge_on_tc(C, d0 * d2, d1 * d3, kk, sdata(C, tl), sdata(C, tr), out))
+      gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
     prof_add(C, PROF_SWAP_GEMM, (double)(clk() - tg));
   }
   Svd R = randomized ? rsvd_swap(C, in, m, n, C.P.chi) : svd_finish(C, in);
@@ -1416,6 +1473,7 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   if (failed(C)) return 0.0;
   SvdIn in = svd_begin(C, qi.rrows, qj.rrows, C.P.cutoff);
   if (failed(C)) return 0.0;
+  if (C.P.Dmax > 0) in.need = C.P.Dmax;   // the cut keeps at most Dmax vectors
   gemm(T, qi.rrows, qj.rrows, d, colmajor(qi.Rb, qi.rrows), transposed(qj.Rb, qj.rrows), svd_target(in));
   Svd R = svd_finish(C, in);
   if (failed(C)) return 0.0;

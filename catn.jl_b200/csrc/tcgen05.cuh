@@ -4,11 +4,11 @@
 // mbarrier by tcgen05.commit, results read back with tcgen05.ld.
 //
 // 3xTF32: an FP32 value x is split into hi = x rounded to TF32 (10 explicit
-// mantissa bits) and lo = x - hi (exact in FP32, itself read as TF32 by the
-// tensor core); a product is accumulated as hi_a hi_b + hi_a lo_b + lo_a hi_b
-// in FP32, which keeps about 21-22 bits of each product (the dropped lo_a
-// lo_b term is 2^-22 relative).  Operands arrive here in FP64 and are
-// rounded to FP32 first.
+// mantissa bits) and lo = x - hi rounded to TF32, so x = hi + lo to about
+// 2^-22; a product is accumulated as hi_a hi_b + hi_a lo_b + lo_a hi_b in
+// FP32, which keeps about 21 bits of each product (measured: errors about
+// 3.5e-7 of |A| |B|).  Operands arrive here in FP64 and are rounded to FP32
+// first.
 //
 // Operand layout in shared memory: K-major, no swizzle ("interleave"), the
 // canonical layout whose core matrix is 8 rows x 16 bytes (4 TF32 values of

@@ -120,14 +120,18 @@ typedef struct {
   int64_t arena_peak;  /* device bytes high-water mark                      */
   double flops;        /* algorithmic FLOPs of the contraction (see below)  */
   double bytes;        /* algorithmic bytes: site tensors read + written    */
-  double prof[16];     /* SM cycles: [0] contraction total, [1] tiny SVDs
+  double prof[24];     /* SM cycles: [0] contraction total, [1] tiny SVDs
                           (one warp), [2] small SVDs (shared memory), [3]
                           large SVDs, [4] edge bookkeeping; counts: [5]
                           tiny, [6] small, [7] large SVDs; cycles: [8] swap
                           merge GEMM, [9] swap epilogue, [10] cano step
                           after its SVD, [11] eat folds, [12] merge fuse,
                           [13] Dmax cut (its SVD included), [14] reverse,
-                          [15] loop control (re-pointing, checks)         */
+                          [15] loop control (re-pointing, checks); within
+                          large SVDs: [16] pivoted QR, [17] Jacobi, [18]
+                          application of Q; [19] block-route Jacobis, [20]
+                          their summed sweeps, [21] summed columns of the
+                          large Jacobi factors; [22], [23] reserved       */
 } catn_result;
 /* Algorithmic work convention (per step, FP64 elements of 8 bytes):
  *   swap / compress pair: 2*m*n*k + 4*m*n*r  (m=d0*d1, n=d2*d3, k bond, r kept)
