@@ -27,6 +27,7 @@
 #pragma once
 #include "linalg.cuh"
 #include "blockjac_tc.cuh"
+#include "blockqr.cuh"
 
 namespace catn {
 
@@ -258,9 +259,9 @@ CATN_HDI inline int block_item(const Team& T, double* X, double* V, long long m,
   return 1;
 }
 
-// The team's share of the current round of a JOB_BLOCK job: the leader
-// claims items one at a time for the whole team, which rotates them and
-// reports each done.
+// The team's share of the current round of a JOB_BLOCK or JOB_PANEL job:
+// the leader claims items one at a time for the whole team, which works
+// them (a block pair, or a tile of trailing columns) and reports each done.
 CATN_HDI inline void block_work(const Team& T, JacobiJob* J, double* ws) {
   for (;;) {
     long long item = -1;
@@ -281,10 +282,21 @@ CATN_HDI inline void block_work(const Team& T, JacobiJob* J, double* ws) {
     double* X = (double*)ldcg_u((const unsigned long long*)&J->B);
     double* V = (double*)ldcg_u((const unsigned long long*)&J->V);
     const long long m = ldcg_i(&J->m), n = ldcg_i(&J->n), ld = ldcg_i(&J->ldb), np = ldcg_i(&J->np);
-    const long long r = ldcg_i(&J->round);
-    long long p, q;
-    rr_pair(np, r, item, &p, &q);
-    const int rot = block_item(T, X, V, m, n, ld, p, q, ldcg(&J->tol), ldcg(&J->tk), ws, ldcg_i(&J->tc) != 0);
+    int rot = 0;
+    if (ldcg_i(&J->kind) == JOB_PANEL) {
+      // 32 trailing columns of a blocked QR panel update
+      long long* cols = (long long*)(ws + kPanelWsDoubles);
+      const long long c0 = ldcg_i(&J->c0) + item * kPanelW;
+      for (int c = T.rank(); c < kPanelW; c += T.size()) cols[c] = (c0 + c < n) ? c0 + c : -1;
+      T.sync();
+      panel_item(T, X, m, ld, V, (const double*)ldcg_u((const unsigned long long*)&J->W2), ldcg_i(&J->k), cols,
+                 (double*)ldcg_u((const unsigned long long*)&J->nrm), ws);
+    } else {
+      const long long r = ldcg_i(&J->round);
+      long long p, q;
+      rr_pair(np, r, item, &p, &q);
+      rot = block_item(T, X, V, m, n, ld, p, q, ldcg(&J->tol), ldcg(&J->tk), ws, ldcg_i(&J->tc) != 0);
+    }
     fence_gpu();
     T.sync();
     if (T.leader()) {
@@ -315,6 +327,144 @@ CATN_HDI inline int job_round_cta(const Team& T, JacobiJob* J, unsigned long lon
   T.sync();
   block_work(T, J, ws);
   return job_wait_done(T, J, count);
+}
+
+// Householder QR of A (m x n, m >= n, ld lda) after sorting its columns by
+// norm, largest first: A P = Q R with piv[k] the original index of column
+// k, R in the upper triangle and the reflectors below it (LAPACK geqrf
+// layout, tau), as qrcp_inplace leaves them.  Blocked: each panel of 32
+// reflectors is factored by the team, and the trailing columns are updated
+// in compact WY form, 32 columns per item, shared through J when J is set.
+// Sorting instead of pivoting at every step keeps the columns graded, which
+// is what the one-sided Jacobi on R^T needs (about one more sweep than full
+// pivoting), with one shared round per panel instead of one per column.
+// With stop_tol > 0 the factorisation ends at the first panel boundary k
+// whose trailing block has Frobenius norm <= stop_tol and returns k (every
+// singular value of the dropped block is below stop_tol); otherwise n.
+// -2: a shared wait ran out.  work: m n + 32 m + 2048 doubles.
+CATN_HDI inline long long qr_sorted_blocked(const Team& T, JacobiJob* J, double* A, long long m, long long n,
+                                            long long lda, double* tau, int* piv, double* nrm, double stop_tol,
+                                            double* work, double* ws) {
+  constexpr int B = kPanelW;
+  double* tmp = work;             // m x n
+  double* Vp = tmp + m * n;       // up to m x 32
+  double* G = Vp + m * B;         // 32 x 32
+  double* Nm = G + B * B;         // 32 x 32
+  // column norms and the descending order (stable: ties by index)
+  for (long long j = T.warp(); j < n; j += T.nwarps()) {
+    const double* aj = A + j * lda;
+    double s2 = 0.0;
+    for (long long i = T.lane(); i < m; i += T.wsize()) s2 = fma(aj[i], aj[i], s2);
+    s2 = T.wsum(s2);
+    if (T.lane() == 0) nrm[j] = s2;
+  }
+  T.sync();
+  for (long long j = T.rank(); j < n; j += T.size()) {
+    const double v = nrm[j];
+    long long rk = 0;
+    for (long long i = 0; i < n; ++i) rk += (nrm[i] > v || (nrm[i] == v && i < j)) ? 1 : 0;
+    piv[rk] = (int)j;
+  }
+  T.sync();
+  for (long long e = T.rank(); e < m * n; e += T.size()) {
+    long long i, k;
+    divmod(e, m, &i, &k);
+    tmp[e] = A[i + (long long)piv[k] * lda];
+  }
+  T.sync();
+  for (long long e = T.rank(); e < m * n; e += T.size()) {
+    long long i, k;
+    divmod(e, m, &i, &k);
+    A[i + k * lda] = tmp[e];
+  }
+  for (long long k = T.rank(); k < n; k += T.size()) nrm[k] = 0.0;
+  fence_gpu();
+  T.sync();
+  unsigned long long seq = 0;
+  if (J) {
+    seq = job_open(T, J);
+    if (T.leader()) {
+      J->kind = JOB_PANEL;
+      fence_gpu();
+      J->open = 1;
+      fence_gpu();
+    }
+    T.sync();
+  }
+  long long rank = n;
+  int timed_out = 0;
+  for (long long k0 = 0; k0 < n && !timed_out; k0 += B) {
+    const long long kb = (n - k0 < B) ? n - k0 : B, mp = m - k0;
+    if (stop_tol > 0.0 && k0 > 0) {
+      double rem = 0.0;
+      for (long long j = k0 + T.rank(); j < n; j += T.size()) rem += ldcg(nrm + j);
+      rem = T.sum(rem);
+      if (rem <= stop_tol * stop_tol) {
+        rank = k0;
+        break;
+      }
+    }
+    double* P = A + k0 + k0 * lda;
+    if (J) {   // the panel's columns as the helpers left them, through this SM
+      for (long long e = T.rank(); e < mp * kb; e += T.size()) {
+        long long i, j;
+        divmod(e, mp, &i, &j);
+        P[i + j * lda] = ldcg(P + i + j * lda);
+      }
+      T.sync();
+    }
+    qr_inplace(T, P, mp, kb, lda, tau + k0);
+    if (k0 + kb >= n) break;
+    // compact WY: V explicit (unit diagonal), G = V^T V, Nm = -T
+    for (long long e = T.rank(); e < mp * kb; e += T.size()) {
+      long long i, j;
+      divmod(e, mp, &i, &j);
+      Vp[e] = (i > j) ? P[i + j * lda] : (i == j ? 1.0 : 0.0);
+    }
+    for (long long e = T.rank(); e < kb * kb; e += T.size()) Nm[e] = 0.0;
+    T.sync();
+    gemm(T, kb, kb, mp, transposed(Vp, mp), colmajor(Vp, mp), colmajor(G, kb));
+    for (long long j = 0; j < kb; ++j) {
+      const double tj = tau[k0 + j];
+      for (long long i = T.rank(); i <= j; i += T.size()) {
+        double s2 = 0.0;
+        for (long long l = i; l < j; ++l) s2 = fma(Nm[i + l * kb], G[l + j * kb], s2);
+        Nm[i + j * kb] = -tj * (i == j ? 1.0 : s2);
+      }
+      T.sync();
+    }
+    fence_gpu();
+    T.sync();
+    const long long c_first = k0 + kb;
+    const long long items = (n - c_first + B - 1) / B;
+    if (J) {
+      if (T.leader()) {
+        J->B = A + k0; J->V = Vp; J->W2 = Nm; J->nrm = nrm;
+        J->m = (int)mp; J->n = (int)n; J->ldb = (int)lda; J->k = (int)kb; J->c0 = (int)c_first;
+        fence_gpu();
+      }
+      timed_out = job_round_cta(T, J, seq, items, ws);
+      ++seq;
+    } else {
+      long long* cols = (long long*)(ws + kPanelWsDoubles);
+      for (long long it = 0; it < items; ++it) {
+        for (int c = T.rank(); c < B; c += T.size()) cols[c] = (c_first + it * B + c < n) ? c_first + it * B + c : -1;
+        T.sync();
+        panel_item(T, A + k0, mp, lda, Vp, Nm, (int)kb, cols, nrm, ws);
+      }
+    }
+  }
+  if (J) {
+    job_close(T, J, seq);
+    // every column as the helpers left it, through this SM
+    for (long long e = T.rank(); e < m * n; e += T.size()) {
+      long long i, k;
+      divmod(e, m, &i, &k);
+      A[i + k * lda] = ldcg(A + i + k * lda);
+    }
+  }
+  T.sync();
+  return timed_out ? -2 : rank;
 }
 
 // Block one-sided Jacobi on X (m x n, ld) with V (n x n) accumulated, the
@@ -465,7 +615,8 @@ __device__ inline void help_jobs(const Team& T, JacobiJob* board, int nslots, co
         __nanosleep(32);
         continue;
       }
-      if (ldcg_i(&J->kind) == JOB_BLOCK) {
+      const int kind = ldcg_i(&J->kind);
+      if (kind == JOB_BLOCK || kind == JOB_PANEL) {
         block_work(T, J, ws);
       } else {
         job_work(T, J);

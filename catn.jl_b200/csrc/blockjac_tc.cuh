@@ -106,7 +106,8 @@ __device__ __forceinline__ void tc_finish(const Team& T, unsigned commits, int p
   __syncthreads();
 }
 
-__device__ __forceinline__ bool tc_ready(const Team& T) { return T.tcs && T.tmem && !tc_ctl(T)->broken; }
+// (the TMEM base address may be 0, so the staging area marks the set-up)
+__device__ __forceinline__ bool tc_ready(const Team& T) { return T.tcs && !tc_ctl(T)->broken; }
 
 // G (32 x 32, row-major FP64) = X_P^T X_P over rows [0, m) on the tensor
 // cores.  Returns false when a wait ran out.

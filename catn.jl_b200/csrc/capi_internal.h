@@ -26,6 +26,7 @@ constexpr int kThreads = 256;
 constexpr int kSmemBytes = 100 * 1024;
 constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - catn::GEMM_STAGE_BYTES) / 8;
 static_assert(kSwsDoubles >= catn::kBlockWsDoubles, "block-route items need their workspace in shared memory");
+static_assert(kSwsDoubles >= catn::kPanelWsDoubles + catn::kPanelW, "panel items need their workspace in shared memory");
 // Launches with split-precision instances add the tensor-core staging area
 // (blockjac_tc.cuh) after the small-SVD workspace.
 constexpr int kSmemBytesTc = kSmemBytes + catn::kTcRegionBytes + 1024;

@@ -428,7 +428,7 @@ CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, l
   int sweeps;
   if (use_block(C, n, X)) {
     // precision 1: rotations stop at the rounding level of FP32 products
-    const double floor_rel = C.P.precision == 1 ? 4e-7 : 0.0;
+    const double floor_rel = C.P.precision == 1 ? 1e-8 : 0.0;
     sweeps = jacobi_block(C.T, block_job(C), X, rows, n, ld, V, 60, C.sws, floor_rel, C.P.precision == 1);
     prof_add(C, PROF_N_BLOCK, 1.0);
     prof_add(C, PROF_BLOCK_SWEEPS, (double)sweeps);
@@ -504,7 +504,16 @@ CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long
                                double* nrm, double stop_tol) {
   const long long t0 = clk();
   long long r;
-  if (share_house(C, m, n, A)) {
+  const long long work = m * n + (long long)kPanelW * m + 2048;
+  if (new_routes(C) && n >= C.block_min_n && A != C.sws && 2 * n * n > C.sws_doubles &&
+      C.sp + 8 * work + 4096 <= C.sp_hi) {
+    // the block route's QR: columns sorted by norm, panels of 32 reflectors
+    const long long mark = C.sp;
+    double* w = spush(C, work);
+    r = qr_sorted_blocked(C.T, block_job(C), A, m, n, lda, tau, piv, nrm, stop_tol, w, C.sws);
+    C.sp = mark;
+    if (r == -2) fail_all(C, CATN_ETIMEOUT);
+  } else if (share_house(C, m, n, A)) {
     r = qrcp_shared(C.T, C.job, A, m, n, lda, tau, piv, nrm, stop_tol);
     if (r == -2) fail_all(C, CATN_ETIMEOUT);
   } else {

@@ -649,8 +649,9 @@ CATN_HDI inline int jacobi_sweeps(const Team& T, double* B, long long m, long lo
 // round (B, V, nrm); Householder reflector k applied to 4-column chunks of C
 // from column c0 (reflector in column k of A), with the trailing squared
 // norms recomputed into nrm when nrm is set (pivoted QR); block pairs of the
-// block Jacobi route (blockjac.cuh), claimed by whole CTAs.
-enum { JOB_JACOBI = 0, JOB_HOUSE = 1, JOB_BLOCK = 2 };
+// block Jacobi route (blockjac.cuh) and 32-column tiles of a blocked QR's
+// trailing update (blockqr.cuh), both claimed by whole CTAs.
+enum { JOB_JACOBI = 0, JOB_HOUSE = 1, JOB_BLOCK = 2, JOB_PANEL = 3 };
 constexpr int JOB_CHUNK = 4;   // columns per Householder claim
 struct JacobiJob {
   unsigned long long word;
@@ -658,9 +659,10 @@ struct JacobiJob {
   int kind, m, n, ldb, np, k, c0, ldc;
   int tc, pad;   // block items: products on the tensor cores (split precision)
   double tol, tk;
-  double* B;     // Jacobi columns / Householder reflectors (A)
-  double* V;     // Jacobi rotations / Householder target (C)
+  double* B;     // Jacobi columns / Householder reflectors (A) / panel-update target
+  double* V;     // Jacobi rotations / Householder target (C) / panel reflectors
   double* nrm;
+  double* W2;    // panel update: -T of the compact WY form
 };
 
 // ---------------------------------------------------------------------------
