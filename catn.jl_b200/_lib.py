@@ -36,7 +36,7 @@ class Tuning(ct.Structure):
     """``catn_tuning``: the process-wide launch-shape and route table."""
     _fields_ = [("helper_ctas", ct.c_int32), ("grad_helper_ctas", ct.c_int32),
                 ("shared_jacobi_min_n", ct.c_int32), ("block_min_n", ct.c_int32),
-                ("shared_house_min", ct.c_int64)]
+                ("shared_house_min", ct.c_int64), ("blocked_qr_min_n", ct.c_int32), ("reserved", ct.c_int32)]
 
 
 class Result(ct.Structure):

@@ -419,6 +419,8 @@ CATN_HDI inline void run_instance_grad(const Team& T, char* slot, const SlotLayo
     C.job_min_n = jl->min_n;
     C.job_pool = jl->pool;
     C.job_min_qr = jl->min_qr;
+    C.block_min_n = jl->block_min_n;
+    C.blocked_qr_min_n = jl->blocked_qr_min_n;
   }
   reset_slot(C);
   tape_enable(C, L.arena_bytes);

@@ -219,8 +219,8 @@ CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* ro
 }
 
 // One item: block pair (p, q) of the round.  ws holds kBlockWsDoubles.
-// With `tc` and the CTA's tensor-core area ready, the Gram and the two
-// rotations are 3xTF32 tensor-core products (blockjac_tc.cuh), else FP64.
+// With `tc` and the CTA's tensor-core area ready, the pair's Gram is a 3xTF32
+// tensor-core product (blockjac_tc.cuh), else FP64.
 // Returns 1 when the pair was rotated, 0 when it was left alone, -1 when a
 // wait for the tensor core ran out (same in every thread).
 CATN_HDI inline int block_item(const Team& T, double* X, double* V, long long m, long long n, long long ld,
@@ -246,14 +246,8 @@ CATN_HDI inline int block_item(const Team& T, double* X, double* V, long long m,
 #endif
   if (!block_needs_rotation(T, G, tol, floor_abs)) return 0;
   block_inner(T, G, Q, rot, tol, kBlockInnerSweeps);
-#if CATN_DEVICE_PASS
-  if (on_tc) {
-    tc_load_q(T, Q);
-    if (!tc_rotate(T, X, m, ld, cols)) return -1;
-    if (!tc_rotate(T, V, n, n, cols)) return -1;
-    return 1;
-  }
-#endif
+  // the rotation itself stays FP64: each column is rotated thousands of
+  // times, and 3xTF32 products would leave ~2^-21 of its norm behind each time
   block_rotate(T, X, m, ld, cols, Q);
   block_rotate(T, V, n, n, cols, Q);
   return 1;
@@ -502,6 +496,14 @@ CATN_HDI inline int jacobi_block(const Team& T, JacobiJob* J, double* X, long lo
   const long long npair = nb / 2;
   const double tol = 2.220446049250313e-16 * (double)(m > 16 ? m : 16);
   const double floor_abs = floor_rel > 0.0 ? floor_rel * sqrt(cmax) : 0.0;
+  // With tc the sweeps run in two phases: first the pair Grams on the tensor
+  // cores (3xTF32), the rotation test at their rounding level (relative
+  // 4e-6, floor 4e-7 of the largest column); then FP64 Grams with the FP64
+  // test until a sweep rotates nothing, which certifies the result at the
+  // FP64 level.  The rotations are FP64 in both phases.
+  int phase = tc ? 0 : 1;
+  auto ptol = [&](int ph) { return ph == 0 ? 4e-6 : tol; };
+  auto pfloor = [&](int ph) { return ph == 0 ? 4e-7 * sqrt(cmax) : floor_abs; };
   int result = -1, timed_out = 0;
   unsigned long long seq = 0;
   if (J) {
@@ -509,8 +511,8 @@ CATN_HDI inline int jacobi_block(const Team& T, JacobiJob* J, double* X, long lo
     if (T.leader()) {
       J->kind = JOB_BLOCK;
       J->B = X; J->V = V; J->nrm = nullptr;
-      J->m = (int)m; J->n = (int)n; J->ldb = (int)ld; J->np = (int)nb; J->tol = tol; J->tk = floor_abs;
-      J->tc = tc ? 1 : 0;
+      J->m = (int)m; J->n = (int)n; J->ldb = (int)ld; J->np = (int)nb;
+      J->tol = ptol(phase); J->tk = pfloor(phase); J->tc = phase == 0 ? 1 : 0;
       J->rotated = 0; J->round = 0;
       fence_gpu();
       J->open = 1;
@@ -537,10 +539,19 @@ CATN_HDI inline int jacobi_block(const Team& T, JacobiJob* J, double* X, long lo
         for (long long pi = 0; pi < npair && !timed_out; ++pi) {
           long long p, q;
           rr_pair(nb, r, pi, &p, &q);
-          const int it = block_item(T, X, V, m, n, ld, p, q, tol, floor_abs, ws, tc);
+          const int it = block_item(T, X, V, m, n, ld, p, q, ptol(phase), pfloor(phase), ws, phase == 0);
           if (it > 0) rot = 1;
           if (it < 0) timed_out = 1;
         }
+    }
+    if (!rot && phase == 0) {
+      phase = 1;
+      if (J && T.leader()) {
+        J->tol = ptol(1); J->tk = pfloor(1); J->tc = 0;
+        fence_gpu();
+      }
+      T.sync();
+      continue;
     }
     if (!rot) {
       result = sweep + 1;

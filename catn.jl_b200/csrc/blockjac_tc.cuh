@@ -1,22 +1,21 @@
-// Split-precision (3xTF32, tcgen05) products of the block Jacobi items:
-// the pair Gram G = X_P^T X_P and the pair rotations Y_P <- Y_P Q.
+// Split-precision (3xTF32, tcgen05) products: the pair Gram G = X_P^T X_P
+// of the block Jacobi's first phase, and the two-site merges of large
+// swaps.
 //
-// Both stream the pair's rows through a shared-memory tile that the threads
+// Both stream their operands through a shared-memory tile that the threads
 // fill with TF32 hi / lo parts (K-major, tcgen05.cuh's layout) while one
 // thread issues the MMAs of the previous tile; the global loads of the next
 // tile are issued into registers before the CTA waits for the tensor core,
 // so their latency overlaps the MMAs.
-//   Gram:     D (128 x 32) = A (128 x K) B (K x 32), K = the pair's rows in
-//             chunks of 64; A's rows 0-31 are the pair's columns and rows
-//             32-127 are zero (the MMA's smallest M here is 128), B is A's
-//             first 32 rows.  Accumulates in TMEM over every chunk.
-//   Rotation: D (128 x 32) = Y chunk (128 rows x 32 pair columns) Q, one
-//             chunk of 128 rows at a time, D read back (tcgen05.ld) and
-//             stored in FP64.
-// The staging area (T.tcs, tc_region_bytes) and the CTA's TMEM columns
-// (T.tmem) are set up by the kernel; a wait for the tensor core that runs
-// out marks the area broken (later items take the FP64 products) and the
-// item reports failure.
+//   Gram:  D (128 x 32) = A (128 x K) B (K x 32), K = the pair's rows in
+//          chunks of 64; A's rows 0-31 are the pair's columns and rows
+//          32-127 are zero (the MMA's smallest M here is 128), B is A's
+//          first 32 rows.  Accumulates in TMEM over every chunk.
+//   Merge: tiles of 128 x 128 of C = A B, K in chunks of 32, read back with
+//          tcgen05.ld and stored in FP64 through the caller's operand map.
+// The staging area (T.tcs) and the CTA's TMEM columns (T.tmem) are set up
+// by the kernel; a wait for the tensor core that runs out marks the area
+// broken (later products take the FP64 path) and the caller reports failure.
 #pragma once
 #include "tcgen05.cuh"
 #include "linalg.cuh"
@@ -24,13 +23,11 @@
 namespace catn {
 
 // Layout of the staging area (offsets in bytes from T.tcs, 1024-aligned).
-constexpr int kTcOffAhi = 0;                 // 128 x 64 TF32 (Gram) / 128 x 32 (rotation)
+constexpr int kTcOffAhi = 0;                 // 128 x 64 TF32 (Gram) / two 128 x 32 (merge)
 constexpr int kTcOffAlo = 32 * 1024;
-constexpr int kTcOffQhi = 64 * 1024;         // 32 x 32, K-major
-constexpr int kTcOffQlo = 68 * 1024;
-constexpr int kTcOffCtl = 72 * 1024;         // mbarrier, TMEM slot, counters
-constexpr int kTcRegionBytes = 72 * 1024 + 64;
-constexpr int kTcTmemCols = 128;   // block items use columns 0-31, merges 0-127
+constexpr int kTcOffCtl = 64 * 1024;         // mbarrier, TMEM slot, counters
+constexpr int kTcRegionBytes = 64 * 1024 + 64;
+constexpr int kTcTmemCols = 128;   // Grams use columns 0-31, merges 0-127
 constexpr long long kTcWaitPolls = 1LL << 22;
 
 #if defined(__CUDACC__)
@@ -182,101 +179,6 @@ __device__ inline bool tc_gram(const Team& T, const double* X, long long m, long
   return true;
 }
 
-// The rotation Q (32 x 32 row-major FP64) split into the B operand: B[n][k]
-// = Q[k][n], K-major.
-__device__ inline void tc_load_q(const Team& T, const double* Q) {
-  float* qhi = (float*)(T.tcs + kTcOffQhi);
-  float* qlo = (float*)(T.tcs + kTcOffQlo);
-  for (int e = threadIdx.x; e < 32 * 32; e += 256) {
-    const int k = e >> 5, n = e & 31;
-    float h, l;
-    tc::split_tf32(Q[e], &h, &l);
-    const uint32_t o = tc::kmajor_off(n, k, 32) / 4;
-    qhi[o] = h;
-    qlo[o] = l;
-  }
-  __syncthreads();
-}
-
-// Y_P <- Y_P Q on rows [0, m) on the tensor cores (Q staged by tc_load_q).
-// Returns false when a wait ran out.
-__device__ inline bool tc_rotate(const Team& T, double* Y, long long m, long long ld, const long long* cols) {
-  constexpr int RC = 128;
-  float* ahi = (float*)(T.tcs + kTcOffAhi);
-  float* alo = (float*)(T.tcs + kTcOffAlo);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  unsigned commits = tc_ctl(T)->commits;
-  __syncthreads();
-  const long long nch = (m + RC - 1) / RC;
-  double v[16];
-  auto load = [&](long long c) {
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int e = tid + 256 * j;
-      const int r = e & 127, k = e >> 7;
-      const long long gr = c * RC + r;
-      v[j] = (cols[k] >= 0 && gr < m) ? ldcg(Y + gr + cols[k] * ld) : 0.0;
-    }
-  };
-  auto store = [&](long long c) {
-    if (warp < 4) {
-      float y[32];
-      tc::tmem_ld32(T.tmem + ((uint32_t)(warp * 32) << 16), y);
-      const long long gr = c * RC + warp * 32 + lane;
-      if (gr < m) {
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-          if (cols[j] >= 0) stcg(Y + gr + cols[j] * ld, (double)y[j]);
-      }
-    }
-    tc::fence_before_sync();
-  };
-  load(0);
-  const uint32_t idesc = tc::idesc_tf32(128, 32);
-  const uint32_t sbo = 32 / 4 * 128;
-  const uint32_t a_hi = tc::smem_u32(ahi), a_lo = tc::smem_u32(alo);
-  const uint32_t q_hi = tc::smem_u32(T.tcs + kTcOffQhi), q_lo = tc::smem_u32(T.tcs + kTcOffQlo);
-  for (long long c = 0; c < nch; ++c) {
-    if (c > 0) {
-      if (!tc_wait(T, &commits)) return false;
-      store(c - 1);
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int e = tid + 256 * j;
-      const int r = e & 127, k = e >> 7;
-      float h, l;
-      tc::split_tf32(v[j], &h, &l);
-      const uint32_t o = tc::kmajor_off(r, k, 32) / 4;
-      ahi[o] = h;
-      alo[o] = l;
-    }
-    tc::fence_smem_to_async();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-#pragma unroll
-      for (int s = 0; s < 4; ++s) {
-        const uint32_t off = (uint32_t)s * 2 * tc::kLBO;
-        const uint64_t ah = tc::smem_desc(a_hi + off, tc::kLBO, sbo);
-        const uint64_t al = tc::smem_desc(a_lo + off, tc::kLBO, sbo);
-        const uint64_t bh = tc::smem_desc(q_hi + off, tc::kLBO, sbo);
-        const uint64_t bl = tc::smem_desc(q_lo + off, tc::kLBO, sbo);
-        tc::mma_tf32(T.tmem, ah, bh, idesc, s > 0 ? 1u : 0u);
-        tc::mma_tf32(T.tmem, ah, bl, idesc, 1u);
-        tc::mma_tf32(T.tmem, al, bh, idesc, 1u);
-      }
-      tc_issue_commit(T);
-    }
-    if (c + 1 < nch) load(c + 1);
-  }
-  if (nch > 0) {
-    if (!tc_wait(T, &commits)) return false;
-    store(nch - 1);
-  }
-  tc_finish(T, commits, 0);
-  return true;
-}
 // C (M x N, written through the operand map `out`) = A (M x K, column-major,
 // lda) * B (K x N, column-major, ldb) on the tensor cores, for the large
 // two-site merges of swap! in split precision.  Tiles of 128 x 128 of C, K

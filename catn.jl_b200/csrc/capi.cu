@@ -206,7 +206,7 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
 
 // The tuning table in force (entries < 0: built-in defaults).
 std::mutex g_tuning_mu;
-catn_tuning g_tuning = {-1, -1, -1, -1, -1};
+catn_tuning g_tuning = {-1, -1, -1, -1, -1, -1, 0};
 
 catn_tuning tuning_now() {
   std::lock_guard<std::mutex> lock(g_tuning_mu);
@@ -216,6 +216,7 @@ catn_tuning tuning_now() {
   if (t.shared_jacobi_min_n < 0) t.shared_jacobi_min_n = kSharedJacobiMinN;
   if (t.block_min_n < 0) t.block_min_n = (int32_t)catn::kBlockMinN;
   if (t.shared_house_min < 0) t.shared_house_min = kSharedHouseMinElems;
+  if (t.blocked_qr_min_n < 0) t.blocked_qr_min_n = 1 << 30;
   return t;
 }
 
@@ -232,6 +233,7 @@ void helper_config(const DeviceRun& R, bool grad, JobLink* jl, int* nhelp) {
   jl->pool = h > 0;
   jl->min_qr = std::max(1LL, (long long)t.shared_house_min);
   jl->block_min_n = std::max(4, (int)t.block_min_n);
+  jl->blocked_qr_min_n = std::max(4, (int)t.blocked_qr_min_n);
 }
 
 catn_status upload(DeviceRun& R, cudaStream_t st) {

@@ -111,6 +111,7 @@ struct Ctx {
   int job_pool;        // CTAs of the launch do nothing but help: share from the start
   long long job_min_qr;   // smallest rows x columns whose Householder work is shared
   int block_min_n;     // smallest Jacobi factor (columns) on the block route
+  int blocked_qr_min_n;   // smallest block-route QR (columns) taking the blocked, norm-sorted form
 };
 
 // Where a batch CTA publishes its shared Jacobi sweeps (null: never).
@@ -121,6 +122,7 @@ struct JobLink {
   int pool;   // the launch has dedicated helper CTAs
   long long min_qr;
   int block_min_n;   // smallest Jacobi factor (columns) on the block route
+  int blocked_qr_min_n;
 };
 
 // ---------------------------------------------------------------------------
@@ -158,7 +160,7 @@ CATN_HD long long clk() {
 enum { PROF_TOTAL = 0, PROF_SVD_TINY, PROF_SVD_SMALL, PROF_SVD_LARGE, PROF_BOOK, PROF_N_TINY, PROF_N_SMALL,
        PROF_N_LARGE, PROF_SWAP_GEMM, PROF_SWAP_EPI, PROF_CANO_EPI, PROF_EAT, PROF_MERGE, PROF_CUT, PROF_REVERSE,
        PROF_CONTROL, PROF_LQR, PROF_LJAC, PROF_LAPPLY, PROF_N_BLOCK, PROF_BLOCK_SWEEPS, PROF_LJAC_COLS,
-       PROF_RESERVED1, PROF_RESERVED2, PROF_SLOTS, PROF_COMPACT = PROF_SLOTS, PROF_N_COMPACT = PROF_SLOTS + 1 };
+       PROF_LJAC_BLOCK, PROF_LJAC_BIG, PROF_SLOTS, PROF_COMPACT = PROF_SLOTS, PROF_N_COMPACT = PROF_SLOTS + 1 };
 CATN_HD void prof_add(Ctx& C, int slot, double v) {
   if (C.T.leader()) C.acct[2 + slot] += v;
 }
@@ -437,8 +439,11 @@ CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, l
                                    : jacobi_sweeps(C.T, X, rows, n, ld, V, 60, nrm);
   }
   if (X != C.sws) {
-    prof_add(C, PROF_LJAC, (double)(clk() - t0));
+    const double dt = (double)(clk() - t0);
+    prof_add(C, PROF_LJAC, dt);
     prof_add(C, PROF_LJAC_COLS, (double)n);
+    if (use_block(C, n, X)) prof_add(C, PROF_LJAC_BLOCK, dt);
+    if (n >= 1024) prof_add(C, PROF_LJAC_BIG, dt);
   }
   return sweeps;
 }
@@ -505,9 +510,9 @@ CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long
   const long long t0 = clk();
   long long r;
   const long long work = m * n + (long long)kPanelW * m + 2048;
-  if (new_routes(C) && n >= C.block_min_n && A != C.sws && 2 * n * n > C.sws_doubles &&
+  if (new_routes(C) && n >= C.blocked_qr_min_n && A != C.sws && 2 * n * n > C.sws_doubles &&
       C.sp + 8 * work + 4096 <= C.sp_hi) {
-    // the block route's QR: columns sorted by norm, panels of 32 reflectors
+    // the blocked QR: columns sorted by norm, panels of 32 reflectors
     const long long mark = C.sp;
     double* w = spush(C, work);
     r = qr_sorted_blocked(C.T, block_job(C), A, m, n, lda, tau, piv, nrm, stop_tol, w, C.sws);
@@ -2125,6 +2130,7 @@ CATN_HDI inline Ctx make_ctx(const Team& T, char* slot, const SlotLayout& L, con
   C.job_pool = 0;
   C.job_min_qr = 1LL << 62;
   C.block_min_n = kBlockMinN;
+  C.blocked_qr_min_n = 1 << 30;
   return C;
 }
 
@@ -2236,6 +2242,7 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
     C.job_pool = jl->pool;
     C.job_min_qr = jl->min_qr;
     C.block_min_n = jl->block_min_n;
+    C.blocked_qr_min_n = jl->blocked_qr_min_n;
   }
   reset_slot(C);
   if (D.trace_cap > 0 && trace_base) {

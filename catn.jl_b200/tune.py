@@ -26,7 +26,8 @@ import numpy as np
 from . import _lib as L
 
 TABLE_PATH = L.TUNING_PATH
-FIELDS = ("helper_ctas", "grad_helper_ctas", "shared_jacobi_min_n", "block_min_n", "shared_house_min")
+FIELDS = ("helper_ctas", "grad_helper_ctas", "shared_jacobi_min_n", "block_min_n", "shared_house_min",
+          "blocked_qr_min_n", "reserved")
 
 
 def get():

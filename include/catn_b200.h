@@ -100,6 +100,12 @@ typedef struct {
                                 * with precision 1, and svd_route 2)        */
   int64_t shared_house_min;    /* smallest rows x columns whose Householder
                                 * steps are opened to helper CTAs           */
+  int32_t blocked_qr_min_n;    /* smallest column count whose QR on the
+                                * block route is the blocked, norm-sorted
+                                * one instead of the column-pivoted one
+                                * (default: never; measured slower overall,
+                                * the Jacobi after it needs more sweeps)    */
+  int32_t reserved;
 } catn_tuning;
 catn_status catn_tuning_get(catn_tuning* t);
 catn_status catn_tuning_set(const catn_tuning* t);
@@ -131,7 +137,9 @@ typedef struct {
                           large SVDs: [16] pivoted QR, [17] Jacobi, [18]
                           application of Q; [19] block-route Jacobis, [20]
                           their summed sweeps, [21] summed columns of the
-                          large Jacobi factors; [22], [23] reserved       */
+                          large Jacobi factors; cycles of [22] the
+                          block-route Jacobis, [23] the Jacobis of >= 1024
+                          columns                                         */
 } catn_result;
 /* Algorithmic work convention (per step, FP64 elements of 8 bytes):
  *   swap / compress pair: 2*m*n*k + 4*m*n*r  (m=d0*d1, n=d2*d3, k bond, r kept)

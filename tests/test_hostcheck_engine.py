@@ -262,6 +262,8 @@ def test_block_route_matches_oracle(host, monkeypatch, name, L_, beta, kw, share
     monkeypatch.setenv("CATN_HOSTCHECK_BLOCK_MIN", "16")
     if shared:
         monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
+        # the blocked, norm-sorted QR in place of the pivoted one
+        monkeypatch.setenv("CATN_HOSTCHECK_BLOCKED_QR_MIN", "16")
     e, w, h = _lattice(name, L_)
     st, res, rows = run_ising(host, L_ * L_, e, w, h, beta, svd_route="block", **kw)
     (lz, err, psi), orows, tn = oracle_ising(L_ * L_, e, w, h, beta, **kw)
@@ -280,6 +282,7 @@ def test_block_route_random_regular_graph(host, monkeypatch):
     default block threshold's side of the route."""
     monkeypatch.setenv("CATN_HOSTCHECK_SWS", "0")
     monkeypatch.setenv("CATN_HOSTCHECK_BLOCK_MIN", "80")
+    monkeypatch.setenv("CATN_HOSTCHECK_BLOCKED_QR_MIN", "80")
     monkeypatch.setenv("CATN_HOSTCHECK_JOB", "1")
     r = np.random.default_rng(110)
     e = X.random_regular_graph(110, 3, r)
