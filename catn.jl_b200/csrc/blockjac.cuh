@@ -67,13 +67,27 @@ CATN_HDI inline void block_gram(const Team& T, const double* X, long long m, lon
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (long long r0 = 0; r0 < m; r0 += 64) {
-    for (int e = tid; e < kBlockK * 64; e += 256) {
+  // the next chunk's 8 values per thread are loaded into registers while
+  // the current one is multiplied
+  double v[8];
+  auto load = [&](long long r0) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = tid + 256 * j;
       const int c = e >> 6, r = e & 63;
       const long long col = cols[c];
-      S[c * 65 + r] = (col >= 0 && r0 + r < m) ? ldcg(X + (r0 + r) + col * ld) : 0.0;
+      v[j] = (col >= 0 && r0 + r < m) ? ldcg(X + (r0 + r) + col * ld) : 0.0;
+    }
+  };
+  load(0);
+  for (long long r0 = 0; r0 < m; r0 += 64) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int e = tid + 256 * j;
+      S[(e >> 6) * 65 + (e & 63)] = v[j];
     }
     __syncthreads();
+    if (r0 + 64 < m) load(r0 + 64);
     for (int r = grp; r < 64; r += 4) {
       double a[4], b[4];
 #pragma unroll
@@ -171,8 +185,73 @@ CATN_HDI inline bool block_needs_rotation(const Team& T, const double* G, double
 // order (kBlockK / 2 disjoint rotations per step); Q accumulates them from
 // the identity.  The rotation of (p, q) is jacobi_rotation's, as in the
 // scalar route: columns p', q' = c p - s q, s p + c q.
-CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* rot, double tol, int sweeps) {
+// On the GPU one warp does it in shared memory, G and Q padded to 33 columns
+// (`pad` holds 2 x 32 x 33 doubles), with warp barriers only: the CTA-wide
+// barriers of three passes per step made this the slowest part of an item.
+CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* rot, double tol, int sweeps,
+                                 double* pad) {
   constexpr int K = kBlockK, H = kBlockK / 2;
+#if CATN_DEVICE_PASS
+  constexpr int P = K + 1;
+  double* Gp = pad;
+  double* Qp = pad + K * P;
+  for (int e = T.rank(); e < K * K; e += T.size()) {
+    const int i = e / K, j = e - i * K;
+    Gp[i * P + j] = G[e];
+    Qp[i * P + j] = (i == j) ? 1.0 : 0.0;
+  }
+  T.sync();
+  if (T.warp() == 0) {
+    const int l = T.lane();
+    for (int sw = 0; sw < sweeps; ++sw) {
+      for (int r = 0; r < K - 1; ++r) {
+        if (l < H) {
+          long long p, q;
+          rr_pair(K, r, l, &p, &q);
+          double c = 1.0, sn = 0.0;
+          const bool on = jacobi_rotation(Gp[p * P + p], Gp[q * P + q], Gp[p * P + q], tol, &c, &sn);
+          rot[3 * l] = on ? c : 1.0;
+          rot[3 * l + 1] = on ? sn : 0.0;
+          rot[3 * l + 2] = on ? 1.0 : 0.0;
+        }
+        __syncwarp();
+        // columns of G and of Q: lane l owns row l
+        for (int pi = 0; pi < H; ++pi) {
+          if (rot[3 * pi + 2] == 0.0) continue;
+          long long p, q;
+          rr_pair(K, r, pi, &p, &q);
+          const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+          const double gp = Gp[l * P + p], gq = Gp[l * P + q];
+          Gp[l * P + p] = c * gp - sn * gq;
+          Gp[l * P + q] = sn * gp + c * gq;
+          const double qp = Qp[l * P + p], qq = Qp[l * P + q];
+          Qp[l * P + p] = c * qp - sn * qq;
+          Qp[l * P + q] = sn * qp + c * qq;
+        }
+        __syncwarp();
+        // rows of G: lane l owns column l
+        for (int pi = 0; pi < H; ++pi) {
+          if (rot[3 * pi + 2] == 0.0) continue;
+          long long p, q;
+          rr_pair(K, r, pi, &p, &q);
+          const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+          const double gp = Gp[p * P + l], gq = Gp[q * P + l];
+          Gp[p * P + l] = c * gp - sn * gq;
+          Gp[q * P + l] = sn * gp + c * gq;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  T.sync();
+  for (int e = T.rank(); e < K * K; e += T.size()) {
+    const int i = e / K, j = e - i * K;
+    G[e] = Gp[i * P + j];
+    Q[e] = Qp[i * P + j];
+  }
+  T.sync();
+#else
+  (void)pad;
   for (int e = T.rank(); e < K * K; e += T.size()) Q[e] = (e / K == e % K) ? 1.0 : 0.0;
   T.sync();
   for (int sw = 0; sw < sweeps; ++sw) {
@@ -216,6 +295,7 @@ CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* ro
       T.sync();
     }
   }
+#endif
 }
 
 // One item: block pair (p, q) of the round.  ws holds kBlockWsDoubles.
@@ -245,7 +325,7 @@ CATN_HDI inline int block_item(const Team& T, double* X, double* V, long long m,
   block_gram(T, X, m, ld, cols, G, part);
 #endif
   if (!block_needs_rotation(T, G, tol, floor_abs)) return 0;
-  block_inner(T, G, Q, rot, tol, kBlockInnerSweeps);
+  block_inner(T, G, Q, rot, tol, kBlockInnerSweeps, part);
   // the rotation itself stays FP64: each column is rotated thousands of
   // times, and 3xTF32 products would leave ~2^-21 of its norm behind each time
   block_rotate(T, X, m, ld, cols, Q);
