@@ -183,116 +183,128 @@ CATN_HDI inline bool block_needs_rotation(const Team& T, const double* G, double
 
 // Cyclic Jacobi sweeps on the symmetric G (k x k, row-major) in parallel
 // order (kBlockK / 2 disjoint rotations per step); Q accumulates them from
-// the identity.  The rotation of (p, q) is jacobi_rotation's, as in the
-// scalar route: columns p', q' = c p - s q, s p + c q.
-// On the GPU one warp does it in shared memory, G and Q padded to 33 columns
-// (`pad` holds 2 x 32 x 33 doubles), with warp barriers only: the CTA-wide
-// barriers of three passes per step made this the slowest part of an item.
+// the identity.  The rotation of (p, q), p < q, is jacobi_rotation's, as in
+// the scalar route: columns p', q' = c p - s q, s p + c q.
+// On the GPU one warp does it with G and Q in registers, lane l holding row
+// l of each: steps pair column j with j ^ m (m = 1 .. 31, every pair once per
+// sweep, the same parallel ordering as the one-warp tiny SVD), so that every
+// index is a compile-time constant; the row update exchanges rows with the
+// partner lane by shuffles.  The CTA-wide barriers of the earlier
+// shared-memory form made this core the slowest part of an item.
+#if CATN_DEVICE_PASS
+__device__ __forceinline__ double lane_pick(const double* a, int idx) {
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < 32; ++k)
+    if (k == idx) v = a[k];
+  return v;
+}
+template <int M>
+__device__ __forceinline__ void inner_xor_steps(double* g, double* qv, int l, double tol) {
+  const unsigned FULL = 0xffffffffu;
+  const int pl = l ^ M;
+  const bool lo = l < pl;
+  const double d = lane_pick(g, l);
+  const double dp = __shfl_xor_sync(FULL, d, M);
+  const double apq = lane_pick(g, pl);
+  double c = 1.0, sn = 0.0;
+  if (!jacobi_rotation(lo ? d : dp, lo ? dp : d, apq, tol, &c, &sn)) {
+    c = 1.0;
+    sn = 0.0;
+  }
+  // both lanes of a pair use the lower lane's rotation
+  const double cx = __shfl_xor_sync(FULL, c, M), sx = __shfl_xor_sync(FULL, sn, M);
+  if (!lo) {
+    c = cx;
+    sn = sx;
+  }
+  // columns (k, k ^ M) of this lane's rows of G and Q
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const int kk = k ^ M;
+    if (k < kk) {
+      const double ck = __shfl_sync(FULL, c, k), sk = __shfl_sync(FULL, sn, k);
+      const double gp = g[k], gq = g[kk];
+      g[k] = ck * gp - sk * gq;
+      g[kk] = sk * gp + ck * gq;
+      const double qp = qv[k], qq = qv[kk];
+      qv[k] = ck * qp - sk * qq;
+      qv[kk] = sk * qp + ck * qq;
+    }
+  }
+  // rows l and l ^ M of G
+#pragma unroll
+  for (int k = 0; k < 32; ++k) {
+    const double o = __shfl_xor_sync(FULL, g[k], M);
+    g[k] = lo ? (c * g[k] - sn * o) : (sn * o + c * g[k]);
+  }
+  if constexpr (M < 31) inner_xor_steps<M + 1>(g, qv, l, tol);
+}
+#endif
+
 CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* rot, double tol, int sweeps,
                                  double* pad) {
   constexpr int K = kBlockK, H = kBlockK / 2;
+  static_assert(K == 32, "the one-warp core holds one row per lane");
 #if CATN_DEVICE_PASS
-  constexpr int P = K + 1;
-  double* Gp = pad;
-  double* Qp = pad + K * P;
-  for (int e = T.rank(); e < K * K; e += T.size()) {
-    const int i = e / K, j = e - i * K;
-    Gp[i * P + j] = G[e];
-    Qp[i * P + j] = (i == j) ? 1.0 : 0.0;
-  }
-  T.sync();
+  (void)pad; (void)rot; (void)H;
   if (T.warp() == 0) {
     const int l = T.lane();
-    for (int sw = 0; sw < sweeps; ++sw) {
-      for (int r = 0; r < K - 1; ++r) {
-        if (l < H) {
-          long long p, q;
-          rr_pair(K, r, l, &p, &q);
-          double c = 1.0, sn = 0.0;
-          const bool on = jacobi_rotation(Gp[p * P + p], Gp[q * P + q], Gp[p * P + q], tol, &c, &sn);
-          rot[3 * l] = on ? c : 1.0;
-          rot[3 * l + 1] = on ? sn : 0.0;
-          rot[3 * l + 2] = on ? 1.0 : 0.0;
-        }
-        __syncwarp();
-        // columns of G and of Q: lane l owns row l
-        for (int pi = 0; pi < H; ++pi) {
-          if (rot[3 * pi + 2] == 0.0) continue;
-          long long p, q;
-          rr_pair(K, r, pi, &p, &q);
-          const double c = rot[3 * pi], sn = rot[3 * pi + 1];
-          const double gp = Gp[l * P + p], gq = Gp[l * P + q];
-          Gp[l * P + p] = c * gp - sn * gq;
-          Gp[l * P + q] = sn * gp + c * gq;
-          const double qp = Qp[l * P + p], qq = Qp[l * P + q];
-          Qp[l * P + p] = c * qp - sn * qq;
-          Qp[l * P + q] = sn * qp + c * qq;
-        }
-        __syncwarp();
-        // rows of G: lane l owns column l
-        for (int pi = 0; pi < H; ++pi) {
-          if (rot[3 * pi + 2] == 0.0) continue;
-          long long p, q;
-          rr_pair(K, r, pi, &p, &q);
-          const double c = rot[3 * pi], sn = rot[3 * pi + 1];
-          const double gp = Gp[p * P + l], gq = Gp[q * P + l];
-          Gp[p * P + l] = c * gp - sn * gq;
-          Gp[q * P + l] = sn * gp + c * gq;
-        }
-        __syncwarp();
-      }
+    double g[32], qv[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      g[k] = G[l * K + k];
+      qv[k] = (k == l) ? 1.0 : 0.0;
+    }
+    for (int sw = 0; sw < sweeps; ++sw) inner_xor_steps<1>(g, qv, l, tol);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      G[l * K + k] = g[k];
+      Q[l * K + k] = qv[k];
     }
   }
   T.sync();
-  for (int e = T.rank(); e < K * K; e += T.size()) {
-    const int i = e / K, j = e - i * K;
-    G[e] = Gp[i * P + j];
-    Q[e] = Qp[i * P + j];
-  }
-  T.sync();
 #else
-  (void)pad;
-  for (int e = T.rank(); e < K * K; e += T.size()) Q[e] = (e / K == e % K) ? 1.0 : 0.0;
-  T.sync();
+  // the host build: the same xor-ordered steps, one rotation after another
+  (void)pad; (void)T;
+  for (int e = 0; e < K * K; ++e) Q[e] = (e / K == e % K) ? 1.0 : 0.0;
   for (int sw = 0; sw < sweeps; ++sw) {
-    for (int r = 0; r < K - 1; ++r) {
-      for (int pi = T.rank(); pi < H; pi += T.size()) {
-        long long p, q;
-        rr_pair(K, r, pi, &p, &q);
-        double c = 1.0, s = 0.0;
-        const bool on = jacobi_rotation(G[p * K + p], G[q * K + q], G[p * K + q], tol, &c, &s);
-        rot[3 * pi] = on ? c : 1.0;
-        rot[3 * pi + 1] = on ? s : 0.0;
-        rot[3 * pi + 2] = on ? 1.0 : 0.0;
+    for (int m = 1; m < K; ++m) {
+      int np = 0;
+      for (int k = 0; k < K; ++k) {   // parameters from the state at the step's start
+        const int kk = k ^ m;
+        if (k > kk) continue;
+        double c = 1.0, sn = 0.0;
+        if (!jacobi_rotation(G[k * K + k], G[kk * K + kk], G[k * K + kk], tol, &c, &sn)) {
+          c = 1.0;
+          sn = 0.0;
+        }
+        rot[3 * np] = c;
+        rot[3 * np + 1] = sn;
+        rot[3 * np + 2] = (double)k;
+        ++np;
       }
-      T.sync();
-      // columns of G and of Q
-      for (int e = T.rank(); e < H * K; e += T.size()) {
-        const int pi = e / K, i = e - pi * K;
-        if (rot[3 * pi + 2] == 0.0) continue;
-        long long p, q;
-        rr_pair(K, r, pi, &p, &q);
-        const double c = rot[3 * pi], s = rot[3 * pi + 1];
-        const double gp = G[i * K + p], gq = G[i * K + q];
-        G[i * K + p] = c * gp - s * gq;
-        G[i * K + q] = s * gp + c * gq;
-        const double qp = Q[i * K + p], qq = Q[i * K + q];
-        Q[i * K + p] = c * qp - s * qq;
-        Q[i * K + q] = s * qp + c * qq;
+      for (int pi = 0; pi < H; ++pi) {   // columns of G and Q
+        const int k = (int)rot[3 * pi + 2], kk = k ^ m;
+        const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+        for (int i = 0; i < K; ++i) {
+          const double gp = G[i * K + k], gq = G[i * K + kk];
+          G[i * K + k] = c * gp - sn * gq;
+          G[i * K + kk] = sn * gp + c * gq;
+          const double qp = Q[i * K + k], qq = Q[i * K + kk];
+          Q[i * K + k] = c * qp - sn * qq;
+          Q[i * K + kk] = sn * qp + c * qq;
+        }
       }
-      T.sync();
-      // rows of G
-      for (int e = T.rank(); e < H * K; e += T.size()) {
-        const int pi = e / K, j = e - pi * K;
-        if (rot[3 * pi + 2] == 0.0) continue;
-        long long p, q;
-        rr_pair(K, r, pi, &p, &q);
-        const double c = rot[3 * pi], s = rot[3 * pi + 1];
-        const double gp = G[p * K + j], gq = G[q * K + j];
-        G[p * K + j] = c * gp - s * gq;
-        G[q * K + j] = s * gp + c * gq;
+      for (int pi = 0; pi < H; ++pi) {   // rows of G
+        const int k = (int)rot[3 * pi + 2], kk = k ^ m;
+        const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+        for (int j = 0; j < K; ++j) {
+          const double gp = G[k * K + j], gq = G[kk * K + j];
+          G[k * K + j] = c * gp - sn * gq;
+          G[kk * K + j] = sn * gp + c * gq;
+        }
       }
-      T.sync();
     }
   }
 #endif
