@@ -186,11 +186,23 @@ CATN_HDI inline bool block_needs_rotation(const Team& T, const double* G, double
 // the identity.  The rotation of (p, q), p < q, is jacobi_rotation's, as in
 // the scalar route: columns p', q' = c p - s q, s p + c q.
 // On the GPU one warp does it with G and Q in registers, lane l holding row
-// l of each: steps pair column j with j ^ m (m = 1 .. 31, every pair once per
-// sweep, the same parallel ordering as the one-warp tiny SVD), so that every
-// index is a compile-time constant; the row update exchanges rows with the
-// partner lane by shuffles.  The CTA-wide barriers of the earlier
-// shared-memory form made this core the slowest part of an item.
+// l of each.  The round-robin order is kept with the players moving instead
+// of the pairing: every step rotates the fixed neighbour pairs (2k, 2k+1),
+// then moves each row and column one place round the circle (position 0
+// fixed, the others shifted), so that after 31 steps every pair has met once
+// and the layout is back where it started.  Every register index is then a
+// compile-time constant and the step's code is the same for every step (the
+// xor-paired form needed 31 unrolled copies, which overflowed the instruction
+// cache), and rows cross lanes by shuffles only.
+CATN_HD constexpr int rr_circ_of_phys(int x) { return (x & 1) ? 31 - (x >> 1) : (x >> 1); }
+CATN_HD constexpr int rr_phys_of_circ(int c) { return c < 16 ? 2 * c : 2 * (31 - c) + 1; }
+// physical place of the element at x after one step, and the place it came from
+CATN_HD constexpr int rr_next(int x) {
+  return rr_phys_of_circ(rr_circ_of_phys(x) == 0 ? 0 : (rr_circ_of_phys(x) == 31 ? 1 : rr_circ_of_phys(x) + 1));
+}
+CATN_HD constexpr int rr_prev(int x) {
+  return rr_phys_of_circ(rr_circ_of_phys(x) == 0 ? 0 : (rr_circ_of_phys(x) == 1 ? 31 : rr_circ_of_phys(x) - 1));
+}
 #if CATN_DEVICE_PASS
 __device__ __forceinline__ double lane_pick(const double* a, int idx) {
   double v = 0.0;
@@ -199,46 +211,53 @@ __device__ __forceinline__ double lane_pick(const double* a, int idx) {
     if (k == idx) v = a[k];
   return v;
 }
-template <int M>
-__device__ __forceinline__ void inner_xor_steps(double* g, double* qv, int l, double tol) {
+__device__ __forceinline__ void inner_circle_step(double* g, double* qv, int l, double tol) {
   const unsigned FULL = 0xffffffffu;
-  const int pl = l ^ M;
-  const bool lo = l < pl;
+  const bool lo = (l & 1) == 0;
   const double d = lane_pick(g, l);
-  const double dp = __shfl_xor_sync(FULL, d, M);
-  const double apq = lane_pick(g, pl);
+  const double dp = __shfl_xor_sync(FULL, d, 1);
+  const double apq = lane_pick(g, l ^ 1);
   double c = 1.0, sn = 0.0;
   if (!jacobi_rotation(lo ? d : dp, lo ? dp : d, apq, tol, &c, &sn)) {
     c = 1.0;
     sn = 0.0;
   }
-  // both lanes of a pair use the lower lane's rotation
-  const double cx = __shfl_xor_sync(FULL, c, M), sx = __shfl_xor_sync(FULL, sn, M);
+  // both lanes of a pair use the even lane's rotation
+  const double cx = __shfl_xor_sync(FULL, c, 1), sx = __shfl_xor_sync(FULL, sn, 1);
   if (!lo) {
     c = cx;
     sn = sx;
   }
-  // columns (k, k ^ M) of this lane's rows of G and Q
+  // columns (2k, 2k+1) of this lane's rows of G and Q
 #pragma unroll
-  for (int k = 0; k < 32; ++k) {
-    const int kk = k ^ M;
-    if (k < kk) {
-      const double ck = __shfl_sync(FULL, c, k), sk = __shfl_sync(FULL, sn, k);
-      const double gp = g[k], gq = g[kk];
-      g[k] = ck * gp - sk * gq;
-      g[kk] = sk * gp + ck * gq;
-      const double qp = qv[k], qq = qv[kk];
-      qv[k] = ck * qp - sk * qq;
-      qv[kk] = sk * qp + ck * qq;
-    }
+  for (int k = 0; k < 16; ++k) {
+    const double ck = __shfl_sync(FULL, c, 2 * k), sk = __shfl_sync(FULL, sn, 2 * k);
+    const double gp = g[2 * k], gq = g[2 * k + 1];
+    g[2 * k] = ck * gp - sk * gq;
+    g[2 * k + 1] = sk * gp + ck * gq;
+    const double qp = qv[2 * k], qq = qv[2 * k + 1];
+    qv[2 * k] = ck * qp - sk * qq;
+    qv[2 * k + 1] = sk * qp + ck * qq;
   }
-  // rows l and l ^ M of G
+  // rows 2k and 2k+1 of G
 #pragma unroll
   for (int k = 0; k < 32; ++k) {
-    const double o = __shfl_xor_sync(FULL, g[k], M);
+    const double o = __shfl_xor_sync(FULL, g[k], 1);
     g[k] = lo ? (c * g[k] - sn * o) : (sn * o + c * g[k]);
   }
-  if constexpr (M < 31) inner_xor_steps<M + 1>(g, qv, l, tol);
+  // move every column of G and Q, and every row of G, one place on
+  double tg[32], tq[32];
+#pragma unroll
+  for (int x = 0; x < 32; ++x) {
+    tg[rr_next(x)] = g[x];
+    tq[rr_next(x)] = qv[x];
+  }
+  const int src = rr_prev(l);
+#pragma unroll
+  for (int x = 0; x < 32; ++x) {
+    g[x] = __shfl_sync(FULL, tg[x], src);
+    qv[x] = tq[x];
+  }
 }
 #endif
 
@@ -256,7 +275,10 @@ CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* ro
       g[k] = G[l * K + k];
       qv[k] = (k == l) ? 1.0 : 0.0;
     }
-    for (int sw = 0; sw < sweeps; ++sw) inner_xor_steps<1>(g, qv, l, tol);
+    for (int sw = 0; sw < sweeps; ++sw) {
+#pragma unroll 1
+      for (int r = 0; r < K - 1; ++r) inner_circle_step(g, qv, l, tol);
+    }
 #pragma unroll
     for (int k = 0; k < 32; ++k) {
       G[l * K + k] = g[k];
@@ -265,46 +287,47 @@ CATN_HDI inline void block_inner(const Team& T, double* G, double* Q, double* ro
   }
   T.sync();
 #else
-  // the host build: the same xor-ordered steps, one rotation after another
+  // the host build: the same pairs in the same order, tracked through the
+  // original indices instead of moving rows and columns
   (void)pad; (void)T;
+  int at[K], nat[K];
+  for (int x = 0; x < K; ++x) at[x] = x;
   for (int e = 0; e < K * K; ++e) Q[e] = (e / K == e % K) ? 1.0 : 0.0;
   for (int sw = 0; sw < sweeps; ++sw) {
-    for (int m = 1; m < K; ++m) {
-      int np = 0;
-      for (int k = 0; k < K; ++k) {   // parameters from the state at the step's start
-        const int kk = k ^ m;
-        if (k > kk) continue;
+    for (int r = 0; r < K - 1; ++r) {
+      for (int k = 0; k < H; ++k) {   // parameters from the state at the step's start
+        const int p = at[2 * k], q = at[2 * k + 1];
         double c = 1.0, sn = 0.0;
-        if (!jacobi_rotation(G[k * K + k], G[kk * K + kk], G[k * K + kk], tol, &c, &sn)) {
+        if (!jacobi_rotation(G[p * K + p], G[q * K + q], G[p * K + q], tol, &c, &sn)) {
           c = 1.0;
           sn = 0.0;
         }
-        rot[3 * np] = c;
-        rot[3 * np + 1] = sn;
-        rot[3 * np + 2] = (double)k;
-        ++np;
+        rot[3 * k] = c;
+        rot[3 * k + 1] = sn;
       }
-      for (int pi = 0; pi < H; ++pi) {   // columns of G and Q
-        const int k = (int)rot[3 * pi + 2], kk = k ^ m;
-        const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+      for (int k = 0; k < H; ++k) {   // columns of G and Q
+        const int p = at[2 * k], q = at[2 * k + 1];
+        const double c = rot[3 * k], sn = rot[3 * k + 1];
         for (int i = 0; i < K; ++i) {
-          const double gp = G[i * K + k], gq = G[i * K + kk];
-          G[i * K + k] = c * gp - sn * gq;
-          G[i * K + kk] = sn * gp + c * gq;
-          const double qp = Q[i * K + k], qq = Q[i * K + kk];
-          Q[i * K + k] = c * qp - sn * qq;
-          Q[i * K + kk] = sn * qp + c * qq;
+          const double gp = G[i * K + p], gq = G[i * K + q];
+          G[i * K + p] = c * gp - sn * gq;
+          G[i * K + q] = sn * gp + c * gq;
+          const double qp = Q[i * K + p], qq = Q[i * K + q];
+          Q[i * K + p] = c * qp - sn * qq;
+          Q[i * K + q] = sn * qp + c * qq;
         }
       }
-      for (int pi = 0; pi < H; ++pi) {   // rows of G
-        const int k = (int)rot[3 * pi + 2], kk = k ^ m;
-        const double c = rot[3 * pi], sn = rot[3 * pi + 1];
+      for (int k = 0; k < H; ++k) {   // rows of G
+        const int p = at[2 * k], q = at[2 * k + 1];
+        const double c = rot[3 * k], sn = rot[3 * k + 1];
         for (int j = 0; j < K; ++j) {
-          const double gp = G[k * K + j], gq = G[kk * K + j];
-          G[k * K + j] = c * gp - sn * gq;
-          G[kk * K + j] = sn * gp + c * gq;
+          const double gp = G[p * K + j], gq = G[q * K + j];
+          G[p * K + j] = c * gp - sn * gq;
+          G[q * K + j] = sn * gp + c * gq;
         }
       }
+      for (int x = 0; x < K; ++x) nat[rr_next(x)] = at[x];
+      for (int x = 0; x < K; ++x) at[x] = nat[x];
     }
   }
 #endif

@@ -1876,157 +1876,173 @@ struct ContractOut {
   int maxdim, nsteps;
 };
 
-CATN_HDI inline ContractOut contract(Ctx& C) {
-  const Team& T = C.T;
+// Loop state of contraction! between steps (contract_begin / _step / _end).
+struct LoopState {
   ContractOut O;
-  O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
-  const bool buckets = (C.P.select == 0 || C.P.select == 1);
+  int maxdim, buckets, step_cap;
+};
+
+// select_edge_init! and the loop state before the first step.
+CATN_HDI inline void contract_begin(Ctx& C, LoopState& S) {
+  const Team& T = C.T;
+  S.O.lnZ = 0.0; S.O.err = 0.0; S.O.psi = 1.0; S.O.sign = 1.0; S.O.maxdim = -1; S.O.nsteps = 0;
+  S.buckets = (C.P.select == 0 || C.P.select == 1);
   if (C.tape && C.P.compress) fail_all(C, CATN_EINVAL);   // no adjoint of the compress sweeps
-  if (buckets) {
+  if (S.buckets) {
     // select_edge_init!: all node ids
     for (int k = 1 + T.rank(); k <= C.n; k += T.size()) C.list[k - 1] = k;
     T.sync();
     count_add_nodes_team(C, C.list, C.n);
   }
-  int maxdim = -1;
+  S.maxdim = -1;
   // Every step clears one node, so a network of n nodes needs fewer than n
   // steps; the cap only guards against corrupted state.
-  const int step_cap = C.n + 16;
-  for (;;) {
-    const long long tc0 = clk();
-    const bool more = !failed(C) && has_real_edges(C);
-    prof_add(C, PROF_CONTROL, (double)(clk() - tc0));
-    if (!more) break;
-    if (O.nsteps > step_cap) {
-      fail_all(C, CATN_ESTATE);
-      break;
-    }
-    // --- select ---
-    const long long tb0 = clk();
-    const long long pk = select_team(C, &maxdim);
-    if (failed(C)) break;
-    int i = (int)(pk >> 32), j = (int)(pk & 0xffffffff);
-    if (C.node[j].nsites > C.node[i].nsites) { int t = i; i = j; j = t; }
-    // --- bookkeeping before any shape change ---
-    if (buckets) {
-      int* list = C.list;
-      const int nl = 2 + C.node[i].nnbr + C.node[j].nnbr;
-      T.sync();
-      if (T.leader()) {
-        int q = 0;
-        list[q++] = i;
-        list[q++] = j;
-        for (int p = 1; p <= C.node[i].nnbr; ++p) list[q++] = nbref(C, i, p);
-        for (int p = 1; p <= C.node[j].nnbr; ++p) list[q++] = nbref(C, j, p);
-      }
-      T.sync();
-      count_remove_nodes_team(C, list, nl);
-      // every node whose sites this step may change: i, j and their neighbours
-      for (int q = T.rank(); q < nl; q += T.size())
-        if (list[q] > 0) C.ldv[list[q]] = 0;
-      T.sync();
-    }
-    prof_add(C, PROF_BOOK, (double)(clk() - tb0));
-    int idx_j_in_i = nb_find(C, i, j);
-    int idx_i_in_j = nb_find(C, j, i);
-    int rev = 0;
-    if (C.P.reverse) {
-      int li = C.node[i].nnbr, lj = C.node[j].nnbr;
-      if (idx_j_in_i < (li + 1) / 2) {
-        reverse_node(C, i);
-        idx_j_in_i = nb_find(C, i, j);
-        rev |= 1;
-      }
-      if (idx_i_in_j >= (lj + 1) / 2) {
-        reverse_node(C, j);
-        idx_i_in_j = nb_find(C, j, i);
-        rev |= 2;
-      }
-    }
-    if (failed(C)) break;
-    // snapshot of j's neighbours (after any reverse)
-    int* neigh_j = C.tmp;
-    int* dup = C.tmp + C.maxs;
-    const int lnj = C.node[j].nnbr;
-    T.sync();
-    if (T.leader())
-      for (int p = 1; p <= lnj; ++p) neigh_j[p - 1] = nbref(C, j, p);
-    T.sync();
-    int nd = 0;
-    unsigned duph = 2166136261u;
-    for (int l = 1; l <= lnj && !failed(C); ++l) {
-      if (l == idx_i_in_j) continue;
-      int k = neigh_j[l - 1];
-      if (k <= 0) continue;
-      int idx_k_in_i = nb_find(C, i, k);
-      int idx_i_in_k = nb_find(C, k, i);
-      int idx_j_in_k = nb_find(C, k, j);
-      if (idx_j_in_k == 0) { fail_all(C, CATN_ESTATE); break; }
-      T.sync();
-      if (T.leader()) {
-        nb_delete_at_leader(C, k, idx_j_in_k);
-        nb_insert_at_leader(C, k, idx_j_in_k, i);
-      }
-      refresh_status(C);
-      if (failed(C)) break;
-      if (idx_k_in_i > 0) {
-        T.sync();
-        if (T.leader()) dup[nd] = k;
-        T.sync();
-        ++nd;
-        duph = fnv_step(duph, k);
-        bool cross = idx_i_in_k > idx_j_in_k;
-        O.err += merge_dup(C, k, i, cross);
-      }
-    }
-    if (failed(C)) break;
-    // --- eat! ---
-    double lnv = eat(C, i, j, idx_j_in_i, idx_i_in_j, &O.err, &O.psi);
-    O.lnZ += lnv;
-    if (failed(C)) break;
-    // --- duplicates: merge into i, then cut ---
-    for (int q = 0; q < nd && !failed(C); ++q) {
-      int k = dup[q];
-      merge_dup(C, i, k, false);   // its error is not accumulated (tensor_network.jl:662)
-      int idx_k_in_i = nb_find(C, i, k);
-      if (failed(C)) break;
-      if (C.P.cut_bond || (C.P.Dmax > 0 && sref(C, i, idx_k_in_i).d > C.P.Dmax))
-        O.err += cut_bond(C, i, idx_k_in_i);
-    }
-    if (failed(C)) break;
-    clear_node(C, j);
-    if (C.P.compress) compress_node(C, i, C.P.svdopt != 0);   // error discarded (:688-694)
-    if (failed(C)) break;
-    if (buckets) {
-      const long long tb1 = clk();
-      int* list = C.list;
-      const int nl = 1 + C.node[i].nnbr;
-      T.sync();
-      if (T.leader()) {
-        list[0] = i;
-        for (int p = 1; p <= C.node[i].nnbr; ++p) list[p] = nbref(C, i, p);
-      }
-      T.sync();
-      count_add_nodes_team(C, list, nl);
-      prof_add(C, PROF_BOOK, (double)(clk() - tb1));
-    }
-    const int nsi = C.node[i].nsites;
-    unsigned shh = 2166136261u;
-    for (int p = 1; p <= nsi; ++p) {
-      int d = sref(C, i, p).d;
-      if (d > maxdim) maxdim = d;
-      shh = fnv_step(shh, d);
-    }
-    if (C.trace && O.nsteps < C.trace_cap) {
-      T.sync();
-      if (T.leader()) {
-        int* r = C.trace + 8LL * O.nsteps;
-        r[0] = i; r[1] = j; r[2] = rev; r[3] = nd; r[4] = (int)duph; r[5] = nsi; r[6] = (int)shh; r[7] = maxdim;
-      }
-      T.sync();
-    }
-    O.nsteps += 1;
+  S.step_cap = C.n + 16;
+}
+
+// One step of the main loop (tensor_network.jl:574-707); false when no real
+// edge is left or the instance failed.
+CATN_HDI inline bool contract_step(Ctx& C, LoopState& S) {
+  const Team& T = C.T;
+  const long long tc0 = clk();
+  const bool more = !failed(C) && has_real_edges(C);
+  prof_add(C, PROF_CONTROL, (double)(clk() - tc0));
+  if (!more) return false;
+  if (S.O.nsteps > S.step_cap) {
+    fail_all(C, CATN_ESTATE);
+    return false;
   }
+  // --- select ---
+  const long long tb0 = clk();
+  const long long pk = select_team(C, &S.maxdim);
+  if (failed(C)) return false;
+  int i = (int)(pk >> 32), j = (int)(pk & 0xffffffff);
+  if (C.node[j].nsites > C.node[i].nsites) { int t = i; i = j; j = t; }
+  // --- bookkeeping before any shape change ---
+  if (S.buckets) {
+    int* list = C.list;
+    const int nl = 2 + C.node[i].nnbr + C.node[j].nnbr;
+    T.sync();
+    if (T.leader()) {
+      int q = 0;
+      list[q++] = i;
+      list[q++] = j;
+      for (int p = 1; p <= C.node[i].nnbr; ++p) list[q++] = nbref(C, i, p);
+      for (int p = 1; p <= C.node[j].nnbr; ++p) list[q++] = nbref(C, j, p);
+    }
+    T.sync();
+    count_remove_nodes_team(C, list, nl);
+    // every node whose sites this step may change: i, j and their neighbours
+    for (int q = T.rank(); q < nl; q += T.size())
+      if (list[q] > 0) C.ldv[list[q]] = 0;
+    T.sync();
+  }
+  prof_add(C, PROF_BOOK, (double)(clk() - tb0));
+  int idx_j_in_i = nb_find(C, i, j);
+  int idx_i_in_j = nb_find(C, j, i);
+  int rev = 0;
+  if (C.P.reverse) {
+    int li = C.node[i].nnbr, lj = C.node[j].nnbr;
+    if (idx_j_in_i < (li + 1) / 2) {
+      reverse_node(C, i);
+      idx_j_in_i = nb_find(C, i, j);
+      rev |= 1;
+    }
+    if (idx_i_in_j >= (lj + 1) / 2) {
+      reverse_node(C, j);
+      idx_i_in_j = nb_find(C, j, i);
+      rev |= 2;
+    }
+  }
+  if (failed(C)) return false;
+  // snapshot of j's neighbours (after any reverse)
+  int* neigh_j = C.tmp;
+  int* dup = C.tmp + C.maxs;
+  const int lnj = C.node[j].nnbr;
+  T.sync();
+  if (T.leader())
+    for (int p = 1; p <= lnj; ++p) neigh_j[p - 1] = nbref(C, j, p);
+  T.sync();
+  int nd = 0;
+  unsigned duph = 2166136261u;
+  for (int l = 1; l <= lnj && !failed(C); ++l) {
+    if (l == idx_i_in_j) continue;
+    int k = neigh_j[l - 1];
+    if (k <= 0) continue;
+    int idx_k_in_i = nb_find(C, i, k);
+    int idx_i_in_k = nb_find(C, k, i);
+    int idx_j_in_k = nb_find(C, k, j);
+    if (idx_j_in_k == 0) { fail_all(C, CATN_ESTATE); break; }
+    T.sync();
+    if (T.leader()) {
+      nb_delete_at_leader(C, k, idx_j_in_k);
+      nb_insert_at_leader(C, k, idx_j_in_k, i);
+    }
+    refresh_status(C);
+    if (failed(C)) break;
+    if (idx_k_in_i > 0) {
+      T.sync();
+      if (T.leader()) dup[nd] = k;
+      T.sync();
+      ++nd;
+      duph = fnv_step(duph, k);
+      bool cross = idx_i_in_k > idx_j_in_k;
+      S.O.err += merge_dup(C, k, i, cross);
+    }
+  }
+  if (failed(C)) return false;
+  // --- eat! ---
+  double lnv = eat(C, i, j, idx_j_in_i, idx_i_in_j, &S.O.err, &S.O.psi);
+  S.O.lnZ += lnv;
+  if (failed(C)) return false;
+  // --- duplicates: merge into i, then cut ---
+  for (int q = 0; q < nd && !failed(C); ++q) {
+    int k = dup[q];
+    merge_dup(C, i, k, false);   // its error is not accumulated (tensor_network.jl:662)
+    int idx_k_in_i = nb_find(C, i, k);
+    if (failed(C)) break;
+    if (C.P.cut_bond || (C.P.Dmax > 0 && sref(C, i, idx_k_in_i).d > C.P.Dmax))
+      S.O.err += cut_bond(C, i, idx_k_in_i);
+  }
+  if (failed(C)) return false;
+  clear_node(C, j);
+  if (C.P.compress) compress_node(C, i, C.P.svdopt != 0);   // error discarded (:688-694)
+  if (failed(C)) return false;
+  if (S.buckets) {
+    const long long tb1 = clk();
+    int* list = C.list;
+    const int nl = 1 + C.node[i].nnbr;
+    T.sync();
+    if (T.leader()) {
+      list[0] = i;
+      for (int p = 1; p <= C.node[i].nnbr; ++p) list[p] = nbref(C, i, p);
+    }
+    T.sync();
+    count_add_nodes_team(C, list, nl);
+    prof_add(C, PROF_BOOK, (double)(clk() - tb1));
+  }
+  const int nsi = C.node[i].nsites;
+  unsigned shh = 2166136261u;
+  for (int p = 1; p <= nsi; ++p) {
+    int d = sref(C, i, p).d;
+    if (d > S.maxdim) S.maxdim = d;
+    shh = fnv_step(shh, d);
+  }
+  if (C.trace && S.O.nsteps < C.trace_cap) {
+    T.sync();
+    if (T.leader()) {
+      int* r = C.trace + 8LL * S.O.nsteps;
+      r[0] = i; r[1] = j; r[2] = rev; r[3] = nd; r[4] = (int)duph; r[5] = nsi; r[6] = (int)shh; r[7] = S.maxdim;
+    }
+    T.sync();
+  }
+  S.O.nsteps += 1;
+  return true;
+}
+
+// network_lognorm (tensor_network.jl:489-501) and the outputs.
+CATN_HDI inline void contract_end(Ctx& C, LoopState& S) {
+  const Team& T = C.T;
   // --- network_lognorm (tensor_network.jl:489-501) ---
   double lsum = 0.0, nneg = 0.0, nzero = 0.0, bad = 0.0;
   for (int k = 1 + T.rank(); k <= C.n; k += T.size()) {
@@ -2063,10 +2079,18 @@ CATN_HDI inline ContractOut contract(Ctx& C) {
   nzero = T.sum(nzero);
   bad = T.sum(bad);
   if (bad > 0.5) fail_all(C, CATN_ESTATE);
-  O.lnZ += lsum;
-  O.sign = nzero > 0.5 ? 0.0 : (((long long)(nneg + 0.5)) % 2 ? -1.0 : 1.0);
-  O.maxdim = maxdim;
-  return O;
+  S.O.lnZ += lsum;
+  S.O.sign = nzero > 0.5 ? 0.0 : (((long long)(nneg + 0.5)) % 2 ? -1.0 : 1.0);
+  S.O.maxdim = S.maxdim;
+}
+
+CATN_HDI inline ContractOut contract(Ctx& C) {
+  LoopState S;
+  contract_begin(C, S);
+  while (contract_step(C, S)) {
+  }
+  contract_end(C, S);
+  return S.O;
 }
 
 // ---------------------------------------------------------------------------

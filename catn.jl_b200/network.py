@@ -171,3 +171,19 @@ def result_tensor(tn):
     L.check(lib, lib.catn_result_tensor(tn._dev.handle, L.ptr(out), out.size, ct.byref(numel), ct.byref(nd),
                                         L.ptr(dims)))
     return out.reshape(tuple(int(d) for d in dims[: nd.value]), order="F")
+
+
+def tc_matmul(A, B):
+    """``A @ B`` of two FP64 matrices on the tensor cores in the
+    split-precision form (catn_tc_matmul: TF32 hi/lo parts, three tcgen05
+    products per pair, FP32 accumulation; about 1e-6 of |A| |B|)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    if A.ndim != 2 or B.ndim != 2 or A.shape[1] != B.shape[0]:
+        raise ValueError("tc_matmul: shapes do not match")
+    M, K = A.shape
+    N = B.shape[1]
+    C = np.zeros((M, N), dtype=np.float64, order="F")
+    lib = L.load()
+    L.check(lib, lib.catn_tc_matmul(M, N, K, L.ptr(A), L.ptr(B), L.ptr(C)))
+    return C
