@@ -29,7 +29,8 @@ class Params(ct.Structure):
                 ("norm_method", ct.c_int32), ("select", ct.c_int32), ("reverse", ct.c_int32),
                 ("svdopt", ct.c_int32), ("swapopt", ct.c_int32), ("compress", ct.c_int32),
                 ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32), ("rsvd", ct.c_int32),
-                ("rsvd_min_dim", ct.c_int32), ("precision", ct.c_int32), ("svd_route", ct.c_int32)]
+                ("rsvd_min_dim", ct.c_int32), ("precision", ct.c_int32), ("svd_route", ct.c_int32),
+                ("ckpt_interval", ct.c_int32)]
 
 
 class Tuning(ct.Structure):
@@ -152,12 +153,14 @@ SVD_ROUTES = {"auto": 0, "scalar": 1, "block": 2}
 
 def make_params(Dmax=32, chi=32, cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True,
                 swapopt=True, compress=False, cut_bond=False, seed=1, trace=False, rsvd=0, rsvd_min_dim=0,
-                precision="fp64", svd_route="auto"):
+                precision="fp64", svd_route="auto", ckpt_interval=0):
     """``catn_params`` from the reference's keywords plus the engine's own:
     ``rsvd`` / ``rsvd_min_dim`` (randomized swap route), ``precision``
-    ("fp64" or "split") and ``svd_route`` ("auto", "scalar", "block")."""
+    ("fp64" or "split"), ``svd_route`` ("auto", "scalar", "block") and
+    ``ckpt_interval`` (gradient runs: steps between checkpoints, 0 = whole
+    tape)."""
     prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     route = SVD_ROUTES[svd_route] if isinstance(svd_route, str) else int(svd_route)
     return Params(int(Dmax), int(chi), float(cutoff), int(norm_method), int(select), int(bool(reverse)),
                   int(bool(svdopt)), int(bool(swapopt)), int(bool(compress)), int(bool(cut_bond)),
-                  int(seed), int(bool(trace)), int(rsvd), int(rsvd_min_dim), prec, route)
+                  int(seed), int(bool(trace)), int(rsvd), int(rsvd_min_dim), prec, route, int(ckpt_interval))

@@ -353,15 +353,17 @@ CATN_HDI inline void bwd_logz(Ctx& C, const TapeRec& r) {
   T.sync();
 }
 
-// Walk the tape backwards from d lnZ = 1.
-CATN_HDI inline void backward(Ctx& C) {
+// Zero the shadow of every heap byte written so far.
+CATN_HDI inline void shadow_zero(Ctx& C) {
   const Team& T = C.T;
-  {
-    double* g = gptr(C, C.h_lo0);
-    const long long len = (C.hb - C.h_lo0) / 8;
-    for (long long e = T.rank(); e < len; e += T.size()) g[e] = 0.0;
-    T.sync();
-  }
+  double* g = gptr(C, C.h_lo0);
+  const long long len = (C.hb - C.h_lo0) / 8;
+  for (long long e = T.rank(); e < len; e += T.size()) g[e] = 0.0;
+  T.sync();
+}
+
+// Walk the records last to first, accumulating into the shadow heap.
+CATN_HDI inline void backward_walk(Ctx& C) {
   for (long long q = C.nrec - 1; q >= 0 && !failed(C); --q) {
     const TapeRec r = C.rec[q];
     const long long mark = C.sp;
@@ -381,6 +383,308 @@ CATN_HDI inline void backward(Ctx& C) {
     }
     C.sp = mark;
   }
+}
+
+// Walk the whole tape backwards from d lnZ = 1.
+CATN_HDI inline void backward(Ctx& C) {
+  shadow_zero(C);
+  backward_walk(C);
+}
+
+// ---------------------------------------------------------------------------
+// Checkpointed gradient runs (ckpt_interval K > 0)
+// ---------------------------------------------------------------------------
+// The forward pass runs in segments of K steps, each from a packed state: the
+// live sites laid out contiguously from the working heap's first byte in node
+// / position order (the layout load_instance writes), together with the
+// slot's graph bookkeeping and the loop state.  Before a segment runs, that
+// state is saved in the checkpoint store; the segment then runs with the tape
+// on, and its end state is packed for the next one.  The backward pass takes
+// the segments last to first.  The last one's records are still in place;
+// every earlier one is restored from its checkpoint and recomputed with the
+// tape on, i.e. the same arithmetic on the same layout, so the values and
+// records are bit-identical to the forward pass.  The shadow of its end
+// state's live sites is seeded with the gradient carried back from the next
+// segment, its records are walked, and the gradient of its packed start state
+// becomes the carry for the segment before (written over that checkpoint's
+// own site data, which is not needed again).  Every site gradient
+// accumulates the same contributions in the same order as on the whole tape,
+// so the result equals the ckpt_interval = 0 run bit for bit.  Memory: the
+// scratch stack, one segment's records, the append-only heap of one segment
+// and its shadow, and one checkpoint (bookkeeping + live sites) per K steps.
+struct CkptHdr {
+  LoopState S;
+  long long prev;         // store offset of the checkpoint before (-1: none)
+  long long meta_bytes;   // bookkeeping (below)
+  long long data_bytes;   // packed live sites
+  long long sp;
+  int rsvd_calls, pad;
+};
+
+// Where the slot's bookkeeping lives.  A checkpoint keeps the node headers,
+// the edge entries and their free stack, the control words, the logdim
+// cache, the site references and neighbour lists of each node up to its
+// counts, and the edge map as one flag per entry (the (n+1)^2 map holds
+// either -1 or the id of an alive entry of that pair, so the flags "entry e
+// is the one mapped" rebuild it exactly); the per-step scratch lists and the
+// work counters are not saved.
+struct CkptStore {
+  long long lo, top, hi;   // byte offsets in the arena
+  long long last;          // offset of the newest checkpoint (-1: none)
+  long long nodes;         // slot bytes [0, nodes): node headers
+  long long ent0, ent1;    // slot bytes [ent0, ent1): edge entries and free stack
+  long long ctl0, ctl1;    // slot bytes [ctl0, ctl1): control words
+  long long ldc0, ldc1;    // slot bytes [ldc0, ldc1): logdim cache
+};
+
+CATN_HD long long ckpt_hdr_bytes() { return al256((long long)sizeof(CkptHdr)); }
+CATN_HD long long ckpt_fixed_bytes(const Ctx& C, const CkptStore& K) {
+  return al256(K.nodes) + al256(K.ent1 - K.ent0) + al256(K.ctl1 - K.ctl0) + al256(K.ldc1 - K.ldc0) +
+         al256(4LL * C.ecap);
+}
+CATN_HD double* ckpt_data(const Ctx& C, long long at) {
+  const CkptHdr* h = (const CkptHdr*)(C.base + at);
+  return (double*)(C.base + at + ckpt_hdr_bytes() + h->meta_bytes);
+}
+
+// Arena of a checkpointed gradient run: scratch 20 %, records 2 %, the
+// checkpoint store 40 %, then the append-only heap of one segment and its
+// shadow (19 % each).  Call after make_ctx and before load_instance.
+CATN_HDI inline void tape_enable_ckpt(Ctx& C, const SlotLayout& L, long long arena_bytes, CkptStore& K) {
+  const long long cap = arena_bytes & ~255LL;
+  const long long sc = (cap / 5) & ~255LL;
+  const long long rb = (cap / 50) & ~255LL;
+  const long long st = (cap * 2 / 5) & ~255LL;
+  const long long H = ((cap - sc - rb - st) / 2) & ~255LL;
+  C.sp_lo = 0;
+  C.sp = 0;
+  C.sp_hi = sc;
+  C.sp_peak = 0;
+  C.rec = (TapeRec*)(C.base + sc);
+  C.rcap = rb / (long long)sizeof(TapeRec);
+  C.nrec = 0;
+  K.lo = K.top = sc + rb;
+  K.hi = sc + rb + st;
+  K.last = -1;
+  K.nodes = L.off_site - L.off_node;
+  K.ent0 = L.off_ent - L.off_node;
+  K.ent1 = L.off_emap - L.off_node;
+  K.ctl0 = L.off_ctl - L.off_node;
+  K.ctl1 = L.off_pairs - L.off_node;
+  K.ldc0 = L.off_ldc - L.off_node;
+  K.ldc1 = L.off_arena - L.off_node;
+  C.h_lo0 = C.h_lo1 = K.hi;
+  C.hsize = H;
+  C.half = 0;
+  C.hb = C.h_lo0;
+  C.he = C.h_lo0 + H;
+  C.h_peak = 0;
+  C.gshift = H;
+  C.tape = 1;
+}
+
+// Team copy of `bytes` (a multiple of 8, both ends 8-byte aligned).
+CATN_HDI inline void copy_bytes(const Team& T, char* dst, const char* src, long long bytes) {
+  long long* d = (long long*)dst;
+  const long long* s = (const long long*)src;
+  for (long long e = T.rank(); e < bytes / 8; e += T.size()) d[e] = s[e];
+}
+
+// Copy each node's site references and neighbour entries (up to its counts)
+// between the slot and a packed area (`save`: slot -> packed).  Every thread
+// walks the node counts alike; thread r moves the nodes k = r + 1 (mod team).
+CATN_HDI inline void ckpt_lists(Ctx& C, SiteRef* ps, int* pn, bool save) {
+  const Team& T = C.T;
+  long long os = 0, on = 0;
+  for (int k = 1; k <= C.n; ++k) {
+    const int ns = C.node[k].nsites, nn = C.node[k].nnbr;
+    if ((k - 1) % T.size() == T.rank()) {
+      for (int p = 1; p <= ns; ++p) {
+        if (save) ps[os + p - 1] = sref(C, k, p);
+        else sref(C, k, p) = ps[os + p - 1];
+      }
+      for (int p = 1; p <= nn; ++p) {
+        if (save) pn[on + p - 1] = nbref(C, k, p);
+        else nbref(C, k, p) = pn[on + p - 1];
+      }
+    }
+    os += ns;
+    on += nn;
+  }
+}
+
+// Save the current state as a new checkpoint: the live sites packed into the
+// store, their references rewritten to the packed layout at the heap's first
+// byte, then the bookkeeping and the loop state.  The working heap is
+// reloaded from the packed copy (the next segment starts from it).
+CATN_HDI inline void ckpt_save(Ctx& C, CkptStore& K, const LoopState& S) {
+  const Team& T = C.T;
+  long long data = 0, nsite = 0, nnbr = 0;
+  for (int k = 1; k <= C.n; ++k) {
+    for (int p = 1; p <= C.node[k].nsites; ++p) data += al256(sbytes(sref(C, k, p)));
+    nsite += C.node[k].nsites;
+    nnbr += C.node[k].nnbr;
+  }
+  const long long meta = ckpt_fixed_bytes(C, K) + al256(nsite * (long long)sizeof(SiteRef)) + al256(4 * nnbr);
+  const long long need = ckpt_hdr_bytes() + meta + data;
+  if (K.top + need > K.hi || data > C.hsize) {
+    fail_all(C, CATN_ENOMEM);
+    return;
+  }
+  const long long at = K.top;
+  char* m = C.base + at + ckpt_hdr_bytes();
+  double* dst = (double*)(m + meta);
+  T.sync();
+  long long cur = 0;
+  for (int k = 1; k <= C.n; ++k)
+    for (int p = 1; p <= C.node[k].nsites; ++p) {
+      const SiteRef s = sref(C, k, p);
+      const long long sz = (long long)s.dl * s.d * s.dr;
+      const double* src = dptr(C, s.off);
+      for (long long e = T.rank(); e < sz; e += T.size()) dst[cur / 8 + e] = src[e];
+      cur += al256(8 * sz);
+    }
+  T.sync();
+  if (T.leader()) {
+    long long c2 = C.h_lo0;
+    for (int k = 1; k <= C.n; ++k)
+      for (int p = 1; p <= C.node[k].nsites; ++p) {
+        SiteRef& s = sref(C, k, p);
+        s.off = c2;
+        c2 += al256(sbytes(s));
+      }
+    CkptHdr h;
+    h.S = S;
+    h.prev = K.last;
+    h.meta_bytes = meta;
+    h.data_bytes = data;
+    h.sp = C.sp;
+    h.rsvd_calls = C.rsvd_calls;
+    h.pad = 0;
+    *(CkptHdr*)(C.base + at) = h;
+  }
+  T.sync();
+  const char* slot = (const char*)C.node;
+  copy_bytes(T, m, slot, K.nodes);
+  m += al256(K.nodes);
+  copy_bytes(T, m, slot + K.ent0, K.ent1 - K.ent0);
+  m += al256(K.ent1 - K.ent0);
+  copy_bytes(T, m, slot + K.ctl0, K.ctl1 - K.ctl0);
+  m += al256(K.ctl1 - K.ctl0);
+  copy_bytes(T, m, slot + K.ldc0, K.ldc1 - K.ldc0);
+  m += al256(K.ldc1 - K.ldc0);
+  int* flag = (int*)m;
+  for (long long e = T.rank(); e < C.ecap; e += T.size()) {
+    const EdgeEnt E = C.ent[e];
+    flag[e] = (E.alive && emap_at(C, E.i, E.j) == (int)e) ? 1 : 0;
+  }
+  m += al256(4LL * C.ecap);
+  ckpt_lists(C, (SiteRef*)m, (int*)(m + al256(nsite * (long long)sizeof(SiteRef))), true);
+  copy_bytes(T, C.base + C.h_lo0, (const char*)dst, data);
+  T.sync();
+  K.last = at;
+  K.top += need;
+  C.hb = C.h_lo0 + data;
+  C.nrec = 0;
+}
+
+// Restore checkpoint `at` (bookkeeping, packed sites, loop state) into the
+// slot and the working heap; the tape restarts empty.
+CATN_HDI inline void ckpt_restore(Ctx& C, const CkptStore& K, long long at, LoopState& S) {
+  const Team& T = C.T;
+  T.sync();
+  const CkptHdr h = *(const CkptHdr*)(C.base + at);
+  char* slot = (char*)C.node;
+  const char* m = C.base + at + ckpt_hdr_bytes();
+  copy_bytes(T, slot, m, K.nodes);
+  m += al256(K.nodes);
+  copy_bytes(T, slot + K.ent0, m, K.ent1 - K.ent0);
+  m += al256(K.ent1 - K.ent0);
+  copy_bytes(T, slot + K.ctl0, m, K.ctl1 - K.ctl0);
+  m += al256(K.ctl1 - K.ctl0);
+  copy_bytes(T, slot + K.ldc0, m, K.ldc1 - K.ldc0);
+  m += al256(K.ldc1 - K.ldc0);
+  const int* flag = (const int*)m;
+  m += al256(4LL * C.ecap);
+  const long long nn = (long long)C.n + 1;
+  for (long long e = T.rank(); e < nn * nn; e += T.size()) C.emap[e] = -1;
+  T.sync();   // node counts and entries in place before the lists and the map
+  for (long long e = T.rank(); e < C.ecap; e += T.size())
+    if (flag[e]) emap_at(C, C.ent[e].i, C.ent[e].j) = (int)e;
+  long long nsite = 0;
+  for (int k = 1; k <= C.n; ++k) nsite += C.node[k].nsites;
+  ckpt_lists(C, (SiteRef*)m, (int*)(m + al256(nsite * (long long)sizeof(SiteRef))), false);
+  copy_bytes(T, C.base + C.h_lo0, (const char*)ckpt_data(C, at), h.data_bytes);
+  T.sync();
+  S = h.S;
+  C.hb = C.h_lo0 + h.data_bytes;
+  C.sp = h.sp;
+  C.rsvd_calls = h.rsvd_calls;
+  C.nrec = 0;
+}
+
+// Seed the shadow of the live sites (node / position order) from `carry`,
+// the gradient of the same sites packed as in a checkpoint.
+CATN_HDI inline void ckpt_seed(Ctx& C, const double* carry) {
+  const Team& T = C.T;
+  long long cur = 0;
+  for (int k = 1; k <= C.n; ++k)
+    for (int p = 1; p <= C.node[k].nsites; ++p) {
+      const SiteRef s = sref(C, k, p);
+      const long long sz = (long long)s.dl * s.d * s.dr;
+      double* g = gptr(C, s.off);
+      for (long long e = T.rank(); e < sz; e += T.size()) g[e] = carry[cur / 8 + e];
+      cur += al256(8 * sz);
+    }
+  T.sync();
+}
+
+// Forward pass in segments of K steps, then the backward pass segment by
+// segment.  Returns the forward outputs; the gradients of the loaded sites
+// are left in the shadow of the heap's first bytes (the load layout).
+CATN_HDI inline ContractOut contract_grad_ckpt(Ctx& C, CkptStore& K, int interval) {
+  const Team& T = C.T;
+  LoopState S;
+  contract_begin(C, S);
+  if (!failed(C)) ckpt_save(C, K, S);
+  while (!failed(C)) {
+    int steps = 0;
+    bool more = true;
+    while (steps < interval && (more = contract_step(C, S))) ++steps;
+    if (failed(C)) break;
+    if (!more) {
+      contract_end(C, S);
+      break;
+    }
+    ckpt_save(C, K, S);
+  }
+  const ContractOut O = S.O;
+  if (failed(C)) return O;
+  const int jacmax = C.ctl[CTL_JACMAX];
+  // the last segment's records and heap are in place
+  shadow_zero(C);
+  backward_walk(C);
+  long long at = K.last;
+  while (!failed(C)) {
+    const CkptHdr h = *(const CkptHdr*)(C.base + at);
+    if (h.prev < 0) break;   // the first checkpoint: the load layout
+    // the gradient of this segment's start state is the carry for the one before
+    double* carry = ckpt_data(C, at);
+    copy_bytes(T, (char*)carry, (const char*)gptr(C, C.h_lo0), h.data_bytes);
+    T.sync();
+    ckpt_restore(C, K, h.prev, S);
+    for (int q = 0; q < interval && !failed(C); ++q)
+      if (!contract_step(C, S) && !failed(C)) fail_all(C, CATN_ESTATE);   // the recomputation must retrace
+    if (failed(C)) break;
+    shadow_zero(C);
+    ckpt_seed(C, carry);
+    backward_walk(C);
+    at = h.prev;
+  }
+  T.sync();
+  if (T.leader() && C.ctl[CTL_JACMAX] < jacmax) C.ctl[CTL_JACMAX] = jacmax;
+  T.sync();
+  return O;
 }
 
 // Gradients of the sites loaded from the image (MPS form), written in the
@@ -423,15 +727,25 @@ CATN_HDI inline void run_instance_grad(const Team& T, char* slot, const SlotLayo
     C.blocked_qr_min_n = jl->blocked_qr_min_n;
   }
   reset_slot(C);
-  tape_enable(C, L.arena_bytes);
+  const int interval = D.P.ckpt_interval;
+  CkptStore K;
+  if (interval > 0)
+    tape_enable_ckpt(C, L, L.arena_bytes, K);
+  else
+    tape_enable(C, L.arena_bytes);
   if (D.kind != 0) fail_all(C, CATN_EINVAL);   // gradients of MPS-form inputs only
   if (!failed(C)) load_instance(C, D, i64, i32, dat);
   ContractOut O;
   O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
   const long long t0 = clk();
-  if (!failed(C)) O = contract(C);
-  prof_add(C, PROF_TOTAL, (double)(clk() - t0));
-  if (!failed(C)) backward(C);
+  if (!failed(C) && interval > 0) {
+    O = contract_grad_ckpt(C, K, interval);   // forward, recomputation and backward
+    prof_add(C, PROF_TOTAL, (double)(clk() - t0));
+  } else if (!failed(C)) {
+    O = contract(C);
+    prof_add(C, PROF_TOTAL, (double)(clk() - t0));
+    if (!failed(C)) backward(C);
+  }
   if (!failed(C)) site_gradients_out(C, D, i64, gimg);
   T.sync();
   if (T.leader()) {

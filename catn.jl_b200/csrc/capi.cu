@@ -57,6 +57,7 @@ catn_status check_params(const catn_params* p) {
   if (p->rsvd_min_dim < 0) return fail(CATN_EINVAL, "rsvd_min_dim must be >= 0");
   if (p->precision < 0 || p->precision > 1) return fail(CATN_EINVAL, "precision must be 0 (FP64) or 1 (split)");
   if (p->svd_route < 0 || p->svd_route > 2) return fail(CATN_EINVAL, "svd_route must be 0, 1 or 2");
+  if (p->ckpt_interval < 0) return fail(CATN_EINVAL, "ckpt_interval must be >= 0");
   return CATN_OK;
 }
 
@@ -370,6 +371,7 @@ void catn_params_default(catn_params* p) {
   p->rsvd_min_dim = 0;
   p->precision = 0;
   p->svd_route = 0;
+  p->ckpt_interval = 0;
 }
 
 catn_status catn_tuning_get(catn_tuning* t) {

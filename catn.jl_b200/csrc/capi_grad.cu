@@ -151,12 +151,12 @@ catn_status catn_ising_grad(catn_net* net, catn_result* res, double* dlnZ_dw, do
                             int32_t ckpt_interval) {
   if (!net || !res || !dlnZ_dh || (!dlnZ_dw && !net->im.ising.empty() && !net->im.ising[0].w.empty()))
     return fail(CATN_EINVAL, "NULL argument");
-  if (ckpt_interval != 0)
-    return fail(CATN_EINVAL, "checkpointed recomputation is not implemented; pass ckpt_interval = 0 "
-                             "(the tape of the whole contraction is kept on the device)");
+  if (ckpt_interval < 0) return fail(CATN_EINVAL, "ckpt_interval must be >= 0");
   if (catn_status s = check_ising_only(net->im)) return s;
   if (catn_status s = grad_prepare(net->im, net->grad ? net->grad->arena : grad_arena(net->R.L.arena_bytes, 1), 1,
                                       net->grad)) return s;
+  // this call's interval, in the uploaded instance descriptor
+  ((InstDesc*)net->grad->R.h_input)[0].P.ckpt_interval = ckpt_interval;
   cudaStream_t st = 0;
   if (catn_status s = grad_launch(net->grad, st)) return s;
   return grad_results(net->im, net->grad, res, dlnZ_dw, dlnZ_dh, st);

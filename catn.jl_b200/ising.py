@@ -30,7 +30,7 @@ class IsingNetwork(TensorNetwork):
     def __init__(self, n, edges, weights, fields, beta, pos1=0, val1=0, pos2=0, val2=0, Dmax=32, chi=32,
                  cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True, swapopt=True,
                  compress=False, cut_bond=False, seed=1, rsvd=0, rsvd_min_dim=0,
-                 precision="fp64", svd_route="auto"):
+                 precision="fp64", svd_route="auto", ckpt_interval=0):
         self.kind = "ising"
         self.n = int(n)
         self.edges = np.asarray(edges, dtype=np.int32).reshape(-1, 2) if len(edges) else np.zeros((0, 2), np.int32)
@@ -45,7 +45,8 @@ class IsingNetwork(TensorNetwork):
         self.params = dict(Dmax=Dmax, chi=chi, cutoff=cutoff, norm_method=norm_method, select=select,
                            reverse=reverse, svdopt=svdopt, swapopt=swapopt, compress=compress,
                            cut_bond=cut_bond, seed=seed, rsvd=rsvd,
-                           rsvd_min_dim=rsvd_min_dim, precision=precision, svd_route=svd_route)
+                           rsvd_min_dim=rsvd_min_dim, precision=precision, svd_route=svd_route,
+                           ckpt_interval=ckpt_interval)
         self.neighbors = [[0, 0] for _ in range(self.edges.shape[0])]   # trace sizing only
         deg = np.zeros(self.n + 1, int)
         for i, j in self.edges:
@@ -69,11 +70,14 @@ def ising_network(n, edges, weights, fields, beta, **kw):
     return IsingNetwork(n, edges, weights, fields, beta, **kw)
 
 
-def gradient(tn):
+def gradient(tn, ckpt_interval=None):
     """``(lnZ, dlnZ_dw, dlnZ_dh)`` of an Ising network from one forward
     contraction with a tape plus one backward pass, both on the device.
     ``dlnZ_dw[e] = beta <s_i s_j>``, ``dlnZ_dh[k] = beta <s_k>`` (exact up to
-    the contraction's own truncations).  Does not consume ``tn``."""
+    the contraction's own truncations).  ``ckpt_interval`` (default: the
+    network's) > 0 keeps a checkpoint every that many steps and recomputes
+    the segments in the backward pass; the gradients are the same bit for
+    bit.  Does not consume ``tn``."""
     if not isinstance(tn, IsingNetwork):
         raise TypeError("gradient: networks built by ising_network only")
     dev = tn._ensure_device()
@@ -81,7 +85,8 @@ def gradient(tn):
     res = L.Result()
     dw = np.zeros(max(tn.edges.shape[0], 1))
     dh = np.zeros(tn.n)
-    L.check(lib, lib.catn_ising_grad(dev.handle, ct.byref(res), L.ptr(dw), L.ptr(dh), 0))
+    k = tn.params.get("ckpt_interval", 0) if ckpt_interval is None else ckpt_interval
+    L.check(lib, lib.catn_ising_grad(dev.handle, ct.byref(res), L.ptr(dw), L.ptr(dh), int(k)))
     return res.lnZ, dw[:tn.edges.shape[0]], dh
 
 

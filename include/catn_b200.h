@@ -68,11 +68,12 @@ typedef struct {
                         * side >= 3 rsvd_min_dim (tests reach it with small
                         * networks); 0 = the reference's 7000 / 20000      */
   int32_t precision;   /* 0 = FP64 throughout; 1 = split: the products of
-                        * large swap merges and of the block-Jacobi SVD
-                        * route (pair Grams, pair rotations) in 3xTF32 on
-                        * the tensor cores with FP32 accumulation, while the
-                        * Jacobi eigen cores, every singular-value cutoff
-                        * test, the Dmax cut and lnZ stay FP64            */
+                        * large swap merges and the pair Grams of the block
+                        * Jacobi route's first phase in 3xTF32 on the
+                        * tensor cores with FP32 accumulation, while the
+                        * rotations, a second Jacobi phase on FP64 Grams,
+                        * every singular-value cutoff test, the Dmax cut
+                        * and lnZ stay FP64                              */
   int32_t svd_route;   /* large SVDs (not held in shared memory):
                         * 0 = auto (precision 0: scalar Jacobi; precision 1:
                         *     block Jacobi from the tuning table's size on),
@@ -81,6 +82,12 @@ typedef struct {
                         *     bit for bit),
                         * 2 = block one-sided Jacobi on the pivoted-QR
                         *     factor from the tuning table's size on      */
+  int32_t ckpt_interval; /* gradient runs: 0 = the tape of the whole
+                        * contraction stays on the device; K > 0 = the
+                        * forward pass keeps a checkpoint every K steps and
+                        * the backward pass recomputes one K-step segment
+                        * at a time (memory: one segment's tape plus the
+                        * checkpoints; gradients bit-identical to K = 0)  */
 } catn_params;
 
 /* Launch-shape and route thresholds, one process-wide table (no reference
@@ -324,8 +331,11 @@ catn_status catn_braket_create(const catn_params* p, int32_t n, const int32_t* n
  * (2.5x the forward arena: tape, append-only heap and its shadow) on the
  * first call and keeps them until destroy.
  *
- * ckpt_interval must be 0: the tape of the whole contraction is kept on the
- * device; checkpointed recomputation is not implemented (CATN_EINVAL). */
+ * ckpt_interval (>= 0) sets the network's catn_params.ckpt_interval for
+ * this call: 0 keeps the tape of the whole contraction on the device; K > 0
+ * keeps a checkpoint every K steps and recomputes one segment at a time in
+ * the backward pass (same gradients, bit for bit, in bounded memory).
+ * Batch gradient runs take each instance's catn_params.ckpt_interval. */
 catn_status catn_ising_grad(catn_net* net, catn_result* res, double* dlnZ_dw, double* dlnZ_dh,
                             int32_t ckpt_interval);
 /* Every instance of a batch in one persistent launch (inputs uploaded by the

@@ -151,6 +151,56 @@ def test_gradient_run_matches_plain_run(host):
     assert lz == res.lnZ
 
 
+CKPT_CASES = [
+    ("sq7_d8", "square", 7, dict(Dmax=8, chi=16)),
+    ("sq7_select0_norm2_noreverse", "square", 7, dict(Dmax=8, chi=16, select=0, norm_method=2, reverse=False)),
+    ("sq7_select2_norm0_plain_svd", "square", 7, dict(Dmax=8, chi=16, select=2, norm_method=0, svdopt=False,
+                                                     swapopt=False)),
+    ("sq7_cutbond", "square", 7, dict(Dmax=4, chi=8, cut_bond=True)),
+    ("rrg40_d16", "rrg", 40, dict(Dmax=16, chi=32)),
+    ("sq4_exact", "square", 4, dict(Dmax=-1, chi=10000)),
+]
+
+
+@pytest.mark.parametrize("name,graph,size,kw", CKPT_CASES, ids=[c[0] for c in CKPT_CASES])
+def test_checkpointed_gradients_bit_identical(host, name, graph, size, kw):
+    """ckpt_interval K > 0 (segments of K steps recomputed in the backward
+    pass from packed checkpoints) gives the whole-tape lnZ and gradients bit
+    for bit, for segment lengths that do and do not divide the step count."""
+    r = np.random.default_rng(zlib.crc32(name.encode()) % 1000)
+    if graph == "square":
+        e, n = X.square_edges(size), size * size
+    else:
+        e, n = X.random_regular_graph(size, 3, r), size
+    w, h = r.normal(size=len(e)), r.normal(0, 0.2, n)
+    st0, lz0, dw0, dh0 = grad(host, n, e, w, h, 0.7, **kw)
+    assert st0 == 0
+    for K in (1, 5, 16, 1000):
+        st, lz, dw, dh = grad(host, n, e, w, h, 0.7, ckpt_interval=K, **kw)
+        assert st == 0
+        assert lz == lz0
+        np.testing.assert_array_equal(dw, dw0)
+        np.testing.assert_array_equal(dh, dh0)
+
+
+def test_checkpointed_run_fits_where_the_whole_tape_does_not(host):
+    """20 x 20 lattice (399 steps): in a 16 MiB arena the whole tape runs out
+    of memory, while checkpoints every 64 steps fit and give the gradients of
+    the whole-tape run made in a larger arena."""
+    r = np.random.default_rng(20)
+    e = X.square_edges(20)
+    w, h = r.normal(size=len(e)), r.normal(0, 0.2, 400)
+    kw = dict(Dmax=4, chi=8)
+    st, _, _, _ = grad(host, 400, e, w, h, 0.8, arena=16 << 20, **kw)
+    assert st == L.CATN_ENOMEM
+    st0, lz0, dw0, dh0 = grad(host, 400, e, w, h, 0.8, arena=64 << 20, **kw)
+    st, lz, dw, dh = grad(host, 400, e, w, h, 0.8, arena=16 << 20, ckpt_interval=64, **kw)
+    assert st0 == 0 and st == 0
+    assert lz == lz0
+    np.testing.assert_array_equal(dw, dw0)
+    np.testing.assert_array_equal(dh, dh0)
+
+
 def test_compress_is_rejected(host):
     e = X.square_edges(3)
     st, _, _, _ = grad(host, 9, e, np.ones(len(e)), np.zeros(9), 0.5, Dmax=4, chi=8, compress=True)
@@ -171,7 +221,8 @@ import test_adjoint_host as T
 from oracle import exact as X
 lib = ct.CDLL({so!r})
 r = np.random.default_rng(3)
-for L, kw in [(5, dict(Dmax=4, chi=16)), (5, dict(Dmax=1000, chi=100000, cut_bond=True)), (4, dict(Dmax=-1, chi=100, norm_method=2))]:
+for L, kw in [(5, dict(Dmax=4, chi=16)), (5, dict(Dmax=1000, chi=100000, cut_bond=True)), (4, dict(Dmax=-1, chi=100, norm_method=2)),
+              (5, dict(Dmax=4, chi=16, ckpt_interval=3))]:
     e = X.square_edges(L)
     st, lz, dw, dh = T.grad(lib, L*L, e, r.normal(size=len(e)), r.normal(0, .1, L*L), 1.0, **kw)
     assert st == 0, st

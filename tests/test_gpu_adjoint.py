@@ -116,5 +116,39 @@ def test_rejections(catn):
     lib = L.load()
     res = L.Result()
     dw, dh = np.zeros(len(e)), np.zeros(9)
-    assert lib.catn_ising_grad(dev.handle, res, L.ptr(dw), L.ptr(dh), 64) == L.CATN_EINVAL
-    assert "checkpointed" in L.last_error(lib)
+    assert lib.catn_ising_grad(dev.handle, res, L.ptr(dw), L.ptr(dh), -1) == L.CATN_EINVAL
+    assert "ckpt_interval" in L.last_error(lib)
+
+
+@pytest.mark.parametrize("K", [1, 7, 64])
+def test_checkpointed_gradients_equal_whole_tape(catn, K):
+    """ckpt_interval K > 0 recomputes K-step segments in the backward pass;
+    the values, records and accumulation order are those of the whole tape,
+    so lnZ and every gradient entry are equal bit for bit."""
+    r = np.random.default_rng(31)
+    L = 10
+    e = X.square_edges(L)
+    n = L * L
+    w, h = r.normal(size=len(e)), r.normal(0, 0.2, n)
+    tn = catn.ising_network(n, e, w, h, 1.0, Dmax=48, chi=256)
+    lz0, dw0, dh0 = catn.gradient(tn, ckpt_interval=0)
+    lz, dw, dh = catn.gradient(tn, ckpt_interval=K)
+    assert lz == lz0
+    np.testing.assert_array_equal(dw, dw0)
+    np.testing.assert_array_equal(dh, dh0)
+
+
+def test_checkpointed_batch_gradients(catn):
+    r = np.random.default_rng(32)
+    insts = []
+    for q in range(5):
+        L = int(r.choice([6, 8, 10]))
+        e = X.square_edges(L)
+        insts.append(dict(n=L * L, edges=e, weights=r.normal(size=len(e)), fields=r.normal(0, 0.1, L * L),
+                          beta=float(r.uniform(0.5, 2.0))))
+    whole = catn.IsingBatch(insts, Dmax=32, chi=128).grad()
+    ckpt = catn.IsingBatch(insts, Dmax=32, chi=128, ckpt_interval=16).grad()
+    for (lz0, dw0, dh0), (lz, dw, dh) in zip(whole, ckpt):
+        assert lz == lz0
+        np.testing.assert_array_equal(dw, dw0)
+        np.testing.assert_array_equal(dh, dh0)
