@@ -30,7 +30,7 @@ class Params(ct.Structure):
                 ("svdopt", ct.c_int32), ("swapopt", ct.c_int32), ("compress", ct.c_int32),
                 ("cut_bond", ct.c_int32), ("seed", ct.c_int32), ("trace", ct.c_int32), ("rsvd", ct.c_int32),
                 ("rsvd_min_dim", ct.c_int32), ("precision", ct.c_int32), ("svd_route", ct.c_int32),
-                ("ckpt_interval", ct.c_int32)]
+                ("ckpt_interval", ct.c_int32), ("braket_loops", ct.c_int32)]
 
 
 class Tuning(ct.Structure):
@@ -153,14 +153,15 @@ SVD_ROUTES = {"auto": 0, "scalar": 1, "block": 2}
 
 def make_params(Dmax=32, chi=32, cutoff=1e-15, norm_method=1, select=1, reverse=True, svdopt=True,
                 swapopt=True, compress=False, cut_bond=False, seed=1, trace=False, rsvd=0, rsvd_min_dim=0,
-                precision="fp64", svd_route="auto", ckpt_interval=0):
+                precision="fp64", svd_route="auto", ckpt_interval=0, braket_loops=False):
     """``catn_params`` from the reference's keywords plus the engine's own:
     ``rsvd`` / ``rsvd_min_dim`` (randomized swap route), ``precision``
     ("fp64" or "split"), ``svd_route`` ("auto", "scalar", "block") and
     ``ckpt_interval`` (gradient runs: steps between checkpoints, 0 = whole
-    tape)."""
+    tape) and ``braket_loops`` (BraKet networks with cycles)."""
     prec = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     route = SVD_ROUTES[svd_route] if isinstance(svd_route, str) else int(svd_route)
     return Params(int(Dmax), int(chi), float(cutoff), int(norm_method), int(select), int(bool(reverse)),
                   int(bool(svdopt)), int(bool(swapopt)), int(bool(compress)), int(bool(cut_bond)),
-                  int(seed), int(bool(trace)), int(rsvd), int(rsvd_min_dim), prec, route, int(ckpt_interval))
+                  int(seed), int(bool(trace)), int(rsvd), int(rsvd_min_dim), prec, route, int(ckpt_interval),
+                  int(bool(braket_loops)))

@@ -5,6 +5,10 @@ seed)`` builds the double-layer network <psi|psi> of a real ket state; the
 label analysis runs in the C library on the host, the BraKet nodes are built
 and contracted on the device.  ``contraction(bk)`` returns
 ``(lnZ, error, psi)`` with ``<psi|psi> = exp(lnZ) * psi``.
+
+``loops=True`` (no reference counterpart; the reference rejects a cyclic
+virtual-bond graph) contracts loopy states such as PEPS: each pair of doubled
+bonds that an eat makes parallel is fused, ket with ket and bra with bra.
 """
 import ctypes as ct
 
@@ -17,7 +21,8 @@ from .network import TensorNetwork
 class BraKetNetwork(TensorNetwork):
     """``BraKetNetwork`` (braket.jl:335-349) of ``braket_network(tensors, ixs)``."""
 
-    def __init__(self, tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1):
+    def __init__(self, tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1,
+                 loops=False):
         self.kind = "braket"
         if len(tensors) != len(ixs):
             raise ValueError("braket_network: length(tensors) != length(ixs)")
@@ -41,12 +46,13 @@ class BraKetNetwork(TensorNetwork):
         self.beta = 1.0
         # the C ABI takes the keyword set of TensorNetwork; Dmax is unused here
         self.params = dict(Dmax=-1, chi=chi, cutoff=cutoff, norm_method=norm_method, select=2, reverse=False,
-                           svdopt=svdopt, swapopt=swapopt, compress=False, cut_bond=False, seed=seed)
+                           svdopt=svdopt, swapopt=swapopt, compress=False, cut_bond=False, seed=seed,
+                           braket_loops=bool(loops))
         self.neighbors = [list(ix) for ix in ixs]   # trace sizing only
         self.num_isolated = 0
         self._reset_outputs()
         self._dev = None
-        _validate(ixs)   # the reference's constructor errors (braket.jl:377-421), before any device work
+        _validate(ixs, loops)   # the reference's constructor errors (braket.jl:377-421), before any device work
 
     def _create(self, lib, p, arena):
         ndims = np.array([t.ndim for t in self.tensors], dtype=np.int32)
@@ -58,7 +64,7 @@ class BraKetNetwork(TensorNetwork):
         return h
 
 
-def _validate(ixs):
+def _validate(ixs, loops=False):
     count, owners = {}, {}
     for k, ix in enumerate(ixs):
         for lbl in ix:
@@ -79,8 +85,15 @@ def _validate(ixs):
             x = parent[x]
         return x
 
+    pairs = set()
     for lbl, o in owners.items():
-        if len(o) == 2:
+        if len(o) == 2 and loops:
+            key = (min(o), max(o))
+            if key in pairs:
+                raise ValueError(f"braket_network: tensors {key[0] + 1} and {key[1] + 1} share more than one label "
+                                 "(parallel bonds are not supported)")
+            pairs.add(key)
+        elif len(o) == 2:
             a, b = root(o[0]), root(o[1])
             if a == b:
                 raise ValueError("braket_network: virtual-bond graph contains a cycle — cyclic graphs are not "
@@ -88,7 +101,9 @@ def _validate(ixs):
             parent[a] = b
 
 
-def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1):
-    """``braket_network`` (braket.jl:369-508)."""
+def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1,
+                   loops=False):
+    """``braket_network`` (braket.jl:369-508); ``loops=True`` accepts cyclic
+    virtual-bond graphs (fusing parallel doubled bonds as they form)."""
     return BraKetNetwork(tensors, ixs, chi=chi, cutoff=cutoff, norm_method=norm_method, svdopt=svdopt,
-                         swapopt=swapopt, seed=seed)
+                         swapopt=swapopt, seed=seed, loops=loops)

@@ -219,6 +219,16 @@ CATN_HDI inline double eat_braket(Ctx& C, int ki, int kj, double* err, double* p
 // edge each step, j absorbed into i (order(i) >= order(j)), compress(_opt)!
 // of i, the eaten edge removed and every edge (and neighbour id) naming j
 // re-pointed to i; finally the norms of the remaining nodes.
+//
+// With P.braket_loops (no reference counterpart: the reference rejects
+// cycles, braket.jl:405-420), a neighbour k of both i and j now holds two
+// doubled bonds to i.  The re-pointed edge is dropped from the list, and the
+// pair is fused as merge! fuses a duplicate bond (mps_node.jl:595-622): in k
+// the ket legs, then the bra legs, each in the order (i's bond, j's bond)
+// (`cross` from their positions before the re-pointing, as
+// tensor_network.jl:641-650 does); then the same two fusions in i, whose
+// own legs precede the ones it took from j.  After the fusions of a step, i
+// is compressed once more.
 CATN_HDI inline ContractOut contract_braket(Ctx& C, const int* edges0, int ne0) {
   const Team& T = C.T;
   ContractOut O;
@@ -237,27 +247,29 @@ CATN_HDI inline ContractOut contract_braket(Ctx& C, const int* edges0, int ne0) 
     if (failed(C)) break;
     O.err += compress_node(C, i, C.P.svdopt != 0);
     if (failed(C)) break;
-    const int nsi = C.node[i].nsites;
-    unsigned shh = 2166136261u, lyh = 2166136261u;
-    for (int p = 1; p <= nsi; ++p) {
-      const int d = sref(C, i, p).d;
-      if (d > maxdim) maxdim = d;
-      shh = fnv_step(shh, d);
-      lyh = fnv_step(lyh, (nbref(C, i, p) & BRA) ? 0 : 1);
-    }
+    for (int p = 1; p <= C.node[i].nsites; ++p) if (sref(C, i, p).d > maxdim) maxdim = sref(C, i, p).d;
+    int* dup = C.list;   // [0] count, then (k, cross bits) pairs
     T.sync();
     if (T.leader()) {
       // drop the eaten edge, re-point the ones naming j (and j's neighbours' ids)
-      int w = 0;
+      int w = 0, nd = 0;
       for (int e = 0; e < ne; ++e) {
         int a = E[2 * e], b = E[2 * e + 1];
         if ((a == i && b == j) || (a == j && b == i)) continue;
         if (a == j || b == j) {
           const int other = a == j ? b : a;
+          const int xk = nb_find(C, other, i), yk = nb_find(C, other, j);
+          const int xb = nb_find(C, other, i | BRA), yb = nb_find(C, other, j | BRA);
           const int nn = C.node[other].nnbr;
           for (int p = 1; p <= nn; ++p) {
             const int v = nbref(C, other, p);
             if ((v & ~BRA) == j) nbref(C, other, p) = i | (v & BRA);
+          }
+          if (xk > 0) {   // a second doubled bond between i and other (loops only)
+            dup[1 + 2 * nd] = other;
+            dup[2 + 2 * nd] = (xk > yk ? 1 : 0) | (xb > yb ? 2 : 0);
+            ++nd;
+            continue;
           }
           if (a == j) a = i; else b = i;
         }
@@ -265,16 +277,39 @@ CATN_HDI inline ContractOut contract_braket(Ctx& C, const int* edges0, int ne0) 
         E[2 * w + 1] = b;
         ++w;
       }
+      dup[0] = nd;
       C.ctl[CTL_BCAST] = w;
       C.node[j].nsites = 0;
       C.node[j].nnbr = 0;
-      if (C.trace && O.nsteps < C.trace_cap) {
-        int* r = C.trace + 8LL * O.nsteps;
-        r[0] = i; r[1] = j; r[2] = 0; r[3] = (int)lyh; r[4] = 0; r[5] = nsi; r[6] = (int)shh; r[7] = maxdim;
-      }
+      if (nd > 0 && !C.P.braket_loops) fail_leader(C, CATN_ESTATE);
+    }
+    refresh_status(C);
+    ne = C.ctl[CTL_BCAST];
+    const int nd = dup[0];
+    for (int q = 0; q < nd && !failed(C); ++q) {
+      const int k = dup[1 + 2 * q], cr = dup[2 + 2 * q];
+      O.err += merge_dup(C, k, i, (cr & 1) != 0);
+      if (!failed(C)) O.err += merge_dup(C, k, i | BRA, (cr & 2) != 0);
+      if (!failed(C)) O.err += merge_dup(C, i, k, false);
+      if (!failed(C)) O.err += merge_dup(C, i, k | BRA, false);
+      for (int p = 1; p <= C.node[k].nsites; ++p) if (sref(C, k, p).d > maxdim) maxdim = sref(C, k, p).d;
+    }
+    if (nd > 0 && !failed(C)) {
+      O.err += compress_node(C, i, C.P.svdopt != 0);
+      for (int p = 1; p <= C.node[i].nsites; ++p) if (sref(C, i, p).d > maxdim) maxdim = sref(C, i, p).d;
+    }
+    if (failed(C)) break;
+    const int nsi = C.node[i].nsites;
+    unsigned shh = 2166136261u, lyh = 2166136261u;
+    for (int p = 1; p <= nsi; ++p) {
+      shh = fnv_step(shh, sref(C, i, p).d);
+      lyh = fnv_step(lyh, (nbref(C, i, p) & BRA) ? 0 : 1);
     }
     T.sync();
-    ne = C.ctl[CTL_BCAST];
+    if (T.leader() && C.trace && O.nsteps < C.trace_cap) {
+      int* r = C.trace + 8LL * O.nsteps;
+      r[0] = i; r[1] = j; r[2] = 0; r[3] = (int)lyh; r[4] = nd; r[5] = nsi; r[6] = (int)shh; r[7] = maxdim;
+    }
     T.sync();
     O.nsteps += 1;
   }

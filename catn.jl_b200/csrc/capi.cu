@@ -58,6 +58,7 @@ catn_status check_params(const catn_params* p) {
   if (p->precision < 0 || p->precision > 1) return fail(CATN_EINVAL, "precision must be 0 (FP64) or 1 (split)");
   if (p->svd_route < 0 || p->svd_route > 2) return fail(CATN_EINVAL, "svd_route must be 0, 1 or 2");
   if (p->ckpt_interval < 0) return fail(CATN_EINVAL, "ckpt_interval must be >= 0");
+  if (p->braket_loops < 0 || p->braket_loops > 1) return fail(CATN_EINVAL, "braket_loops must be 0 or 1");
   return CATN_OK;
 }
 
@@ -120,7 +121,12 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     // CTAs drain the queue).
     if (T.bcast(threadIdx.x == 0 ? res[inst].status : 0) == CATN_ETIMEOUT) break;
   }
-  if (board) help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+  if (board) {
+    if (jl.cta_jobs)
+      help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+    else
+      help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
+  }
   tc_teardown(T);
 }
 
@@ -153,8 +159,11 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   R.ninst = (int)im.desc.size();
   if (R.ninst == 0) return fail(CATN_EINVAL, "no instances");
   R.use_tc = 0;
-  for (const InstDesc& d : im.desc)
+  R.cta_jobs = 0;
+  for (const InstDesc& d : im.desc) {
     if (d.P.precision == 1) R.use_tc = 1;
+    if (d.P.svd_route == 2 || (d.P.svd_route == 0 && d.P.precision == 1)) R.cta_jobs = 1;
+  }
   R.L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
   int dev = 0, nsm = 0, per_sm = 0;
   CUDA_TRY(cudaGetDevice(&dev));
@@ -235,6 +244,7 @@ void helper_config(const DeviceRun& R, bool grad, JobLink* jl, int* nhelp) {
   jl->min_qr = std::max(1LL, (long long)t.shared_house_min);
   jl->block_min_n = std::max(4, (int)t.block_min_n);
   jl->blocked_qr_min_n = std::max(4, (int)t.blocked_qr_min_n);
+  jl->cta_jobs = R.cta_jobs;
 }
 
 catn_status upload(DeviceRun& R, cudaStream_t st) {
@@ -372,6 +382,7 @@ void catn_params_default(catn_params* p) {
   p->precision = 0;
   p->svd_route = 0;
   p->ckpt_interval = 0;
+  p->braket_loops = 0;
 }
 
 catn_status catn_tuning_get(catn_tuning* t) {

@@ -56,7 +56,12 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     // CTAs drain the queue).
     if (T.bcast(threadIdx.x == 0 ? res[inst].status : 0) == CATN_ETIMEOUT) break;
   }
-  if (board) help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+  if (board) {
+    if (jl.cta_jobs)
+      help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
+    else
+      help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
+  }
   tc_teardown(T);
 }
 

@@ -70,6 +70,7 @@ struct DeviceRun {
   int ngrid = 0;   // CTAs per launch: nslots, or every resident CTA for one network (the rest help)
   int ninst = 0;
   int use_tc = 0;  // some instance runs in split precision: TMEM and the staging area per CTA
+  int cta_jobs = 0;   // some instance takes the block SVD route (its jobs are CTA items)
   long long input_bytes = 0;
 
   void release() {

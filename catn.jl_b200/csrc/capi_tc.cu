@@ -17,16 +17,19 @@ constexpr int kTcBN = 128;   // columns per CTA tile (MMA N, TMEM columns)
 constexpr int kTcBK = 32;    // K per stage
 constexpr int kTcThreads = 256;
 constexpr uint32_t kTcTmemCols = 128;
-constexpr int kTcTileBytes = kTcBM * kTcBK * 4;   // one FP32 operand tile (16 KiB)
-constexpr int kTcSmem = 4 * kTcTileBytes + 1024 + 64;
+constexpr int kTcTileBytes = kTcBM * kTcBK * 4;        // one FP32 operand tile (16 KiB)
+constexpr int kTcStageBytes = 4 * kTcTileBytes;         // A hi, A lo, B hi, B lo
+constexpr int kTcSmem = 2 * kTcStageBytes + 1024 + 64;  // two stages, alignment, barriers
 constexpr long long kTcWaitPolls = 1LL << 24;
 
 // C (M x N) = A (M x K) * B (K x N), column-major FP64, one 128 x 128 tile of
-// C per CTA.  Per stage of 32 values of K the threads split A and B into
-// TF32 hi / lo parts in shared memory (K-major), one thread issues the 4 x 3
-// MMAs into the TMEM accumulator and commits them to an mbarrier, and the
-// CTA waits for them before it overwrites the operands.  *err is set when a
-// wait ran out (the tile is then not written).
+// C per CTA.  Two shared-memory stages of 32 values of K: while one thread's
+// 4 x 3 MMAs of stage s run on the tensor cores (TMEM accumulator, completion
+// committed to the stage's mbarrier), the threads load stage s + 1 from
+// global memory into registers, wait until the MMAs of stage s - 1 have
+// released the other buffer, and split the values into TF32 hi / lo parts
+// there (K-major).  *err is set when a wait ran out (the tile is then not
+// written).
 __global__ void __launch_bounds__(kTcThreads) catn_tc_matmul_kernel(int M, int N, int K, const double* A, int lda,
                                                                      const double* B, int ldb, double* C, int ldc,
                                                                      int* err) {
@@ -34,18 +37,15 @@ __global__ void __launch_bounds__(kTcThreads) catn_tc_matmul_kernel(int M, int N
   using namespace catn::tc;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   unsigned char* base = (unsigned char*)(((uintptr_t)tc_smem + 1023) & ~(uintptr_t)1023);
-  float* a_hi = (float*)base;
-  float* a_lo = (float*)(base + kTcTileBytes);
-  float* b_hi = (float*)(base + 2 * kTcTileBytes);
-  float* b_lo = (float*)(base + 3 * kTcTileBytes);
-  uint64_t* bar = (uint64_t*)(base + 4 * kTcTileBytes);
-  uint32_t* tslot = (uint32_t*)(base + 4 * kTcTileBytes + 16);
+  uint64_t* bar = (uint64_t*)(base + 2 * kTcStageBytes);   // one per stage buffer
+  uint32_t* tslot = (uint32_t*)(base + 2 * kTcStageBytes + 16);
   __shared__ int failed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const long long m0 = (long long)blockIdx.x * kTcBM, n0 = (long long)blockIdx.y * kTcBN;
   if (tid == 0) {
     failed = 0;
     mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
   }
   if (warp == 0) tmem_alloc(tslot, kTcTmemCols);
   fence_before_sync();
@@ -54,25 +54,48 @@ __global__ void __launch_bounds__(kTcThreads) catn_tc_matmul_kernel(int M, int N
   const uint32_t tmem = *tslot;
   const uint32_t idesc = idesc_tf32(kTcBM, kTcBN);
   const uint32_t sbo = kTcBK / 4 * 128;
-  uint32_t phase = 0;
-  for (int k0 = 0; k0 < K; k0 += kTcBK) {
-    for (int e = tid; e < kTcBM * kTcBK; e += kTcThreads) {
-      const int r = e % kTcBM, k = e / kTcBM;   // consecutive rows: coalesced column reads
+  const int ns = (K + kTcBK - 1) / kTcBK;
+  double va[16], vb[16];
+  auto load = [&](int st) {
+    const long long k0 = (long long)st * kTcBK;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + kTcThreads * j;
+      const int r = e & 127, k = e >> 7;   // A: consecutive rows (coalesced column reads)
       const long long gr = m0 + r, gk = k0 + k;
-      const double v = (gr < M && gk < K) ? A[gr + gk * (long long)lda] : 0.0;
+      va[j] = (gr < M && gk < K) ? A[gr + gk * (long long)lda] : 0.0;
+      const int kb = e & 31, n = e >> 5;   // B: consecutive k
+      const long long gn = n0 + n, gkb = k0 + kb;
+      vb[j] = (gn < N && gkb < K) ? B[gkb + gn * (long long)ldb] : 0.0;
+    }
+  };
+  if (ns > 0) load(0);
+  int st = 0;
+  for (; st < ns; ++st) {
+    const int b = st & 1;
+    float* a_hi = (float*)(base + b * kTcStageBytes);
+    float* a_lo = a_hi + kTcBM * kTcBK;
+    float* b_hi = a_lo + kTcBM * kTcBK;
+    float* b_lo = b_hi + kTcBN * kTcBK;
+    if (st >= 2) {
+      // the MMAs of stage st - 2 read this buffer: the barrier's use number (st - 2) / 2
+      const bool ok = mbar_wait(bar + b, (uint32_t)(((st - 2) >> 1) & 1), kTcWaitPolls);
+      fence_after_sync();
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) failed = 1;
+        break;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int e = tid + kTcThreads * j;
       float h, l;
-      split_tf32(v, &h, &l);
-      const uint32_t o = kmajor_off(r, k, kTcBK) / 4;
+      split_tf32(va[j], &h, &l);
+      uint32_t o = kmajor_off(e & 127, e >> 7, kTcBK) / 4;
       a_hi[o] = h;
       a_lo[o] = l;
-    }
-    for (int e = tid; e < kTcBN * kTcBK; e += kTcThreads) {
-      const int k = e % kTcBK, n = e / kTcBK;   // consecutive k: coalesced column reads
-      const long long gn = n0 + n, gk = k0 + k;
-      const double v = (gn < N && gk < K) ? B[gk + gn * (long long)ldb] : 0.0;
-      float h, l;
-      split_tf32(v, &h, &l);
-      const uint32_t o = kmajor_off(n, k, kTcBK) / 4;
+      split_tf32(vb[j], &h, &l);
+      o = kmajor_off(e >> 5, e & 31, kTcBK) / 4;
       b_hi[o] = h;
       b_lo[o] = l;
     }
@@ -80,25 +103,28 @@ __global__ void __launch_bounds__(kTcThreads) catn_tc_matmul_kernel(int M, int N
     __syncthreads();
     if (tid == 0) {
       fence_after_sync();
+#pragma unroll
       for (int s = 0; s < kTcBK / 8; ++s) {
         const uint32_t off = (uint32_t)s * 2 * kLBO;
         const uint64_t dah = smem_desc(smem_u32(a_hi) + off, kLBO, sbo);
         const uint64_t dal = smem_desc(smem_u32(a_lo) + off, kLBO, sbo);
         const uint64_t dbh = smem_desc(smem_u32(b_hi) + off, kLBO, sbo);
         const uint64_t dbl = smem_desc(smem_u32(b_lo) + off, kLBO, sbo);
-        mma_tf32(tmem, dah, dbh, idesc, (k0 > 0 || s > 0) ? 1u : 0u);
+        mma_tf32(tmem, dah, dbh, idesc, (st > 0 || s > 0) ? 1u : 0u);
         mma_tf32(tmem, dah, dbl, idesc, 1u);
         mma_tf32(tmem, dal, dbh, idesc, 1u);
       }
-      mma_commit(bar);
+      mma_commit(bar + b);
     }
-    const bool ok = mbar_wait(bar, phase, kTcWaitPolls);
-    phase ^= 1u;
+    if (st + 1 < ns) load(st + 1);   // global latency under the MMAs just issued
+  }
+  // MMAs complete in issue order: the last committed stage's barrier covers all
+  const int issued = st;   // stages whose MMAs were committed
+  if (issued > 0) {
+    const int last = issued - 1;
+    const bool ok = mbar_wait(bar + (last & 1), (uint32_t)((last >> 1) & 1), kTcWaitPolls);
     fence_after_sync();
-    if (__syncthreads_or(!ok)) {
-      if (tid == 0) failed = 1;
-      break;
-    }
+    if (__syncthreads_or(!ok) && tid == 0) failed = 1;
   }
   __syncthreads();
   if (K > 0 && !failed) {
@@ -121,10 +147,7 @@ __global__ void __launch_bounds__(kTcThreads) catn_tc_matmul_kernel(int M, int N
       if (r < M && c < N) C[r + c * (long long)ldc] = 0.0;
     }
   }
-  if (failed && tid == 0) {
-    *err = 1;
-    mbar_wait(bar, phase ^ 1u, kTcWaitPolls);   // let the MMAs in flight land before freeing TMEM
-  }
+  if (failed && tid == 0) *err = 1;
   fence_before_sync();
   __syncthreads();
   fence_after_sync();

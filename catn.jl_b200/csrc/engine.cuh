@@ -123,6 +123,7 @@ struct JobLink {
   long long min_qr;
   int block_min_n;   // smallest Jacobi factor (columns) on the block route
   int blocked_qr_min_n;
+  int cta_jobs;      // some instance may publish CTA items (block route): helpers claim as whole CTAs
 };
 
 // ---------------------------------------------------------------------------

@@ -209,12 +209,22 @@ struct Image {
     std::vector<int> epairs;
     for (size_t x = 0; x < order.size(); ++x) {
       if (owners[x].size() != 2) continue;
-      const int a = root(owners[x][0]), b = root(owners[x][1]);
-      if (a == b)
-        return "braket_network: virtual-bond graph contains a cycle — cyclic graphs are not supported in v1";
-      parent[a] = b;
-      epairs.push_back(owners[x][0]);
-      epairs.push_back(owners[x][1]);
+      const int u = owners[x][0], v = owners[x][1];
+      if (P.braket_loops) {
+        // cycles of three or more nodes are contracted; two labels on the
+        // same pair of tensors (a parallel bond) are not
+        for (size_t q = 0; q + 1 < epairs.size(); q += 2)
+          if ((epairs[q] == u && epairs[q + 1] == v) || (epairs[q] == v && epairs[q + 1] == u))
+            return "braket_network: tensors " + std::to_string(u) + " and " + std::to_string(v) +
+                   " share more than one label (parallel bonds are not supported)";
+      } else {
+        const int a = root(u), b = root(v);
+        if (a == b)
+          return "braket_network: virtual-bond graph contains a cycle — cyclic graphs are not supported in v1";
+        parent[a] = b;
+      }
+      epairs.push_back(u);
+      epairs.push_back(v);
     }
     InstDesc D;
     std::memset(&D, 0, sizeof(D));

@@ -1156,6 +1156,73 @@ CATN_HDI inline int qr_apply_q_shared(const Team& T, JacobiJob* J, const double*
 // worked on for that job's next round before it scans the board again.
 constexpr int kJobStickPolls = 64;
 
+#if defined(__CUDACC__)
+// Whether J is open with unclaimed items of its current round (warp-uniform:
+// lane 0's view).
+__device__ __forceinline__ bool job_has_items(const JacobiJob* J) {
+  int open = ldcg_i(&J->open);
+  unsigned long long word = ldcg_u(&J->word);
+  open = __shfl_sync(0xffffffffu, open, 0);
+  word = __shfl_sync(0xffffffffu, word, 0);
+  return open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
+}
+
+// Helper loop of launches whose jobs are all warp items (scalar Jacobi pairs
+// and Householder columns): every warp scans the board, claims items and
+// stays with its job independently, with no CTA barrier, until every
+// instance of the launch is finished.  Launches that can publish CTA items
+// (block Jacobi pairs, blocked-QR panels) use help_jobs instead.
+__device__ inline void help_jacobi(const Team& T, JacobiJob* board, int nslots, const int* finished, int ninst) {
+  const unsigned FULL = 0xffffffffu;
+  const int w = (int)blockIdx.x * T.nwarps() + T.warp();
+  const int lane = T.lane();
+  long long idle = 0;
+  while (idle < (1LL << 22)) {
+    if (ldcg_i(finished) >= ninst) return;
+    // find a job with unclaimed items: the lanes check 32 slots at once
+    // (independent L2 loads), starting at a warp-specific block so that
+    // helpers spread over the open jobs
+    const int nblk = (nslots + 31) / 32;
+    int pick = -1;
+    for (int b = 0; b < nblk && pick < 0; ++b) {
+      const int base = ((b + w) % nblk) * 32;
+      const int s = base + lane;
+      bool ok = false;
+      if (s < nslots) {
+        const JacobiJob* J = board + s;
+        const int open = ldcg_i(&J->open);
+        const unsigned long long word = ldcg_u(&J->word);
+        ok = open && (word & 0xfffffULL) < ((word >> 20) & 0xfffffULL);
+      }
+      const unsigned mask = __ballot_sync(FULL, ok);
+      if (mask) {
+        const int r = w & 31;   // first candidate at or after lane r (cyclically)
+        const unsigned hi = mask & (~0u << r);
+        pick = base + __ffs(hi ? hi : mask) - 1;
+      }
+    }
+    if (pick < 0) {
+      ++idle;
+      __nanosleep(256);
+      continue;
+    }
+    idle = 0;
+    JacobiJob* J = board + pick;
+    job_work(T, J);
+    // stay with J: its owner opens the next round within microseconds
+    for (int t = 0; t < kJobStickPolls; ++t) {
+      if (job_has_items(J)) {
+        job_work(T, J);
+        t = -1;
+        continue;
+      }
+      if (!ldcg_i(&J->open)) break;
+      __nanosleep(32);
+    }
+  }
+}
+#endif
+
 // Column norms of B (n columns), then stable descending order.
 // S_out[r] = sigma of the r-th largest column, perm[r] = its column index.
 CATN_HDI inline void sort_columns(const Team& T, const double* B, long long m, long long n,

@@ -88,6 +88,12 @@ typedef struct {
                         * the backward pass recomputes one K-step segment
                         * at a time (memory: one segment's tape plus the
                         * checkpoints; gradients bit-identical to K = 0)  */
+  int32_t braket_loops; /* catn_braket_create: 0 = a cyclic virtual-bond
+                        * graph is rejected, as the reference does
+                        * (src/braket.jl:405-420); 1 = cycles are allowed
+                        * and each pair of doubled bonds that an eat makes
+                        * parallel is fused (ket with ket, bra with bra)
+                        * before the next step                           */
 } catn_params;
 
 /* Launch-shape and route thresholds, one process-wide table (no reference
@@ -309,9 +315,11 @@ catn_status catn_batch_destroy(catn_batch* b);
  * column-major data; labels[...] holds one positive label per axis.  A label
  * on one tensor is its physical index (exactly one per tensor), a label on
  * two tensors a virtual bond; a cyclic bond graph is rejected (CATN_EINVAL,
- * as the reference errors).  Contract it with catn_contract: lnZ = log of
- * <psi|psi> up to psi, err = discarded weight, maxdim = largest leg seen.
- * Only p->chi, cutoff, norm_method and svdopt are used.  The edges are taken
+ * as the reference errors) unless p->braket_loops is 1, and two labels
+ * shared by the same two tensors are always rejected.  Contract it with
+ * catn_contract: lnZ = log of <psi|psi> up to psi, err = discarded weight,
+ * maxdim = largest leg seen.  Only p->chi, cutoff, norm_method, svdopt and
+ * braket_loops are used.  The edges are taken
  * in the order their labels first appear (the reference iterates a Julia
  * Dict there, src/braket.jl:489-497). */
 catn_status catn_braket_create(const catn_params* p, int32_t n, const int32_t* ndims, const int64_t* dims,

@@ -96,8 +96,9 @@ def move(node, a, b):
 class BraKetNetwork:
     """``BraKetNetwork`` (braket.jl:335-349)."""
 
-    def __init__(self, tensors, edges, chi, cutoff, norm_method, svdopt, swapopt):
+    def __init__(self, tensors, edges, chi, cutoff, norm_method, svdopt, swapopt, loops=False):
         self.tensors = tensors
+        self.loops = loops
         self.edges = edges          # list of (i, j), in processing order
         self.chi, self.cutoff, self.norm_method = chi, cutoff, norm_method
         self.svdopt, self.swapopt = svdopt, swapopt
@@ -105,8 +106,11 @@ class BraKetNetwork:
         self.maxdim_intermediate = 0
 
 
-def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1):
-    """(braket.jl:369-508); edges in first-appearance order of their labels."""
+def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=True, swapopt=True, seed=1,
+                   loops=False):
+    """(braket.jl:369-508); edges in first-appearance order of their labels.
+    ``loops=True`` restates the library's loopy extension (no reference
+    counterpart): cycles are accepted, parallel bonds in the input are not."""
     n = len(tensors)
     if n != len(ixs):
         raise ValueError("braket_network: length(tensors) != length(ixs)")
@@ -132,8 +136,15 @@ def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=Tru
             x = parent[x]
         return x
 
+    pairs = set()
     for lbl in order:
-        if count[lbl] == 2:
+        if count[lbl] == 2 and loops:
+            key = tuple(sorted(owners[lbl]))
+            if key in pairs:
+                raise ValueError(f"braket_network: tensors {key[0]} and {key[1]} share more than one label "
+                                 "(parallel bonds are not supported)")
+            pairs.add(key)
+        elif count[lbl] == 2:
             a, b = root(owners[lbl][0]), root(owners[lbl][1])
             if a == b:
                 raise ValueError("braket_network: virtual-bond graph contains a cycle — cyclic graphs are not "
@@ -151,7 +162,7 @@ def braket_network(tensors, ixs, chi=64, cutoff=1e-15, norm_method=1, svdopt=Tru
         nodes[i + 1] = braket_node(np.asarray(tensors[i], dtype=np.float64), kn, phys, chi=chi, cutoff=cutoff,
                                    norm_method=norm_method, svdopt=svdopt, swapopt=swapopt)
     edges = [tuple(owners[lbl]) for lbl in order if count[lbl] == 2]
-    return BraKetNetwork(nodes, edges, chi, cutoff, norm_method, svdopt, swapopt)
+    return BraKetNetwork(nodes, edges, chi, cutoff, norm_method, svdopt, swapopt, loops)
 
 
 def _norm(node, t):
@@ -223,6 +234,26 @@ def eat(ni, nj, j_id, i_id):
     return _finish(ni, err)
 
 
+def merge_leg(node, j, isket, cross):
+    """Loopy extension: fuse the two legs of ``node`` pointing to ``j`` in one
+    layer, as ``merge!`` (mps_node.jl:595-622) fuses a duplicate bond, the
+    layer tags riding along with the swaps."""
+    positions = [k + 1 for k in range(len(node.mps)) if node.neighbor[k] == j and node.layer[k] == isket]
+    if len(positions) != 2:
+        raise ValueError(f"merge: expected 2 legs to {j} in one layer, found {len(positions)}")
+    idx1, idx2 = positions
+    target = idx1 if cross else idx1 + 1
+    err = move(node, idx2, target)
+    del node.neighbor[target - 1]
+    del node.layer[target - 1]
+    M.cano_to(node, idx1)
+    a, b = node.mps[idx1 - 1], node.mps[idx1]
+    node.mps[idx1 - 1] = rs(np.einsum("ijk,kab->ijab", a, b), a.shape[0], a.shape[1] * b.shape[1], b.shape[2])
+    del node.mps[idx1]
+    M.cano_to(node, idx1)
+    return err
+
+
 def braket_lognorm(bk):
     """(braket.jl:915-940)"""
     total = 0.0
@@ -254,16 +285,35 @@ def contraction(bk):
         for t in ni.mps:
             bk.maxdim_intermediate = max(bk.maxdim_intermediate, t.shape[1])
         bk.edges = [(a, b) for (a, b) in bk.edges if not ((a, b) == (i, j) or (a, b) == (j, i))]
-        new = []
+        new, dups = [], []
         for (a, b) in bk.edges:
             if a == j or b == j:
                 other = b if a == j else a
                 on = bk.tensors[other]
+                xk, yk = find_leg(on, i, True), find_leg(on, j, True)
+                xb, yb = find_leg(on, i, False), find_leg(on, j, False)
                 on.neighbor = [i if v == j else v for v in on.neighbor]
+                if xk > 0:   # a second doubled bond between i and other (loops only)
+                    dups.append((other, xk > yk, xb > yb))
+                    continue
                 new.append((i, other) if a == j else (other, i))
             else:
                 new.append((a, b))
         bk.edges = new
+        if dups and not bk.loops:
+            raise ValueError("contraction!: parallel doubled bonds in a network built without loops")
+        for (k, ck, cb) in dups:
+            nk = bk.tensors[k]
+            err += merge_leg(nk, i, True, ck)
+            err += merge_leg(nk, i, False, cb)
+            err += merge_leg(ni, k, True, False)
+            err += merge_leg(ni, k, False, False)
+            for t in nk.mps:
+                bk.maxdim_intermediate = max(bk.maxdim_intermediate, t.shape[1])
+        if dups:
+            err += M.compress_opt(ni) if bk.svdopt else M.compress(ni)
+            for t in ni.mps:
+                bk.maxdim_intermediate = max(bk.maxdim_intermediate, t.shape[1])
         if TRACE is not None:
             TRACE.append((i, j, tuple(M.shape(ni)), tuple(int(x) for x in ni.layer)))
         del bk.tensors[j]

@@ -53,6 +53,7 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   // CATN_HOSTCHECK_BLOCKED_QR_MIN: the same for the blocked, norm-sorted QR
   jl.blocked_qr_min_n = 1 << 30;
   if (const char* eq = std::getenv("CATN_HOSTCHECK_BLOCKED_QR_MIN")) jl.blocked_qr_min_n = std::atoi(eq);
+  jl.cta_jobs = 1;
   run_instance(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
                sws_doubles, &jl);
   if (trace && im.desc[0].trace_cap > 0)

@@ -94,6 +94,41 @@ def test_oracle_rejects_cycles_and_bad_labels():
         B.braket_network([r.normal(size=(2, 2)), r.normal(size=(2, 2))], [["a", "b"], ["a", "b"]])
 
 
+def loopy_states(seed):
+    """Cyclic virtual-bond graphs: a triangle and open PEPS (L_x x L_y, bond D,
+    physical 2), the loopy extension's test shapes (the reference rejects
+    them, test/test_braket.jl:340-345)."""
+    r = np.random.default_rng(seed)
+    out = [([r.normal(size=(2, 2, 2)) for _ in range(3)], [["a", "c", "p1"], ["a", "b", "p2"], ["b", "c", "p3"]])]
+    for (lx, ly, D) in [(2, 2, 2), (2, 3, 2), (3, 3, 2), (3, 3, 3), (4, 3, 2)]:
+        ts, ixs = [], []
+        for y in range(ly):
+            for x in range(lx):
+                ix = ([f"h{x - 1}_{y}"] if x > 0 else []) + ([f"h{x}_{y}"] if x < lx - 1 else []) + \
+                     ([f"v{x}_{y - 1}"] if y > 0 else []) + ([f"v{x}_{y}"] if y < ly - 1 else []) + [f"p{x}_{y}"]
+                ts.append(r.normal(size=[D] * (len(ix) - 1) + [2]))
+                ixs.append(ix)
+        out.append((ts, ixs))
+    return out
+
+
+@pytest.mark.parametrize("svdopt", [True, False])
+def test_oracle_loopy_norm_matches_exact(svdopt):
+    """Loopy extension in exact mode: <psi|psi> of triangles and PEPS against
+    the dense norm, at the reference's own tolerance."""
+    for ts, ixs in loopy_states(41):
+        lz, err, psi, tr, _ = oracle_run(ts, ixs, chi=10_000, svdopt=svdopt, loops=True)
+        assert np.exp(lz) * psi == pytest.approx(B.exact_norm(ts, ixs), rel=1e-10)
+        assert any(len(t) == 4 for t in tr)
+
+
+def test_loopy_rejections():
+    r = np.random.default_rng(9)
+    with pytest.raises(ValueError, match="parallel"):
+        B.braket_network([r.normal(size=(2, 2, 2)), r.normal(size=(2, 2, 2))], [["a", "b", "p1"], ["a", "b", "p2"]],
+                         loops=True)
+
+
 @pytest.fixture(scope="module")
 def host():
     return ct.CDLL(hostbuild.build())
@@ -135,6 +170,52 @@ def test_host_engine_matches_oracle(host, kw):
         assert res.maxdim == bk.maxdim_intermediate
 
 
+LOOPY_KW = [dict(chi=10_000), dict(chi=10_000, svdopt=False), dict(chi=4), dict(chi=3, norm_method=2)]
+
+
+def _loopy_check(lz, err, psi, tr, bk, dlz, derr, dpsi, dtr, maxdim, exact=None):
+    assert [(int(a), int(b)) for a, b in dtr[:, :2]] == [(t[0], t[1]) for t in tr]
+    assert abs(dlz - lz) <= 1e-10 * max(1.0, abs(lz))
+    assert abs(derr - err) <= 1e-10 + 1e-8 * abs(err)
+    assert dpsi == psi
+    assert maxdim == bk.maxdim_intermediate
+    if exact is not None:
+        assert np.exp(dlz) * dpsi == pytest.approx(exact, rel=1e-10)
+
+
+@pytest.mark.parametrize("kw", LOOPY_KW)
+def test_host_engine_loopy_matches_oracle(host, kw):
+    """Loopy extension: the engine compiled for the host against the oracle's
+    restatement, edge order and fused-bond dims included (trace column 4
+    counts the fusions of a step)."""
+    fused = 0
+    for ts, ixs in loopy_states(43):
+        lz, err, psi, tr, bk = oracle_run(ts, ixs, loops=True, **kw)
+        st, res, dtr = host_run(host, ts, ixs, braket_loops=True, **kw)
+        assert st == 0
+        _loopy_check(lz, err, psi, tr, bk, res.lnZ, res.err, res.psi, dtr, res.maxdim,
+                     B.exact_norm(ts, ixs) if kw["chi"] > 100 else None)
+        fused += int(dtr[:, 4].sum())
+    assert fused > 0
+
+
+def test_host_engine_rejects_cycles_without_loops(host):
+    ts, ixs = loopy_states(44)[1]
+    st, _, _ = host_run(host, ts, ixs, chi=100)
+    assert st == L.CATN_EINVAL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kw", LOOPY_KW)
+def test_gpu_loopy_braket_matches_oracle(catn, kw):
+    for ts, ixs in loopy_states(45):
+        lz, err, psi, tr, bk = oracle_run(ts, ixs, loops=True, **kw)
+        net = catn.braket_network(ts, ixs, loops=True, **kw)
+        dlz, derr, dpsi = catn.contraction(net, trace=True)
+        _loopy_check(lz, err, psi, tr, bk, dlz, derr, dpsi, net.trace, net.maxdim_intermediate,
+                     B.exact_norm(ts, ixs) if kw["chi"] > 100 else None)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("kw", [dict(chi=10_000), dict(chi=10_000, svdopt=False), dict(chi=2)])
 def test_gpu_braket_matches_oracle_and_exact(catn, kw):
@@ -158,3 +239,6 @@ def test_gpu_braket_rejections(catn):
         catn.braket_network([r.normal(size=(2, 2, 2))] * 3, [["a", "c", "p1"], ["a", "b", "p2"], ["b", "c", "p3"]])
     with pytest.raises(NotImplementedError):
         catn.braket_network([np.ones((2, 2), complex), np.ones((2, 2), complex)], [["p1", "a"], ["a", "p2"]])
+    with pytest.raises(ValueError, match="parallel"):
+        catn.braket_network([r.normal(size=(2, 2, 2)), r.normal(size=(2, 2, 2))], [["a", "b", "p1"], ["a", "b", "p2"]],
+                            loops=True)
