@@ -53,7 +53,7 @@ catn_status check_params(const catn_params* p) {
   if (p->norm_method < 0 || p->norm_method > 2) return fail(CATN_EINVAL, "norm_method must be 0, 1 or 2");
   if (p->select < 0 || p->select > 2) return fail(CATN_EINVAL, "select must be 0, 1 or 2");
   if (!(p->cutoff >= 0.0)) return fail(CATN_EINVAL, "cutoff must be >= 0");
-  if (p->rsvd < 0 || p->rsvd > 1) return fail(CATN_EINVAL, "rsvd must be 0 or 1");
+  if (p->rsvd < 0 || p->rsvd > 2) return fail(CATN_EINVAL, "rsvd must be 0, 1 or 2");
   if (p->rsvd_min_dim < 0) return fail(CATN_EINVAL, "rsvd_min_dim must be >= 0");
   if (p->precision < 0 || p->precision > 1) return fail(CATN_EINVAL, "precision must be 0 (FP64) or 1 (split)");
   if (p->svd_route < 0 || p->svd_route > 2) return fail(CATN_EINVAL, "svd_route must be 0, 1 or 2");

@@ -920,6 +920,89 @@ CATN_HDI inline Svd rsvd_swap(Ctx& C, const SvdIn& in, long long m, long long n,
   return R;
 }
 
+// Matrix-free products with the swap matrix M = reshape(ein"ijk,kab->iajb"(tl,
+// tr), d0 d1, d2 d3) (tl: d0 x d2 x kk, tr: kk x d1 x d3, column-major), M
+// never formed: M[(i,a), (j,b)] = sum_k tl[i,j,k] tr[k,a,b], rows i + d0 a,
+// columns j + d2 b.  X is (d0 kk d3 p) doubles of workspace.
+// Y (m x p) = M G, G (n x p): X[(i,k), (b,c)] = sum_j tl[i,j,k] G[(j,b), c],
+// then Y[(i,a), c] = sum_(k,b) X[(i,k), (b,c)] tr[k,a,b].
+CATN_HDI inline void mf_apply(const Team& T, const double* tl, const double* tr, long long d0, long long d1,
+                              long long d2, long long d3, long long kk, const double* G, long long p, double* X,
+                              double* Y) {
+  const long long m = d0 * d1, n = d2 * d3;
+  gemm(T, d0 * kk, d3 * p, d2, mop((double*)tl, imap((int)d0, 1, d0 * d2), imap(1, 0, d0)),
+       mop((double*)G, rows_plain(), imap((int)d3, d2, n)), colmajor(X, d0 * kk));
+  gemm(T, d0 * p, d1, kk * d3, mop(X, imap((int)d0, 1, d0 * kk * d3), imap((int)kk, d0, d0 * kk)),
+       mop((double*)tr, imap((int)kk, 1, kk * d1), imap(1, 0, kk)), mop(Y, imap((int)d0, 1, m), imap(1, 0, d0)));
+}
+// Z (n x p) = M^T Y, Y (m x p): X[(i,c), (k,b)] = sum_a Y[(i,a), c] tr[k,a,b],
+// then Z[(j,b), c] = sum_(i,k) tl[i,j,k] X[(i,c), (k,b)].
+CATN_HDI inline void mf_apply_t(const Team& T, const double* tl, const double* tr, long long d0, long long d1,
+                                long long d2, long long d3, long long kk, const double* Y, long long p, double* X,
+                                double* Z) {
+  const long long m = d0 * d1, n = d2 * d3;
+  gemm(T, d0 * p, kk * d3, d1, mop((double*)Y, imap((int)d0, 1, m), imap(1, 0, d0)),
+       mop((double*)tr, imap(1, 0, kk), imap((int)kk, 1, kk * d1)), colmajor(X, d0 * p));
+  gemm(T, d2, d3 * p, d0 * kk, mop((double*)tl, imap(1, 0, d0), imap((int)d0, 1, d0 * d2)),
+       mop(X, imap((int)d0, 1, d0 * p), imap((int)d3, d0 * p * kk, d0)), mop(Z, rows_plain(), imap((int)d3, d2, n)));
+}
+
+// rsvd_swap with the products of M applied from (tl, tr) (catn_params.rsvd
+// = 2): the same sketch, power iterations, thin Qs and projected SVD, for
+// swap matrices too large to hold (M of (chi Dmax)^2 doubles); B = Q^T M is
+// formed as (M^T Q)^T.  Its workspace is O((m + n + d0 kk d3) p).
+CATN_HDI inline Svd rsvd_swap_mf(Ctx& C, const double* tl, const double* tr, long long d0, long long d1, long long d2,
+                                 long long d3, long long kk, long long k) {
+  const Team& T = C.T;
+  const long long m = d0 * d1, n = d2 * d3;
+  Svd R;
+  R.m = m; R.n = n; R.p = 0; R.U = R.S = R.V = nullptr;
+  const long long p = n < 10 * k ? n : 10 * k;
+  double* G = spush(C, n * p);
+  double* Y = spush(C, m * p);
+  double* Z = spush(C, n * p);
+  double* Qm = spush(C, m * p);
+  double* tau = spush(C, p);
+  double* X = spush(C, d0 * kk * d3 * p);
+  if (failed(C)) return R;
+  const unsigned long long key = (unsigned long long)(unsigned)C.P.seed;
+  const unsigned long long stream = 16ULL + (unsigned long long)C.rsvd_calls;
+  C.rsvd_calls += 1;   // every thread keeps the same count
+  for (long long e = T.rank(); e < n * p; e += T.size()) G[e] = disorder_normal(key, stream, (unsigned long long)e);
+  T.sync();
+  mf_apply(T, tl, tr, d0, d1, d2, d3, kk, G, p, X, Y);
+  for (int it = 0; it < 10; ++it) {
+    mf_apply_t(T, tl, tr, d0, d1, d2, d3, kk, Y, p, X, Z);   // Z = M^T Y
+    mf_apply(T, tl, tr, d0, d1, d2, d3, kk, Z, p, X, Y);     // Y = M Z
+    if (!thin_q(C, Y, m, p, tau, Qm)) return R;
+    copy(T, Y, Qm, m * p);
+  }
+  if (!thin_q(C, Y, m, p, tau, Qm)) return R;              // Q (m x p)
+  mf_apply_t(T, tl, tr, d0, d1, d2, d3, kk, Qm, p, X, Z);   // Z = M^T Q (n x p)
+  SvdIn bin = svd_begin(C, p, n, 0.0);
+  if (failed(C)) return R;
+  {
+    const MOp Bt = svd_target(bin);   // B (p x n) = Z^T
+    for (long long e = T.rank(); e < p * n; e += T.size()) {
+      long long r, c;
+      divmod(e, p, &r, &c);
+      Bt.ref(r, c) = Z[c + n * r];
+    }
+    T.sync();
+  }
+  Svd F = svd_finish(C, bin);
+  if (failed(C) || !F.U) return R;
+  const long long kq = F.p < k ? F.p : k;
+  double* U = spush(C, m * kq);
+  if (failed(C)) return R;
+  gemm(T, m, kq, p, colmajor(Qm, m), colmajor(F.U, p), colmajor(U, m));
+  R.p = kq;
+  R.U = U;
+  R.S = F.S;
+  R.V = F.V;
+  return R;
+}
+
 // swap! (mps_node.jl:126-178)
 // ---------------------------------------------------------------------------
 CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
@@ -946,13 +1029,18 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   const bool rsvd_route = C.P.swapopt && ((m > rmin && n > rmin) || m > rbig || n > rbig);
   // the reference's randomized algorithm on request (forward runs, sketch no
   // wider than M); otherwise the exact top-chi subspace it approximates
-  const bool randomized = rsvd_route && C.P.rsvd == 1 && !C.tape && m >= (n < 10LL * C.P.chi ? n : 10LL * C.P.chi);
-  SvdIn in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);
-  if (failed(C)) return 0.0;
-  in.need = C.P.chi;   // keep_rule and the randomized route keep at most chi
+  const bool randomized = rsvd_route && C.P.rsvd >= 1 && !C.tape && m >= (n < 10LL * C.P.chi ? n : 10LL * C.P.chi);
+  // rsvd = 2: the same algorithm with M applied from (tl, tr), never formed
+  const bool matfree = randomized && C.P.rsvd == 2;
+  SvdIn in = SvdIn();
+  if (!matfree) {
+    in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);
+    if (failed(C)) return 0.0;
+    in.need = C.P.chi;   // keep_rule and the randomized route keep at most chi
+  }
   // W = ein"ijk,kab->iajb"(tl, tr); M = reshape(W, d0*d1, d2*d3), written
   // straight into the SVD's oriented input.
-  {
+  if (!matfree) {
     const long long tg = clk();
     MOp out = in.wide ? mop(in.W, imap((int)d0, n, 1), imap((int)d1, n * d0, d2))
                       : mop(in.W, imap((int)d0, 1, d0 * d1), imap((int)d1, d0, d0 * d1 * d2));
@@ -960,7 +1048,9 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
       gemm(T, d0 * d2, d1 * d3, kk, colmajor(sdata(C, tl), d0 * d2), colmajor(sdata(C, tr), kk), out);
     prof_add(C, PROF_SWAP_GEMM, (double)(clk() - tg));
   }
-  Svd R = randomized ? rsvd_swap(C, in, m, n, C.P.chi) : svd_finish(C, in);
+  Svd R = matfree      ? rsvd_swap_mf(C, sdata(C, tl), sdata(C, tr), d0, d1, d2, d3, kk, C.P.chi)
+          : randomized ? rsvd_swap(C, in, m, n, C.P.chi)
+                       : svd_finish(C, in);
   if (failed(C)) return 0.0;
   const long long te = clk();
   double err = 0.0;

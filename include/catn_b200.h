@@ -61,7 +61,10 @@ typedef struct {
                         * (linalg_utils.jl:44-58: sketch of min(n, 10 chi)
                         * columns, 10 power iterations), its Gaussian sketch
                         * drawn from the counter-based generator keyed by
-                        * seed (forward runs; gradient runs use 0)          */
+                        * seed (forward runs; gradient runs use 0); 2 = the
+                        * same with the products of the swap matrix applied
+                        * from the two sites (matrix-free: the (d0 d1) x
+                        * (d2 d3) matrix is never formed)                 */
   /* Fields below have no counterpart in the reference's keywords. */
   int32_t rsvd_min_dim; /* > 0: the randomized route above takes swap!
                         * matrices with both sides >= rsvd_min_dim or one

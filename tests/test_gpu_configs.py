@@ -103,6 +103,27 @@ def test_peps_norm_exact(catn, L):
     assert np.exp(lnZ) * psi == pytest.approx(ref, rel=1e-10)
 
 
+def test_peps_norm_matrix_free_randomized_swaps(catn, monkeypatch):
+    """The fused double-layer PEPS norm with every large swap on the
+    randomized route, matrix-free (rsvd = 2: the swap matrix applied from
+    the two sites), against the oracle running the reference's randomized
+    SVD on the formed matrix with the same sketch; the route's threshold is
+    lowered to 12 so that a 4 x 4 PEPS reaches it (16 randomized swaps)."""
+    from catn_b200 import graphs
+    from oracle import mps as OM
+    monkeypatch.setattr(OM, "RSVD_MIN", 12)
+    monkeypatch.setattr(OM, "RSVD_SKETCH_SEED", 5)
+    monkeypatch.setattr(OM, "RSVD_CALLS", 0)
+    _, _, et, ei = graphs.peps_double_layer(4, 2, 2, np.random.default_rng(300))
+    (lz, err, psi), orows, tn = oracle_trace(lambda: ON.TensorNetwork.from_tensors(et, ei, Dmax=16, chi=8))
+    assert OM.RSVD_CALLS > 0
+    net = catn.TensorNetwork(et, ei, Dmax=16, chi=8, rsvd=2, rsvd_min_dim=12, seed=5)
+    dlz, derr, dpsi = catn.contraction(net, trace=True)
+    assert [tuple(int(x) for x in row[:7]) for row in net.trace] == orows
+    assert abs(dlz - lz) <= 1e-10 * max(1.0, abs(lz))
+    assert dpsi == psi
+
+
 @pytest.mark.parametrize("L,D,Dmax,chi", [(4, 2, 8, 16), (5, 2, 8, 16), (4, 3, 16, 32)])
 def test_peps_norm_truncated_matches_oracle(catn, L, D, Dmax, chi):
     from catn_b200 import graphs

@@ -2,7 +2,9 @@
 linalg_utils.jl:44-58) with a reproducible sketch (catn_params.rsvd = 1):
 the engine draws the Gaussian sketch from its counter-based generator
 keyed by (seed, call index), and the oracle, given the same sketch, runs the
-reference's algorithm.  The route's size threshold is lowered through
+reference's algorithm.  With catn_params.rsvd = 2 the engine runs the same
+algorithm matrix-free: the products with the swap matrix are applied from
+the two sites, the matrix itself is never formed.  The route's size threshold is lowered through
 catn_params.rsvd_min_dim (engine) and RSVD_MIN (oracle) so that small
 networks reach it; the default thresholds are the reference's 7000 / 20000.
 
@@ -70,27 +72,29 @@ def test_oracle_sketched_rsvd_is_exact_with_a_full_sketch():
     np.testing.assert_allclose(np.abs(U.T @ U), np.eye(5), atol=1e-12)
 
 
+@pytest.mark.parametrize("mode", [1, 2], ids=["formed", "matrix_free"])
 @pytest.mark.parametrize("name,L,kw,rmin", CASES, ids=[c[0] for c in CASES])
-def test_host_engine_matches_oracle(monkeypatch, name, L, kw, rmin):
+def test_host_engine_matches_oracle(monkeypatch, name, L, kw, rmin, mode):
     route(monkeypatch, rmin)
     lib = ct.CDLL(hostbuild.build())
     n, e, w, h, beta = instance(L, 7)
     lz, rows, calls = oracle_run(n, e, w, h, beta, kw)
     assert calls > 0   # the route was taken
-    st, res, drows = run_ising(lib, n, e, w, h, beta, rsvd=1, rsvd_min_dim=rmin, seed=3, **kw)
+    st, res, drows = run_ising(lib, n, e, w, h, beta, rsvd=mode, rsvd_min_dim=rmin, seed=3, **kw)
     assert st == 0
     assert drows == rows
     assert abs(res.lnZ - lz) / n <= 1e-10
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mode", [1, 2], ids=["formed", "matrix_free"])
 @pytest.mark.parametrize("name,L,kw,rmin", CASES, ids=[c[0] for c in CASES])
-def test_gpu_matches_oracle(monkeypatch, catn, name, L, kw, rmin):
+def test_gpu_matches_oracle(monkeypatch, catn, name, L, kw, rmin, mode):
     route(monkeypatch, rmin)
     n, e, w, h, beta = instance(L, 7)
     lz, rows, calls = oracle_run(n, e, w, h, beta, kw)
     assert calls > 0
-    tn = catn.ising_network(n, e, w, h, beta, rsvd=1, rsvd_min_dim=rmin, seed=3, **kw)
+    tn = catn.ising_network(n, e, w, h, beta, rsvd=mode, rsvd_min_dim=rmin, seed=3, **kw)
     dlz, err, psi = catn.contraction(tn, trace=True)
     drows = [tuple(int(x) for x in r[:7]) for r in tn.trace]
     assert drows == rows
