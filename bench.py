@@ -272,8 +272,10 @@ def main():
                     help="time budget of the plain GPU form sample (0 = skip)")
     ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
     ap.add_argument("--no-c2", action="store_true", help="skip the n=200 random-regular leg")
-    ap.add_argument("--c2-oracle", action="store_true",
-                    help="also time the FP64 oracle on one beta of the n=200 random-regular leg (~40 s)")
+    ap.add_argument("--c2-scalar", action="store_true",
+                    help="also time the n=200 leg on the scalar Jacobi route (about 40 s per beta)")
+    ap.add_argument("--no-c2-oracle", action="store_true",
+                    help="skip timing the FP64 oracle on beta = 1 of the n=200 random-regular leg (~25 s)")
     ap.add_argument("--arena-mb", type=int, default=64, help="device arena per slot, MiB")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -474,9 +476,10 @@ def _oracle_rrg200(beta):
 def c2_leg(catn, args):
     """The n=200 random 3-regular +-1 spin glass (300 edges, h ~ N(0, 0.1^2),
     beta in {0.5, 1, 1.5}, Dmax 32, chi 128), one network per beta through
-    the public API (host image in, results out), in three forms: FP64 on the
-    scalar Jacobi route, FP64 on the block Jacobi route, and the split
-    precision form (3xTF32 tensor-core products, block route).  Errors are
+    the public API (host image in, results out), in two forms: FP64 on the
+    block Jacobi route and the split precision form (3xTF32 tensor-core
+    products, block route); with --c2-scalar also FP64 on the scalar Jacobi
+    route.  The FP64 oracle is timed on beta = 1 on the host cores.  Errors are
     against the FP64 oracle's values frozen in tests/golden/rrg200.json (made
     by tests/golden/make_golden.py); the trace must equal the oracle's."""
     d = json.load(open(os.path.join(ROOT, "tests", "golden", "rrg200.json")))
@@ -486,8 +489,8 @@ def c2_leg(catn, args):
            "timing": "host wall clock around catn.contraction (device move done before; the launch and the "
                      "result read-back inside)",
            "forms": {}}
-    forms = [("fp64_scalar", dict(svd_route="scalar"), [1.0]),
-             ("fp64_block", dict(svd_route="block"), d["betas"]),
+    forms = ([("fp64_scalar", dict(svd_route="scalar"), [1.0])] if args.c2_scalar else []) + \
+            [("fp64_block", dict(svd_route="block"), d["betas"]),
              ("split", dict(svd_route="block", precision="split"), d["betas"])]
     for name, kw, betas in forms:
         per = []
@@ -505,11 +508,14 @@ def c2_leg(catn, args):
         res["forms"][name] = {"s_per_beta": round(sum(p["s"] for p in per) / len(per), 3),
                               "max_abs_dlnZ_per_spin": max(p["abs_dlnZ_per_spin"] for p in per),
                               "traces_identical": all(p["trace_identical"] for p in per), "runs": per}
-    if args.c2_oracle:
+    if not args.no_c2_oracle:
         with mp.get_context("spawn").Pool(1) as pool:
             lz, secs = pool.apply(_oracle_rrg200, (1.0,))
         res["oracle_fp64_cpu"] = {"beta": 1.0, "s": round(secs, 3), "cores": host_cores(),
-                                  "what": "the oracle port (numpy/OpenBLAS, all cores to BLAS)"}
+                                  "what": "the oracle port (numpy/OpenBLAS, all cores to BLAS), same network"}
+        b1 = [p["s"] for p in res["forms"]["fp64_block"]["runs"] if p["beta"] == 1.0]
+        if b1:
+            res["fp64_block_speedup_vs_oracle_at_beta_1"] = round(secs / b1[0], 2)
     return res
 
 
