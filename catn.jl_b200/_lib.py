@@ -57,6 +57,7 @@ SIGNATURES = {
     "catn_net_create_dense": ([ct.POINTER(Params), ct.c_int32, _P, _P, _P, _P, ct.c_int64,
                                ct.POINTER(ct.c_void_p)], ct.c_int),
     "catn_contract": ([ct.c_void_p, ct.POINTER(Result), _P, ct.c_int32], ct.c_int),
+    "catn_cut_bondim": ([ct.c_void_p, ct.c_int32, ct.c_int32, ct.c_int32, ct.POINTER(ct.c_double)], ct.c_int),
     "catn_result_tensor": ([ct.c_void_p, _P, ct.c_int64, ct.POINTER(ct.c_int64),
                             ct.POINTER(ct.c_int32), _P], ct.c_int),
     "catn_net_destroy": ([ct.c_void_p], ct.c_int),

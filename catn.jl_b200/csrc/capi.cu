@@ -405,7 +405,8 @@ static catn_status net_finish(catn_net* net, long long arena_bytes, catn_net** o
     delete net;
     return fail(CATN_EINVAL, "no instances");
   }
-  catn_status s = prepare(net->im, default_arena(arena_bytes, net->im.desc[0].P), 1, net->R);
+  net->arena = default_arena(arena_bytes, net->im.desc[0].P);
+  catn_status s = prepare(net->im, net->arena, 1, net->R);
   if (s != CATN_OK) {
     net->R.release();
     delete net;
@@ -490,6 +491,62 @@ catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32
     if (cnt > 0) CUDA_TRY(cudaMemcpy(trace, net->R.d_trace, sizeof(int) * 8 * cnt, cudaMemcpyDeviceToHost));
   }
   if (res->status != CATN_OK) return fail((catn_status)res->status, std::string("contraction failed: ") + status_text(res->status));
+  return CATN_OK;
+}
+
+catn_status catn_cut_bondim(catn_net* net, int32_t i, int32_t idx_j_in_i, int32_t opt, double* err) {
+  if (!net || !err) return fail(CATN_EINVAL, "NULL argument");
+  *err = 0.0;
+  if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
+  const InstDesc& D0 = net->im.desc[0];
+  if (D0.kind == 2) return fail(CATN_EINVAL, "cut_bondim!: BraKet networks have no bond cuts");
+  if (D0.P.Dmax < 0) return CATN_OK;   // tensor_network.jl:344 (and :401): a no-op returning 0.0
+  const char* name = opt ? "cut_bondim_opt!" : "cut_bondim!";
+  if (i < 1 || i > D0.n) return fail(CATN_EINVAL, std::string(name) + ": node id out of range");
+  const std::vector<int> nbi = net->im.neighbors_of(i);
+  if (idx_j_in_i < 1 || idx_j_in_i > (int)nbi.size()) return fail(CATN_EINVAL, std::string(name) + ": leg out of range");
+  const int j = nbi[idx_j_in_i - 1];
+  if (j <= 0)
+    return fail(CATN_ESTATE, std::string(name) + ": leg " + std::to_string(idx_j_in_i) + " of node " +
+                                 std::to_string(i) + " is an open leg (no neighbor)");
+  const std::vector<int> nbj = net->im.neighbors_of(j);
+  if (std::find(nbj.begin(), nbj.end(), i) == nbj.end())
+    return fail(CATN_ESTATE, std::string(name) + ": node " + std::to_string(i) + " not found as neighbor of node " +
+                                 std::to_string(j));
+  // The network's state is its image plus the cuts so far: the launch loads
+  // the image, replays every cut in order and stops after the new one.
+  std::vector<int> cuts = net->cuts;
+  cuts.push_back(i);
+  cuts.push_back(idx_j_in_i);
+  cuts.push_back(opt ? 1 : 0);
+  net->im.set_cuts(cuts);
+  net->im.desc[0].cut_only = 1;
+  net->R.release();
+  catn_status s = prepare(net->im, net->arena, 1, net->R);
+  net->im.desc[0].cut_only = 0;
+  if (s != CATN_OK) {
+    net->im.set_cuts(net->cuts);
+    net->R.release();
+    if (prepare(net->im, net->arena, 1, net->R) != CATN_OK) net->contracted = true;   // unusable from here
+    return s;
+  }
+  cudaStream_t st = 0;
+  catn_result res;
+  std::memset(&res, 0, sizeof(res));
+  if ((s = upload(net->R, st)) == CATN_OK && (s = launch(net->R, st)) == CATN_OK) {
+    CUDA_TRY(cudaMemcpyAsync(&res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  // the host copy of the image goes back to contraction launches
+  ((InstDesc*)net->R.h_input)[0].cut_only = 0;
+  if (s != CATN_OK) return s;
+  if (res.status != CATN_OK) {
+    net->im.set_cuts(net->cuts);
+    std::memcpy(net->R.h_input, net->im.desc.data(), sizeof(InstDesc));
+    return fail((catn_status)res.status, std::string(name) + " failed: " + status_text(res.status));
+  }
+  net->cuts = cuts;
+  *err = res.err;
   return CATN_OK;
 }
 

@@ -158,6 +158,7 @@ catn_status catn_ising_grad(catn_net* net, catn_result* res, double* dlnZ_dw, do
     return fail(CATN_EINVAL, "NULL argument");
   if (ckpt_interval < 0) return fail(CATN_EINVAL, "ckpt_interval must be >= 0");
   if (catn_status s = check_ising_only(net->im)) return s;
+  if (!net->cuts.empty()) return fail(CATN_EINVAL, "gradients of a network with cut_bondim! calls are not taped");
   if (catn_status s = grad_prepare(net->im, net->grad ? net->grad->arena : grad_arena(net->R.L.arena_bytes, 1), 1,
                                       net->grad)) return s;
   // this call's interval, in the uploaded instance descriptor

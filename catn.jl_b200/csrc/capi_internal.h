@@ -115,6 +115,8 @@ catn_status braket_launch(DeviceRun& R, cudaStream_t st);
 struct catn_net {
   catn::Image im;
   catn_capi::DeviceRun R;
+  long long arena = 0;      // arena bytes of the slot (after defaults)
+  std::vector<int> cuts;    // cut_bondim! calls so far: i, idx_j_in_i, opt
   bool contracted = false;
   catn_capi::GradRun* grad = nullptr;
 };

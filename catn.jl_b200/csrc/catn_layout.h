@@ -63,7 +63,10 @@ struct InstDesc {
   long long trace_off; // int32 offset into the trace buffer
   long long edge_off;  // BraKet (kind 2): int32 image, edge pairs in processing order
   int n_edges;
-  int pad3;
+  int n_cuts;          // cut_bondim! calls before the contraction (kinds 0, 1)
+  long long cut_off;   // int32 image: 3 words per call (i, idx_j_in_i, opt)
+  int cut_only;        // 1: stop after the cuts (the error of the last one)
+  int pad4;
 };
 
 // Byte layout of one CTA slot (control state + arena).

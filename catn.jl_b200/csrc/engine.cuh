@@ -1549,18 +1549,36 @@ CATN_HDI inline double compress_node(Ctx& C, int k, bool opt) {
   return err;
 }
 
+// The matrix itself as a QRed without reduction (cut_bondim!).
+CATN_HDI inline QRed qr_none(double* X, long long rows, long long cols) {
+  QRed q;
+  q.rows = rows;
+  q.cols = cols;
+  q.house = X;
+  q.tau = nullptr;
+  q.flag = false;
+  q.Rb = X;
+  q.rrows = rows;
+  return q;
+}
+
 // ---------------------------------------------------------------------------
-// cut_bondim_opt! (tensor_network.jl:399-477).  Returns the discarded sum.
+// cut_bondim_opt! (tensor_network.jl:399-477) with `opt`, cut_bondim!
+// (tensor_network.jl:342-388) without: the plain cut neither canonicalises
+// the two nodes nor pre-reduces the two matrices by QR, so its SVD takes the
+// whole (da_l da_r) x (db_l db_r) product.  Returns the discarded sum.
 // ---------------------------------------------------------------------------
-CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
+CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i, bool opt = true) {
   const Team& T = C.T;
   if (C.P.Dmax < 0) return 0.0;
   int j = nbref(C, i, idx_j_in_i);
   if (j <= 0) { fail_all(C, CATN_ESTATE); return 0.0; }
   int idx_i_in_j = nb_find(C, j, i);
   if (idx_i_in_j == 0) { fail_all(C, CATN_ESTATE); return 0.0; }
-  cano_to(C, i, idx_j_in_i);
-  cano_to(C, j, idx_i_in_j);
+  if (opt) {
+    cano_to(C, i, idx_j_in_i);
+    cano_to(C, j, idx_i_in_j);
+  }
   if (failed(C)) return 0.0;
   const long long tcut = clk();
   const long long mark = C.sp;
@@ -1573,8 +1591,8 @@ CATN_HDI inline double cut_bond(Ctx& C, int i, int idx_j_in_i) {
   if (failed(C)) return 0.0;
   materialize(T, mi, ri_rows, d, ri_rows, mop(sdata(C, Ai), imap(Ai.dl, 1, (long long)Ai.dl * d), cols_plain(Ai.dl)));
   materialize(T, mj, rj_rows, d, rj_rows, mop(sdata(C, Aj), imap(Aj.dl, 1, (long long)Aj.dl * d), cols_plain(Aj.dl)));
-  QRed qi = qr_reduce(C, mi, ri_rows, d);
-  QRed qj = qr_reduce(C, mj, rj_rows, d);
+  QRed qi = opt ? qr_reduce(C, mi, ri_rows, d) : qr_none(mi, ri_rows, d);
+  QRed qj = opt ? qr_reduce(C, mj, rj_rows, d) : qr_none(mj, rj_rows, d);
   if (failed(C)) return 0.0;
   SvdIn in = svd_begin(C, qi.rrows, qj.rrows, C.P.cutoff);
   if (failed(C)) return 0.0;
@@ -2367,8 +2385,18 @@ CATN_HDI inline void run_instance(const Team& T, char* slot, const SlotLayout& L
   load_instance(C, D, i64, i32, dat);
   ContractOut O;
   O.lnZ = 0.0; O.err = 0.0; O.psi = 1.0; O.sign = 1.0; O.maxdim = -1; O.nsteps = 0;
+  // cut_bondim! / cut_bondim_opt! calls made on the network before its
+  // contraction, replayed in order (i, idx_j_in_i, opt per call); with
+  // cut_only the instance stops after them and reports the discarded sum of
+  // the last one as its error.
+  double cut_err = 0.0;
+  for (int q = 0; q < D.n_cuts && !failed(C); ++q) {
+    const int* c = i32 + D.cut_off + 3LL * q;
+    cut_err = cut_bond(C, c[0], c[1], c[2] != 0);
+  }
   const long long t0 = clk();
-  if (!failed(C)) O = contract(C);
+  if (D.cut_only) O.err = cut_err;
+  else if (!failed(C)) O = contract(C);
   prof_add(C, PROF_TOTAL, (double)(clk() - t0));
   T.sync();
   if (T.leader()) {

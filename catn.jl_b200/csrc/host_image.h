@@ -431,6 +431,30 @@ struct Image {
     return err;
   }
 
+  // Neighbour list of node k (1-based) of the first instance, from the
+  // image (MPS and dense forms; empty for BraKet images or a bad k).
+  std::vector<int> neighbors_of(int k) const {
+    std::vector<int> out;
+    if (desc.empty() || desc[0].kind == 2 || k < 1 || k > desc[0].n) return out;
+    const InstDesc& D = desc[0];
+    const int col = D.kind == 0 ? 1 : 0;   // MPS: nnbr is word 1; dense: ndims (word 0)
+    long long off = D.nbr_off;
+    for (int q = 1; q < k; ++q) off += i64[D.hdr_off + 4 * (q - 1) + col];
+    const long long nn = i64[D.hdr_off + 4 * (k - 1) + col];
+    for (long long p = 0; p < nn; ++p) out.push_back(i32[off + p]);
+    return out;
+  }
+
+  // The cut_bondim! calls (3 words each: i, idx_j_in_i, opt) replayed before
+  // the first instance's contraction, kept at the end of the int32 image.
+  void set_cuts(const std::vector<int>& cuts) {
+    InstDesc& D = desc[0];
+    if (D.n_cuts > 0) i32.resize((size_t)D.cut_off);
+    D.cut_off = (long long)i32.size();
+    D.n_cuts = (int)(cuts.size() / 3);
+    i32.insert(i32.end(), cuts.begin(), cuts.end());
+  }
+
  private:
   void finish(InstDesc& D, int n, int edges, int trace_cap) {
     // the randomized-SVD route's size threshold (0: the reference's)

@@ -154,6 +154,33 @@ def contraction(tn, trace=False, arena_bytes=0):
     return res.lnZ, res.err, res.psi
 
 
+def _cut(tn, i, idx_j_in_i, opt):
+    if tn.result is not None:
+        raise ValueError("network already contracted (contraction! consumes tn)")
+    dev = tn._ensure_device()
+    lib = L.load()
+    err = ct.c_double()
+    L.check(lib, lib.catn_cut_bondim(dev.handle, int(i), int(idx_j_in_i), 1 if opt else 0, ct.byref(err)))
+    return err.value
+
+
+def cut_bondim(tn, i, idx_j_in_i):
+    """``cut_bondim!(tn, i, idx_j_in_i) -> error`` (tensor_network.jl:342-388):
+    truncate the bond between node ``i`` and its neighbour on leg
+    ``idx_j_in_i`` to ``Dmax`` singular values of the plain product of the
+    two bond sites (no canonicalisation, no QR pre-reduction), on the
+    device.  Returns the discarded singular-value sum; a later
+    ``contraction(tn)`` contracts the cut network."""
+    return _cut(tn, i, idx_j_in_i, False)
+
+
+def cut_bondim_opt(tn, i, idx_j_in_i):
+    """``cut_bondim_opt!(tn, i, idx_j_in_i) -> error``
+    (tensor_network.jl:399-477): the same cut after canonicalising both
+    nodes to the shared leg, with QR pre-reduction of both sides."""
+    return _cut(tn, i, idx_j_in_i, True)
+
+
 def result_tensor(tn):
     """``result_tensor(tn)`` (tensor_network.jl:517-523): dense tensor of the
     single surviving open-leg node (legs in its final MPS order); a 0-d one()

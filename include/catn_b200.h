@@ -198,6 +198,19 @@ catn_status catn_net_create_dense(const catn_params* p, int32_t n_nodes, const i
  *   fnv(phys dims of i), maxdim_intermediate. */
 catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32_t trace_cap);
 
+/* cut_bondim!(tn, i, idx_j_in_i) (src/tensor_network.jl:342-388) with
+ * opt = 0, cut_bondim_opt!(tn, i, idx_j_in_i) (src/tensor_network.jl:399-477)
+ * with opt != 0: truncates the bond between node i and its neighbour on leg
+ * idx_j_in_i to at most Dmax singular values (after the cutoff) and writes
+ * the discarded sum to *err.  Dmax < 0: a no-op with *err = 0, as in the
+ * reference.  The cut changes the network that a later catn_contract
+ * contracts; every cut runs on the device (the network's image is loaded
+ * and the cuts so far are replayed in order).  CATN_ESTATE for an open leg
+ * or a one-sided bond, as the reference's error() calls; CATN_EINVAL for a
+ * BraKet network, for ids out of range, and later for catn_ising_grad on a
+ * cut network. */
+catn_status catn_cut_bondim(catn_net* net, int32_t i, int32_t idx_j_in_i, int32_t opt, double* err);
+
 /* Shapes of the surviving nodes after contraction (result_tensor support,
  * src/tensor_network.jl:517-523): dense tensor of the single surviving
  * open-leg node, legs in its final MPS order.  `out` may be NULL to query

@@ -138,6 +138,20 @@ int catn_hostcheck_dense(const catn_params* p, int n, const int* ndims, const lo
   return run_image(im, arena_bytes, res, trace);
 }
 
+// A dense network with cut_bondim! calls (3 ints each: i, idx_j_in_i, opt)
+// replayed before the contraction; cut_only stops after the cuts (res->err:
+// the discarded sum of the last cut).
+int catn_hostcheck_dense_cuts(const catn_params* p, int n, const int* ndims, const long long* dims,
+                              const double* data, const int* neighbors, const int* cuts, int n_cuts, int cut_only,
+                              long long arena_bytes, catn_result* res, int* trace, int trace_cap) {
+  Image im;
+  std::string e = im.add_dense(*p, n, ndims, dims, data, neighbors, trace_cap);
+  if (!e.empty()) return CATN_EINVAL;
+  im.set_cuts(std::vector<int>(cuts, cuts + 3 * n_cuts));
+  im.desc[0].cut_only = cut_only;
+  return run_image(im, arena_bytes, res, trace);
+}
+
 // Ising site recipes (ising_build.cuh) checked on the host: the batch is
 // built from (w, h, betas) with recipes recorded, the recipes are evaluated
 // with (w2, h2, betas2), and the values are compared with a batch built
