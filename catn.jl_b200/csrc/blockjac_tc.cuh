@@ -44,6 +44,12 @@ __device__ __forceinline__ TcCtl* tc_ctl(const Team& T) { return (TcCtl*)(T.tcs 
 // Kernel prologue / epilogue: TMEM columns and the mbarrier.  Every thread
 // of the CTA calls both.
 __device__ inline void tc_setup(Team& T, unsigned char* region) {
+#if defined(CATN_NO_TCGEN05)
+  (void)region;
+  T.tcs = nullptr;
+  T.tmem = 0;
+  return;
+#endif
   T.tcs = region;
   TcCtl* c = tc_ctl(T);
   if (threadIdx.x == 0) {

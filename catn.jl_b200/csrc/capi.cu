@@ -16,6 +16,7 @@
 #include "engine.cuh"
 #include "host_image.h"
 #include "capi_internal.h"
+#include "persistent.cuh"
 
 using namespace catn;
 using namespace catn_capi;
@@ -81,55 +82,6 @@ namespace {
 constexpr int kSharedJacobiMinN = 128;
 constexpr int kHelperCtas = 16;
 
-// `order` lists instance ids by descending work estimate, so the longest
-// contractions start first (longest-processing-time scheduling).  With a job
-// board, the last `nhelp` CTAs and every CTA that finds the queue drained
-// help the large SVDs of the CTAs still contracting (help_jobs) until all are
-// finished.  With split-precision instances every CTA holds TMEM columns and
-// the tensor-core staging area for the block route's products.
-__global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
-    const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
-    const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, int* trace, int* queue,
-    JacobiJob* board, int nhelp, JobLink jl, int use_tc) {
-  extern __shared__ double smem[];
-  Team T;
-  T.red = smem;
-  T.stage = (char*)(smem + 64);
-  T.stage_bytes = GEMM_STAGE_BYTES;
-  T.tcs = nullptr;
-  T.tmem = 0;
-  if (use_tc) tc_setup(T, tc_region(smem));
-  double* sws = (double*)(T.stage + GEMM_STAGE_BYTES);
-  char* slot = slots + (long long)blockIdx.x * L.slot_bytes;
-  jl.job = board ? board + blockIdx.x : nullptr;
-  jl.qhead = queue;
-  const bool helper = board && (int)blockIdx.x >= (int)gridDim.x - nhelp;
-  for (;;) {
-    if (helper) break;
-    long long inst = 0;
-    if (threadIdx.x == 0) {
-      const int q = atomicAdd(queue, 1);
-      inst = q < ninst ? order[q] : ninst;
-    }
-    inst = T.bcast(inst);
-    if (inst >= ninst) break;
-    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles,
-                 board ? &jl : nullptr);
-    if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
-    // A shared wait that ran out leaves a helper warp that may still write
-    // into this slot's arena: the slot takes no further instance (the other
-    // CTAs drain the queue).
-    if (T.bcast(threadIdx.x == 0 ? res[inst].status : 0) == CATN_ETIMEOUT) break;
-  }
-  if (board) {
-    if (jl.cta_jobs)
-      help_jobs(T, board, (int)gridDim.x, queue + 1, ninst, sws);
-    else
-      help_jacobi(T, board, (int)gridDim.x, queue + 1, ninst);
-  }
-  tc_teardown(T);
-}
-
 __global__ void __launch_bounds__(kThreads) catn_result_tensor_kernel(
     char* slot, SlotLayout L, catn_params P, int n, double* out, long long cap, long long* meta) {
   extern __shared__ double smem[];
@@ -160,16 +112,19 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   if (R.ninst == 0) return fail(CATN_EINVAL, "no instances");
   R.use_tc = 0;
   R.cta_jobs = 0;
+  R.lean = 1;
   for (const InstDesc& d : im.desc) {
     if (d.P.precision == 1) R.use_tc = 1;
     if (d.P.svd_route == 2 || (d.P.svd_route == 0 && d.P.precision == 1)) R.cta_jobs = 1;
+    if (d.P.precision != 0 || d.P.svd_route == 2 || d.P.rsvd == 2 || d.kind == 2) R.lean = 0;
   }
+  if (R.lean) CUDA_TRY(persistent_lean_attr());
   R.L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
   int dev = 0, nsm = 0, per_sm = 0;
   CUDA_TRY(cudaGetDevice(&dev));
   CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  CUDA_TRY(cudaFuncSetAttribute(catn_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesTc));
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, catn_persistent_kernel, kThreads, kSmemBytes));
+  CUDA_TRY(cudaFuncSetAttribute(catn_persistent_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesTc));
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, catn_persistent_kernel<0>, kThreads, kSmemBytes));
   if (per_sm < 1) per_sm = 1;
   long long resident = (long long)nsm * per_sm;
   long long ns = R.ninst < resident ? R.ninst : resident;
@@ -281,7 +236,11 @@ catn_status launch(DeviceRun& R, cudaStream_t st) {
   int nhelp = 0;
   JobLink jl;
   helper_config(R, false, &jl, &nhelp);
-  catn_persistent_kernel<<<R.ngrid, kThreads, R.use_tc ? kSmemBytesTc : kSmemBytes, st>>>(
+  if (R.lean) {
+    CUDA_TRY(persistent_lean_launch(R, nhelp, jl, st));
+    return CATN_OK;
+  }
+  catn_persistent_kernel<0><<<R.ngrid, kThreads, R.use_tc ? kSmemBytesTc : kSmemBytes, st>>>(
       R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32, R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace, R.d_queue,
       R.d_board, nhelp, jl, R.use_tc);
   CUDA_TRY(cudaGetLastError());

@@ -71,6 +71,7 @@ struct DeviceRun {
   int ninst = 0;
   int use_tc = 0;  // some instance runs in split precision: TMEM and the staging area per CTA
   int cta_jobs = 0;   // some instance takes the block SVD route (its jobs are CTA items)
+  int lean = 0;       // forward launches run the lean instantiation (capi_lean.cu)
   long long input_bytes = 0;
 
   void release() {
@@ -107,6 +108,10 @@ constexpr int kGradHelperCtas = 8;
 long long default_arena(long long a, const catn_params& p);
 // Frees a gradient run (capi_grad.cu).
 void grad_release(GradRun* g);
+// The lean persistent kernel (capi_lean.cu): its shared-memory attribute,
+// and a launch of R.
+cudaError_t persistent_lean_attr();
+cudaError_t persistent_lean_launch(const DeviceRun& R, int nhelp, const catn::JobLink& jl, cudaStream_t st);
 // Runs the BraKet kernel over a prepared run (capi_braket.cu).
 catn_status braket_launch(DeviceRun& R, cudaStream_t st);
 

@@ -401,6 +401,10 @@ CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const d
 // rotations must lie outside the shared-memory workspace, which the block
 // items use (the SVD routines place both there when 2 n^2 doubles fit).
 CATN_HD bool use_block(const Ctx& C, long long n, const double* X) {
+#if CATN_LEAN
+  (void)C; (void)n; (void)X;
+  return false;
+#endif
   if (X == C.sws || 2 * n * n <= C.sws_doubles || n < C.block_min_n) return false;
   return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
 }
@@ -408,6 +412,10 @@ CATN_HD bool use_block(const Ctx& C, long long n, const double* X) {
 // available, singular vectors formed only as far as the caller uses them);
 // svd_route 1, and svd_route 0 in FP64, keep the earlier arithmetic bit for bit.
 CATN_HD bool new_routes(const Ctx& C) {
+#if CATN_LEAN
+  (void)C;
+  return false;
+#endif
   return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
 }
 // Columns of U and V an SVD of nn values forms for its caller.
@@ -456,7 +464,7 @@ CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, l
 constexpr long long kTcMergeMinElems = 1LL << 18;
 CATN_HDI inline bool merge_on_tc(Ctx& C, long long M, long long N, long long K, const double* A, const double* B,
                                  const MOp& out) {
-#if CATN_DEVICE_PASS
+#if CATN_DEVICE_PASS && !CATN_LEAN
   if (C.P.precision != 1 || M * N < kTcMergeMinElems || !tc_ready(C.T)) return false;
   if (!tc_gemm_mop(C.T, M, N, K, A, M, B, K, out)) fail_all(C, CATN_ETIMEOUT);
   C.T.sync();
@@ -1031,7 +1039,7 @@ CATN_HDI inline double swap(Ctx& C, int k, int i, int j) {
   // wider than M); otherwise the exact top-chi subspace it approximates
   const bool randomized = rsvd_route && C.P.rsvd >= 1 && !C.tape && m >= (n < 10LL * C.P.chi ? n : 10LL * C.P.chi);
   // rsvd = 2: the same algorithm with M applied from (tl, tr), never formed
-  const bool matfree = randomized && C.P.rsvd == 2;
+  const bool matfree = !CATN_LEAN && randomized && C.P.rsvd == 2;
   SvdIn in = SvdIn();
   if (!matfree) {
     in = svd_begin(C, m, n, rsvd_route ? 0.0 : C.P.cutoff);

@@ -56,6 +56,11 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
 
 // TMEM allocation of `ncols` columns (a power of two >= 32) by one whole
 // warp; the base address is written to *slot (shared memory).
+//
+// A translation unit that defines CATN_NO_TCGEN05 before including this file
+// compiles no tcgen05 instruction: there tc_setup leaves the staging area
+// unset (tc_ready is false) and no tensor-core routine is reached.
+#if !defined(CATN_NO_TCGEN05)
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
                "r"(ncols));
@@ -67,6 +72,12 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+#else
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t) { *slot = 0; }
+__device__ __forceinline__ void tmem_dealloc(uint32_t, uint32_t) {}
+__device__ __forceinline__ void fence_before_sync() {}
+__device__ __forceinline__ void fence_after_sync() {}
+#endif
 // Make this thread's generic-proxy shared-memory writes visible to the
 // tensor core (async proxy); followed by a barrier before the MMA issue.
 __device__ __forceinline__ void fence_smem_to_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -93,6 +104,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
   return false;
 }
 
+#if !defined(CATN_NO_TCGEN05)
 // D[tmem] (+)= A[smem] * B[smem], one instruction (issued by one thread).
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
@@ -126,6 +138,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 #pragma unroll
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+#else
+__device__ __forceinline__ void mma_tf32(uint32_t, uint64_t, uint64_t, uint32_t, uint32_t) {}
+__device__ __forceinline__ void mma_commit(uint64_t*) {}
+__device__ __forceinline__ void tmem_ld32(uint32_t, float* v) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = 0.f;
+}
+#endif
 
 // x rounded to TF32: nearest on the dropped 13 mantissa bits, ties away
 // from zero (a carry into the exponent is the correct rounding).

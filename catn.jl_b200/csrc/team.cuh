@@ -26,6 +26,14 @@
 #define CATN_DEVICE_PASS 0
 #endif
 
+// CATN_LEAN = 1 (set by a translation unit before its includes) compiles the
+// engine without the block Jacobi route, the blocked QR, the tensor-core
+// merges and the matrix-free randomized swaps: the persistent kernel of
+// launches that use none of them (FP64, svd_route != 2, rsvd != 2).
+#ifndef CATN_LEAN
+#define CATN_LEAN 0
+#endif
+
 namespace catn {
 
 struct Team {
