@@ -22,11 +22,25 @@ namespace catn_capi {
 constexpr int kThreads = 256;
 // Dynamic shared memory per CTA: reduction area, GEMM tile staging, and the
 // small-SVD workspace.  The persistent kernel's 255 registers per thread
-// limit an SM to one 256-thread CTA; the 100 KiB would fit twice.
-constexpr int kSmemBytes = 100 * 1024;
+// limit an SM to one 256-thread CTA.  Shared memory and the L1 cache share
+// the SM's 256 KB, in configurations of 0 / 8 / 16 / 32 / 64 / 100 / 132 /
+// 164 / 196 / 228 KB of shared memory, and the runtime reserves 1 KB per CTA.
+// The engine's loads of slot data (L2-resident) go through L1, and its time
+// follows L1's capacity (measured on the 512-instance spin-glass batch:
+// 315 ms at 100 KB, i.e. the 132 KB configuration and 124 KB of L1; 305 ms
+// at 98 KB, the 100 KB configuration; 300 ms at 62 KB, the 64 KB
+// configuration; 378 ms at 200 KB).  98 KB keeps the block route's items and
+// the blocked QR's panels in shared memory.
+constexpr int kSmemBytes = 98 * 1024;
 constexpr long long kSwsDoubles = (kSmemBytes - 64 * 8 - catn::GEMM_STAGE_BYTES) / 8;
 static_assert(kSwsDoubles >= catn::kBlockWsDoubles, "block-route items need their workspace in shared memory");
 static_assert(kSwsDoubles >= catn::kPanelWsDoubles + catn::kPanelW, "panel items need their workspace in shared memory");
+// The lean instantiation (capi_lean.cu) has neither: 62 KB, the 64 KB
+// configuration (192 KB of L1); its small-SVD workspace still holds the
+// tiny one-warp SVDs (64 x 16) and every SVD up to 5792 doubles of workspace.
+constexpr int kSmemBytesLean = 62 * 1024;
+constexpr long long kSwsDoublesLean = (kSmemBytesLean - 64 * 8 - catn::GEMM_STAGE_BYTES) / 8;
+static_assert(kSwsDoublesLean >= 2 * 64 * 16 + 3 * 16 * 16 + 8 * 16 + 64, "the tiny SVDs need their workspace");
 // Launches with split-precision instances add the tensor-core staging area
 // (blockjac_tc.cuh) after the small-SVD workspace.
 constexpr int kSmemBytesTc = kSmemBytes + catn::kTcRegionBytes + 1024;

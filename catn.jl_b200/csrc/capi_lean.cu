@@ -16,11 +16,11 @@
 namespace catn_capi {
 
 cudaError_t persistent_lean_attr() {
-  return cudaFuncSetAttribute(catn_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+  return cudaFuncSetAttribute(catn_persistent_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesLean);
 }
 
 cudaError_t persistent_lean_launch(const DeviceRun& R, int nhelp, const JobLink& jl, cudaStream_t st) {
-  catn_persistent_kernel<1><<<R.ngrid, kThreads, kSmemBytes, st>>>(
+  catn_persistent_kernel<1><<<R.ngrid, kThreads, kSmemBytesLean, st>>>(
       R.d_desc, R.d_order, R.ninst, R.d_i64, R.d_i32, R.d_dat, R.d_slots, R.L, R.d_res, R.d_trace, R.d_queue,
       R.d_board, nhelp, jl, 0);
   return cudaGetLastError();

@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(kThreads) catn_persistent_kernel(
     }
     inst = T.bcast(inst);
     if (inst >= ninst) break;
-    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws, kSwsDoubles,
+    run_instance(T, slot, L, descs[inst], i64, i32, dat, res + inst, trace, sws,
+                 kVariant == 1 ? kSwsDoublesLean : kSwsDoubles,
                  board ? &jl : nullptr);
     if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
     // A shared wait that ran out leaves a helper warp that may still write

@@ -27,7 +27,7 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   T.tmem = 0;
   std::vector<int> tr((size_t)im.trace_total + 8);
   // stand-in for the GPU's shared-memory SVD workspace (same capacity)
-  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  long long sws_doubles = (98 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   // CATN_HOSTCHECK_SWS overrides the capacity (0 sends every SVD through the
   // large-matrix path, including its rank-revealing truncation)
   if (const char* e = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(e);
@@ -90,7 +90,7 @@ int catn_hostcheck_ising_grad(const catn_params* p, int n, int n_edges, const in
   T.stage_bytes = 0;
   T.tcs = nullptr;
   T.tmem = 0;
-  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  long long sws_doubles = (98 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   if (const char* ev = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(ev);
   // at least the block route's item workspace, whatever capacity is reported
   std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
@@ -119,7 +119,7 @@ int catn_hostcheck_braket(const catn_params* p, int n, const int* ndims, const l
   T.stage_bytes = 0;
   T.tcs = nullptr;
   T.tmem = 0;
-  long long sws_doubles = (100 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
+  long long sws_doubles = (98 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
   std::vector<int> tr((size_t)im.trace_total + 8);
   run_instance_braket(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
