@@ -25,7 +25,7 @@ namespace {
 __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     const InstDesc* __restrict__ descs, const int* __restrict__ order, int ninst, const long long* i64,
     const int* i32, const double* dat, char* slots, SlotLayout L, catn_result* res, double* gimg, int* queue,
-    JacobiJob* board, int nhelp, JobLink jl, int use_tc) {
+    JacobiJob* board, int nhelp, JobLink jl, int use_tc, long long sws_doubles) {
   extern __shared__ double smem[];
   Team T;
   T.red = smem;
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
     }
     inst = T.bcast(inst);
     if (inst >= ninst) break;
-    run_instance_grad(T, slot, L, descs[inst], i64, i32, dat, res + inst, gimg, sws, kSwsDoubles,
+    run_instance_grad(T, slot, L, descs[inst], i64, i32, dat, res + inst, gimg, sws, sws_doubles,
                       board ? &jl : nullptr);
     if (board && threadIdx.x == 0) atomicAdd(queue + 1, 1);
     // A shared wait that ran out leaves a helper warp that may still write
@@ -100,9 +100,13 @@ catn_status grad_launch(GradRun* g, cudaStream_t st) {
   int nhelp = 0;
   JobLink jl;
   helper_config(g->R, true, &jl, &nhelp);
-  catn_grad_kernel<<<g->R.ngrid, kThreads, g->R.use_tc ? kSmemBytesTc : kSmemBytes, st>>>(
+  // Runs without the tensor-core area or block-route items take the smaller
+  // shared-memory configuration, which leaves more of the SM to L1 (as the
+  // lean forward kernel does).
+  const bool small = !g->R.use_tc && !g->R.cta_jobs;
+  catn_grad_kernel<<<g->R.ngrid, kThreads, g->R.use_tc ? kSmemBytesTc : (small ? kSmemBytesLean : kSmemBytes), st>>>(
       g->R.d_desc, g->R.d_order, g->R.ninst, g->R.d_i64, g->R.d_i32, g->R.d_dat, g->R.d_slots, g->R.L, g->R.d_res,
-      g->d_gimg, g->R.d_queue, g->R.d_board, nhelp, jl, g->R.use_tc);
+      g->d_gimg, g->R.d_queue, g->R.d_board, nhelp, jl, g->R.use_tc, small ? kSwsDoublesLean : kSwsDoubles);
   CUDA_TRY(cudaGetLastError());
   return CATN_OK;
 }
