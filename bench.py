@@ -272,6 +272,8 @@ def main():
                     help="time budget of the plain GPU form sample (0 = skip)")
     ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
     ap.add_argument("--no-c2", action="store_true", help="skip the n=200 random-regular leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 8x8 ferromagnet and the reduced 32x32 Gaussian-lattice legs")
     ap.add_argument("--c2-scalar", action="store_true",
                     help="also time the n=200 leg on the scalar Jacobi route (about 40 s per beta)")
     ap.add_argument("--no-c2-oracle", action="store_true",
@@ -456,6 +458,9 @@ def main():
                       f"~{args.plain_seconds:.0f} s wall clock"}
     if world == 1 and not args.no_c2:
         out["rrg200"] = c2_leg(catn, args)
+    if world == 1 and not args.no_configs:
+        out["ferro8"] = c1_leg(catn)
+        out["gaussian_lattice_reduced"] = c4_reduced_leg(catn)
     print(json.dumps(out))
     if dist:
         dist.barrier()
@@ -517,6 +522,110 @@ def c2_leg(catn, args):
         if b1:
             res["fp64_block_speedup_vs_oracle_at_beta_1"] = round(secs / b1[0], 2)
     return res
+
+
+def c1_leg(catn):
+    """The 8 x 8 open ferromagnet (w = 1, h = 0, beta = 0.44, Dmax 20, chi
+    200), one network through the public API: latency of one contraction,
+    lnZ per site and free energy (ising.jl:239-244), the error against the
+    transfer-matrix value and the trace against the FP64 oracle's, both
+    frozen in tests/golden/config1_ferro8.json, and the HBM fraction of the
+    one launch (algorithmic bytes / CUDA-event time)."""
+    import torch
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "config1_ferro8.json")))
+    edges = [tuple(e) for e in d["edges"]]
+    times, out = [], None
+    for rep in range(4):
+        tn = catn.ising_network(d["n"], edges, d["weights"], d["fields"], d["beta"], **d["params"])
+        catn.adapt(catn.B200, tn, trace=True)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record()
+        lnZ, err, psi = catn.contraction(tn, trace=True)
+        b.record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        if rep > 0:   # the first contraction is a warm-up
+            times.append((a.elapsed_time(b) / 1e3, wall))
+        out = (tn, lnZ, err)
+    tn, lnZ, err = out
+    dev_s = sum(t[0] for t in times) / len(times)
+    rows = [[int(x) for x in r[:7]] for r in tn.trace]
+    nbytes = tn.result.bytes
+    peak, _ = load_peaks()
+    return {"workload": "8x8 open square lattice, w=1, h=0, beta=0.44, Dmax=20, chi=200 (tests/golden/config1_ferro8.json)",
+            "ms_per_contraction": round(1e3 * dev_s, 3),
+            "ms_per_contraction_wall": round(1e3 * sum(t[1] for t in times) / len(times), 3),
+            "lnZ_per_site": lnZ / d["n"], "free_energy_per_site": -lnZ / d["n"] / d["beta"],
+            "abs_dlnZ_per_site_vs_transfer_matrix": abs(lnZ - d["exact_lnZ"]) / d["n"],
+            "abs_dlnZ_per_site_vs_oracle": abs(lnZ - d["oracle"]["lnZ"]) / d["n"],
+            "trace_identical_to_oracle": rows == d["oracle"]["trace"], "err": err,
+            "roofline": {"bound": "hbm", "achieved": round(nbytes / dev_s / 1e9, 4), "peak": peak, "unit": "GB/s",
+                         "frac": round(nbytes / dev_s / 1e9 / peak, 7) if peak else None,
+                         "algorithmic_bytes": nbytes},
+            "timing": "CUDA events around catn.contraction (upload, one launch, read-back), mean of 3 after one warm-up"}
+
+
+def c4_reduced_leg(catn, L=10, seed=4):
+    """The 32 x 32 Gaussian lattice configuration (J ~ N(0,1), h ~ N(0,0.2^2),
+    beta 1, Dmax 48, chi 256) at L = 10: the forward contraction, the device
+    adjoint of lnZ (whole tape, and checkpointed every 64 steps), and the
+    reference's pinning definition of every <s_k> and <s_i s_j> (1 + 2n +
+    4|E| networks, all of them: as one batch, and one network at a time as
+    the reference's loop runs them), each timed through the public calls;
+    the observables of the two routes are compared on every spin and edge."""
+    from catn_b200.graphs import square_edges
+    r = np.random.default_rng(seed)
+    n = L * L
+    edges = square_edges(L)
+    w, h, beta = r.normal(size=len(edges)), r.normal(0, 0.2, n), 1.0
+    kw = dict(Dmax=48, chi=256)
+    catn.contraction(catn.ising_network(n, edges, w, h, beta, **kw))   # warm-up
+    t0 = time.perf_counter()
+    lnZ, err, _ = catn.contraction(catn.ising_network(n, edges, w, h, beta, **kw))
+    t_fwd = time.perf_counter() - t0
+    grads = {}
+    for k in (0, 64):
+        net = catn.ising_network(n, edges, w, h, beta, **kw)
+        catn.gradient(net, ckpt_interval=k)   # warm-up (allocates the gradient slot)
+        t0 = time.perf_counter()
+        lz_g, dw, dh = catn.gradient(net, ckpt_interval=k)
+        grads[k] = (time.perf_counter() - t0, lz_g, dw, dh)
+    inst = dict(n=n, edges=edges, weights=w, fields=h, beta=beta)
+    pins = _pin_sets(inst)
+    b = catn.IsingBatch([dict(inst, pos1=p1, val1=v1, pos2=p2, val2=v2) for (p1, v1, p2, v2) in pins], **kw)
+    b.run()   # warm-up (allocates the slots)
+    t0 = time.perf_counter()
+    b.run()
+    t_pin = time.perf_counter() - t0
+    lz = b.lnZ()
+    z1 = np.exp(lz[1:1 + 2 * n] - lz[0]).reshape(n, 2)
+    m_pin = z1[:, 1] - z1[:, 0]   # val 2 pins spin +1, val 1 spin -1 (ising.jl:255-290)
+    z2 = np.exp(lz[1 + 2 * n:] - lz[0]).reshape(len(edges), 2, 2)
+    c_pin = z2[:, 0, 0] - z2[:, 0, 1] - z2[:, 1, 0] + z2[:, 1, 1]
+    t_adj, lz_g, dw, dh = grads[0]
+    # the reference's loop: every pinned network built and contracted on its
+    # own (ising.jl:276-289, 321-337), through the same public calls
+    t0 = time.perf_counter()
+    lz_seq = [catn.contraction(catn.ising_network(n, edges, w, h, beta, pos1=p1, val1=v1, pos2=p2, val2=v2, **kw))[0]
+              for (p1, v1, p2, v2) in pins]
+    t_seq = time.perf_counter() - t0
+    return {"workload": f"{L}x{L} open lattice (the 32x32 configuration reduced), J~N(0,1), h~N(0,0.2^2), beta=1, "
+                        f"Dmax=48, chi=256, seed {seed}",
+            "forward_s": round(t_fwd, 4), "lnZ": lnZ, "err": err,
+            "adjoint_s": round(t_adj, 4), "adjoint_ckpt64_s": round(grads[64][0], 4),
+            "ckpt64_gradients_identical": bool(np.array_equal(grads[64][2], dw) and np.array_equal(grads[64][3], dh)),
+            "pinning_networks": len(pins), "pinning_s": round(t_pin, 4),
+            "speedup_adjoint_vs_pinning_batched": round(t_pin / t_adj, 2),
+            "pinning_sequential_s": round(t_seq, 3),
+            "speedup_adjoint_vs_pinning_sequential": round(t_seq / t_adj, 1),
+            "max_abs_dlnZ_sequential_vs_batched": float(np.max(np.abs(np.array(lz_seq) - lz))),
+            "max_abs_diff_magnetization": float(np.max(np.abs(dh / beta - m_pin))),
+            "max_abs_diff_correlation": float(np.max(np.abs(dw / beta - c_pin))),
+            "timing": "host wall clock around the public calls (network upload, launches and read-back inside), "
+                      "after one warm-up call of each; pinning batched = one IsingBatch.run() over every pinned network, "
+                      "sequential = ising_network + contraction per pinned network"}
 
 
 def _pin_sets(d):
