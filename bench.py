@@ -272,6 +272,9 @@ def main():
                     help="time budget of the plain GPU form sample (0 = skip)")
     ap.add_argument("--max-slots", type=int, default=0, help="cap on CTA slots (0 = all resident)")
     ap.add_argument("--no-c2", action="store_true", help="skip the n=200 random-regular leg")
+    ap.add_argument("--c4-full", action="store_true",
+                    help="also run the 32x32 Gaussian lattice at full size (forward, checkpointed adjoint, one "
+                         "central difference, 8 pinned edges; several minutes)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the 8x8 ferromagnet and the reduced 32x32 Gaussian-lattice legs")
     ap.add_argument("--c2-scalar", action="store_true",
@@ -458,6 +461,8 @@ def main():
                       f"~{args.plain_seconds:.0f} s wall clock"}
     if world == 1 and not args.no_c2:
         out["rrg200"] = c2_leg(catn, args)
+    if world == 1 and args.c4_full:
+        out["gaussian_lattice_32"] = c4_full_leg(catn)
     if world == 1 and not args.no_configs:
         out["ferro8"] = c1_leg(catn)
         out["gaussian_lattice_reduced"] = c4_reduced_leg(catn)
@@ -626,6 +631,75 @@ def c4_reduced_leg(catn, L=10, seed=4):
             "timing": "host wall clock around the public calls (network upload, launches and read-back inside), "
                       "after one warm-up call of each; pinning batched = one IsingBatch.run() over every pinned network, "
                       "sequential = ising_network + contraction per pinned network"}
+
+
+def c4_full_leg(catn, L=32, seed=32, fd_edges=1, pin_edges=4):
+    """The 32 x 32 Gaussian lattice at full size (J ~ N(0,1), h ~ N(0,0.2^2),
+    beta 1, Dmax 48, chi 256): the forward contraction, the checkpointed
+    adjoint of lnZ (a checkpoint every 64 steps), central differences (step
+    1e-5) on `fd_edges` couplings, and pinning of `pin_edges` edges (4
+    networks each, one batch: one CTA per network, no helper CTAs), all
+    through the public calls.  Progress goes
+    to stderr as each part ends."""
+    from catn_b200.graphs import square_edges
+    r = np.random.default_rng(seed)
+    n = L * L
+    edges = square_edges(L)
+    w, h, beta = r.normal(size=len(edges)), r.normal(0, 0.2, n), 1.0
+    kw = dict(Dmax=48, chi=256)
+    out = {"workload": f"{L}x{L} open lattice ({len(edges)} edges), J~N(0,1), h~N(0,0.2^2), beta=1, Dmax=48, chi=256, "
+                       f"seed {seed}",
+           "timing": "host wall clock around the public calls (network upload, launches and read-back inside)"}
+    t0 = time.perf_counter()
+    net = catn.ising_network(n, edges, w, h, beta, **kw)
+    lnZ, err, _ = catn.contraction(net)
+    out.update(forward_s=round(time.perf_counter() - t0, 3), lnZ=lnZ, lnZ_per_site=lnZ / n, err=err,
+               maxdim_intermediate=net.maxdim_intermediate,
+               forward_engine_ms=round(net.result.prof[0] / 1.965e6, 1), forward_arena_peak=net.result.arena_peak)
+    print("c4 forward", out["forward_s"], lnZ, err, file=sys.stderr, flush=True)
+    t0 = time.perf_counter()
+    lz_g, dw, dh = catn.gradient(catn.ising_network(n, edges, w, h, beta, **kw), ckpt_interval=64)
+    out.update(adjoint_ckpt64_s=round(time.perf_counter() - t0, 3), adjoint_lnZ_minus_forward=lz_g - lnZ)
+    print("c4 adjoint", out["adjoint_ckpt64_s"], file=sys.stderr, flush=True)
+    fd = []
+    for q in r.choice(len(edges), size=fd_edges, replace=False).tolist():
+        eps = 1e-5
+        wp, wm = w.copy(), w.copy()
+        wp[q] += eps
+        wm[q] -= eps
+        lp = catn.contraction(catn.ising_network(n, edges, wp, h, beta, **kw))[0]
+        lm = catn.contraction(catn.ising_network(n, edges, wm, h, beta, **kw))[0]
+        fd.append({"edge": q, "fd": (lp - lm) / (2 * eps), "adjoint": float(dw[q]),
+                   "abs_diff": abs((lp - lm) / (2 * eps) - float(dw[q]))})
+        print("c4 fd", fd[-1], file=sys.stderr, flush=True)
+    out["central_differences"] = fd
+    subset = sorted(r.choice(len(edges), size=pin_edges, replace=False).tolist())
+    insts = [dict(n=n, edges=edges, weights=w, fields=h, beta=beta)]
+    for q in subset:
+        m, nn = edges[q]
+        for v1 in (1, 2):
+            for v2 in (1, 2):
+                insts.append(dict(n=n, edges=edges, weights=w, fields=h, beta=beta, pos1=m, val1=v1, pos2=nn, val2=v2))
+    # each pinned network's slot gets 1.5x the arena the forward run peaked at
+    arena = max(1 << 30, int(1.5 * net.result.arena_peak) // 256 * 256)
+    t0 = time.perf_counter()
+    b = catn.IsingBatch(insts, slot_arena_bytes=arena, **kw)
+    b.run()
+    t_pin = time.perf_counter() - t0
+    lz = b.lnZ()
+    p = np.exp(lz[1:] - lz[0]).reshape(len(subset), 2, 2)
+    c_pin = p[:, 0, 0] - p[:, 0, 1] - p[:, 1, 0] + p[:, 1, 1]
+    npin = 1 + 2 * n + 4 * len(edges)
+    out.update(pinning_subset_edges=len(subset), pinning_subset_networks=len(insts),
+               pinning_subset_s=round(t_pin, 3), pinning_slots=b.slots, pinning_slot_arena=arena,
+               max_abs_diff_correlation_vs_adjoint=float(np.max(np.abs(dw[subset] / beta - c_pin))),
+               pinning_networks_full_definition=npin,
+               pinning_full_s_at_subset_rate=round(t_pin / len(insts) * npin, 1),
+               speedup_adjoint_vs_pinning_at_subset_rate=round(t_pin / len(insts) * npin / out["adjoint_ckpt64_s"], 1),
+               speedup_adjoint_vs_pinning_sequential_at_forward_time=round(npin * out["forward_s"] /
+                                                                           out["adjoint_ckpt64_s"], 1))
+    print("c4 pinning", t_pin, file=sys.stderr, flush=True)
+    return out
 
 
 def _pin_sets(d):
