@@ -635,7 +635,8 @@ def c4_reduced_leg(catn, L=10, seed=4):
 
 def c4_full_leg(catn, L=32, seed=32, fd_edges=1, pin_edges=4):
     """The 32 x 32 Gaussian lattice at full size (J ~ N(0,1), h ~ N(0,0.2^2),
-    beta 1, Dmax 48, chi 256): the forward contraction, the checkpointed
+    beta 1, Dmax 48, chi 256): the forward contraction (FP64, and split
+    precision against it), the checkpointed
     adjoint of lnZ (a checkpoint every 64 steps), central differences (step
     1e-5) on `fd_edges` couplings, and pinning of `pin_edges` edges (4
     networks each, one batch: one CTA per network, no helper CTAs), all
@@ -657,6 +658,14 @@ def c4_full_leg(catn, L=32, seed=32, fd_edges=1, pin_edges=4):
                maxdim_intermediate=net.maxdim_intermediate,
                forward_engine_ms=round(net.result.prof[0] / 1.965e6, 1), forward_arena_peak=net.result.arena_peak)
     print("c4 forward", out["forward_s"], lnZ, err, file=sys.stderr, flush=True)
+    # the split-precision form (3xTF32 tensor-core merges and block-route Grams)
+    t0 = time.perf_counter()
+    net_s = catn.ising_network(n, edges, w, h, beta, precision="split", **kw)
+    lnZ_s, err_s, _ = catn.contraction(net_s)
+    out["split"] = {"forward_s": round(time.perf_counter() - t0, 3), "lnZ": lnZ_s, "err": err_s,
+                    "abs_dlnZ_per_site_vs_fp64": abs(lnZ_s - lnZ) / n,
+                    "engine_ms": round(net_s.result.prof[0] / 1.965e6, 1)}
+    print("c4 split forward", out["split"], file=sys.stderr, flush=True)
     t0 = time.perf_counter()
     lz_g, dw, dh = catn.gradient(catn.ising_network(n, edges, w, h, beta, **kw), ckpt_interval=64)
     out.update(adjoint_ckpt64_s=round(time.perf_counter() - t0, 3), adjoint_lnZ_minus_forward=lz_g - lnZ)
