@@ -202,6 +202,16 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_bf16_peak(key="bf16_tflops_sustained"):
+    """Dense bf16 GEMM TFLOP/s from MEASURED_PEAKS.json (the sustained figure
+    by default: the launches it is compared with run for seconds), or None."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        v = json.load(open(p)).get(key)
+        return float(v) if v else None
+    return None
+
+
 # ----------------------------------------------------------------------------
 def lpt_order(instances):
     """Largest instances first (by edge count), as the device work queue
@@ -460,7 +470,7 @@ def main():
                       f"PyTorch FP64 on cuda:{local} (torch.linalg.svd/qr + einsum per op, host loop), "
                       f"~{args.plain_seconds:.0f} s wall clock"}
     if world == 1 and not args.no_c2:
-        out["rrg200"] = c2_leg(catn, args)
+        out["rrg200"] = c2_leg(catn, args, fp64_peak, load_bf16_peak())
     if world == 1 and args.c4_full:
         out["gaussian_lattice_32"] = c4_full_leg(catn)
     if world == 1 and not args.no_configs:
@@ -483,7 +493,7 @@ def _oracle_rrg200(beta):
     return lnZ, time.perf_counter() - t0
 
 
-def c2_leg(catn, args):
+def c2_leg(catn, args, fp64_peak=None, bf16_peak=None):
     """The n=200 random 3-regular +-1 spin glass (300 edges, h ~ N(0, 0.1^2),
     beta in {0.5, 1, 1.5}, Dmax 32, chi 128), one network per beta through
     the public API (host image in, results out), in two forms: FP64 on the
@@ -491,7 +501,10 @@ def c2_leg(catn, args):
     products, block route); with --c2-scalar also FP64 on the scalar Jacobi
     route.  The FP64 oracle is timed on beta = 1 on the host cores.  Errors are
     against the FP64 oracle's values frozen in tests/golden/rrg200.json (made
-    by tests/golden/make_golden.py); the trace must equal the oracle's."""
+    by tests/golden/make_golden.py); the trace must equal the oracle's.
+    Rates: algorithmic FLOPs of the contraction (the same per-step
+    convention as the batch's roofline) per second, against the measured
+    DGEMM rate (FP64 forms) or the TF32 rate (split form)."""
     d = json.load(open(os.path.join(ROOT, "tests", "golden", "rrg200.json")))
     edges = [tuple(e) for e in d["edges"]]
     res = {"workload": "random 3-regular +-1 spin glass, n=200 (300 edges), h~N(0,0.1^2), beta in {0.5,1,1.5}, "
@@ -514,8 +527,21 @@ def c2_leg(catn, args):
             dt = time.perf_counter() - t0
             rows = [[int(x) for x in r[:7]] for r in tn.trace]
             per.append({"beta": beta, "s": round(dt, 3), "abs_dlnZ_per_spin": abs(lnZ - ref["lnZ"]) / d["n"],
-                        "trace_identical": rows == ref["trace"], "err": err, "oracle_err": ref["err"]})
+                        "trace_identical": rows == ref["trace"], "err": err, "oracle_err": ref["err"],
+                        "algorithmic_tflops": round(tn.result.flops / dt / 1e12, 4)})
+        rate = sum(p["algorithmic_tflops"] for p in per) / len(per)
+        if name == "split":
+            # the tensor pipe runs TF32 at half the bf16 rate; the split products
+            # are three TF32 products each
+            pk, src = (bf16_peak / 2, "half the measured sustained bf16 GEMM rate (MEASURED_PEAKS.json), "
+                                      "the TF32 rate") \
+                if bf16_peak else (None, None)
+        else:
+            pk, src = fp64_peak, "cuBLAS DGEMM measured in this run"
         res["forms"][name] = {"s_per_beta": round(sum(p["s"] for p in per) / len(per), 3),
+                              "algorithmic_tflops": round(rate, 4),
+                              "peak_tflops": pk, "peak_source": src,
+                              "frac": round(rate / pk, 6) if pk else None,
                               "max_abs_dlnZ_per_spin": max(p["abs_dlnZ_per_spin"] for p in per),
                               "traces_identical": all(p["trace_identical"] for p in per), "runs": per}
     if not args.no_c2_oracle:

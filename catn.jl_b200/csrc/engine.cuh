@@ -378,8 +378,21 @@ CATN_HDI inline void svd_fill(Ctx& C, const SvdIn& s, const MOp& A) {
 // shared job: always when the launch has dedicated helper CTAs, otherwise
 // once the launch's queue is drained (idle CTAs then help); the same answer
 // in every thread.
-CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X) {
-  if (!C.job || n < C.job_min_n || X == C.sws) return false;
+// Whether p points into this CTA's shared memory (the SVD workspace or any
+// other part of it).  Such an address means nothing to another CTA, so work
+// on an array there is never published to helper CTAs.
+CATN_HD bool cta_local(const Ctx& C, const void* p) {
+#if CATN_DEVICE_PASS
+  (void)C;
+  return p && __isShared(p);
+#else
+  const double* q = (const double*)p;
+  return q && q >= C.sws && q < C.sws + C.sws_doubles;
+#endif
+}
+
+CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X, const double* V, const double* nrm) {
+  if (!C.job || n < C.job_min_n || cta_local(C, X) || cta_local(C, V) || cta_local(C, nrm)) return false;
   if (C.job_pool) return true;
   long long drained = 0;
   if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
@@ -387,9 +400,10 @@ CATN_HDI inline bool share_jacobi(Ctx& C, long long n, const double* X) {
 }
 
 // Whether the Householder work on a rows x cols matrix in global memory goes
-// to the shared job (same rule as share_jacobi, by element count).
-CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const double* X) {
-  if (!C.job || rows * cols < C.job_min_qr || X == C.sws) return false;
+// to the shared job (same rule as share_jacobi, by element count); X and Y
+// are the arrays the helpers would read and write.
+CATN_HDI inline bool share_house(Ctx& C, long long rows, long long cols, const double* X, const double* Y) {
+  if (!C.job || rows * cols < C.job_min_qr || cta_local(C, X) || cta_local(C, Y)) return false;
   if (C.job_pool) return true;
   long long drained = 0;
   if (C.T.leader()) drained = ldcg_i(C.qhead) >= C.ninst ? 1 : 0;
@@ -405,7 +419,7 @@ CATN_HD bool use_block(const Ctx& C, long long n, const double* X) {
   (void)C; (void)n; (void)X;
   return false;
 #endif
-  if (X == C.sws || 2 * n * n <= C.sws_doubles || n < C.block_min_n) return false;
+  if (cta_local(C, X) || 2 * n * n <= C.sws_doubles || n < C.block_min_n) return false;
   return C.P.svd_route == 2 || (C.P.svd_route == 0 && C.P.precision == 1);
 }
 // Whether the large-SVD routes of this release are selected (block route
@@ -437,21 +451,22 @@ CATN_HDI inline int jacobi_any(Ctx& C, double* X, long long rows, long long n, l
                                double* nrm) {
   const long long t0 = clk();
   int sweeps;
-  if (use_block(C, n, X)) {
+  const bool blk = use_block(C, n, X) && !cta_local(C, V) && !cta_local(C, nrm);
+  if (blk) {
     // precision 1: rotations stop at the rounding level of FP32 products
     const double floor_rel = C.P.precision == 1 ? 1e-8 : 0.0;
     sweeps = jacobi_block(C.T, block_job(C), X, rows, n, ld, V, 60, C.sws, floor_rel, C.P.precision == 1);
     prof_add(C, PROF_N_BLOCK, 1.0);
     prof_add(C, PROF_BLOCK_SWEEPS, (double)sweeps);
   } else {
-    sweeps = share_jacobi(C, n, X) ? jacobi_sweeps_shared(C.T, C.job, X, rows, n, ld, V, 60, nrm)
+    sweeps = share_jacobi(C, n, X, V, nrm) ? jacobi_sweeps_shared(C.T, C.job, X, rows, n, ld, V, 60, nrm)
                                    : jacobi_sweeps(C.T, X, rows, n, ld, V, 60, nrm);
   }
   if (X != C.sws) {
     const double dt = (double)(clk() - t0);
     prof_add(C, PROF_LJAC, dt);
     prof_add(C, PROF_LJAC_COLS, (double)n);
-    if (use_block(C, n, X)) prof_add(C, PROF_LJAC_BLOCK, dt);
+    if (blk) prof_add(C, PROF_LJAC_BLOCK, dt);
     if (n >= 1024) prof_add(C, PROF_LJAC_BIG, dt);
   }
   return sweeps;
@@ -483,7 +498,7 @@ constexpr long long kBlockedQMinElems = 8192;
 // qr_apply_q, shared when large; false when a shared wait ran out.
 CATN_HDI inline bool apply_q_any(Ctx& C, const double* A, long long m, long long n, long long lda, const double* tau,
                                  double* Cm, long long ncols, long long ldc) {
-  if (share_house(C, m, ncols, Cm)) {
+  if (share_house(C, m, ncols, Cm, A)) {
     if (qr_apply_q_shared(C.T, C.job, A, m, n, lda, tau, Cm, ncols, ldc)) {
       fail_all(C, CATN_ETIMEOUT);
       return false;
@@ -519,7 +534,8 @@ CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long
   const long long t0 = clk();
   long long r;
   const long long work = m * n + (long long)kPanelW * m + 2048;
-  if (new_routes(C) && n >= C.blocked_qr_min_n && A != C.sws && 2 * n * n > C.sws_doubles &&
+  if (new_routes(C) && n >= C.blocked_qr_min_n && !cta_local(C, A) && !cta_local(C, nrm) &&
+      2 * n * n > C.sws_doubles &&
       C.sp + 8 * work + 4096 <= C.sp_hi) {
     // the blocked QR: columns sorted by norm, panels of 32 reflectors
     const long long mark = C.sp;
@@ -527,7 +543,7 @@ CATN_HDI inline long long qrcp(Ctx& C, double* A, long long m, long long n, long
     r = qr_sorted_blocked(C.T, block_job(C), A, m, n, lda, tau, piv, nrm, stop_tol, w, C.sws);
     C.sp = mark;
     if (r == -2) fail_all(C, CATN_ETIMEOUT);
-  } else if (share_house(C, m, n, A)) {
+  } else if (share_house(C, m, n, A, nrm)) {
     r = qrcp_shared(C.T, C.job, A, m, n, lda, tau, piv, nrm, stop_tol);
     if (r == -2) fail_all(C, CATN_ETIMEOUT);
   } else {
