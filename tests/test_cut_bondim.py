@@ -196,3 +196,23 @@ def test_gpu_cut_boundary_cases(catn):
         catn.cut_bondim(tn, 1, 1)          # contraction! consumed the network
     exact = catn.TensorNetwork(ts, ixs, Dmax=-1, chi=16)
     assert catn.cut_bondim(exact, 1, 1) == 0.0   # Dmax < 0: a no-op returning 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("opt", [False, True])
+def test_gpu_cut_of_a_low_rank_bond_is_exact(catn, opt):
+    """test/test_contraction.jl:42-57: a bond of rank 2 stored as dimension
+    4, cut to Dmax = 2, keeps the network's value (here the open-leg result
+    of contracting it)."""
+    r = np.random.default_rng(42)
+    P = r.normal(size=(3, 2)) @ r.normal(size=(2, 4))
+    Qm = r.normal(size=(4, 2)) @ r.normal(size=(2, 3))
+    tn = catn.TensorNetwork([P, Qm], [["a", "m"], ["m", "b"]], chi=1000, Dmax=2)
+    err = (catn.cut_bondim_opt if opt else catn.cut_bondim)(tn, 1, 2)
+    assert abs(err) < 1e-12 * np.abs(P @ Qm).max()
+    lnZ, _, psi = catn.contraction(tn)
+    got = catn.result_tensor(tn) * (np.exp(lnZ) * psi)   # the survivor is kept normalised
+    ref = P @ Qm
+    if got.shape != ref.shape or not np.allclose(got, ref, atol=1e-8):
+        got = got.T
+    np.testing.assert_allclose(got, ref, atol=1e-8)
