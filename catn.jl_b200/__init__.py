@@ -13,10 +13,11 @@ the package ``catn_b200`` (``__graft_entry__.load_package()`` does it).
 """
 from ._lib import CatnError, load as load_library
 from .braket import BraKetNetwork, braket_network
-from .network import B200, TensorNetwork, adapt, contraction, cut_bondim, cut_bondim_opt, result_tensor, tc_matmul
+from .network import (B200, TensorNetwork, adapt, contraction, cut_bondim, cut_bondim_opt, release_cached_memory,
+                      result_tensor, tc_matmul)
 from .ising import (IsingBatch, IsingNetwork, correlation, free_energy, gradient, ising_lnZ, ising_network,
                     magnetization)
 
 __all__ = ["B200", "BraKetNetwork", "CatnError", "IsingBatch", "IsingNetwork", "TensorNetwork", "adapt", "braket_network", "contraction",
            "correlation", "free_energy", "gradient", "ising_lnZ", "ising_network", "load_library",
-           "magnetization", "result_tensor", "tc_matmul", "cut_bondim", "cut_bondim_opt"]
+           "magnetization", "result_tensor", "tc_matmul", "cut_bondim", "cut_bondim_opt", "release_cached_memory"]

@@ -89,6 +89,8 @@ SIGNATURES = {
     "catn_tuning_get": ([ct.POINTER(Tuning)], ct.c_int),
     "catn_tuning_set": ([ct.POINTER(Tuning)], ct.c_int),
     "catn_last_error": ([ct.c_char_p, ct.c_size_t], ct.c_size_t),
+    "catn_release_cached_memory": ([], ct.c_int),
+    "catn_cached_bytes": ([ct.c_int32], ct.c_int64),
     "catn_version": ([], ct.c_char_p),
 }
 

@@ -15,7 +15,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "-Xcompiler", "-fPIC"]
 # Each unit compiles the device engine on its own (no device linking), so one
 # kernel's register allocation never depends on another unit's kernels.
-UNITS = ["capi.cu", "capi_static.cu", "capi_grad.cu", "capi_braket.cu", "capi_tc.cu", "capi_lean.cu"]
+UNITS = ["capi.cu", "capi_static.cu", "capi_grad.cu", "capi_braket.cu", "capi_tc.cu", "capi_lean.cu", "pool.cu"]
 OBJ = os.path.join(HERE, "_build")
 
 

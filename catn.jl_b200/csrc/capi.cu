@@ -131,6 +131,7 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   if (max_slots > 0 && ns > max_slots) ns = max_slots;
   size_t freeb = 0, totalb = 0;
   CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+  freeb += pool_cached_bytes(false);   // cached blocks are given back when an allocation needs them
   long long budget = (long long)(freeb * 0.85);
   if (ns * R.L.slot_bytes > budget) ns = budget / R.L.slot_bytes;
   if (ns < 1) return fail(CATN_ENOMEM, "not enough device memory for one slot");
@@ -147,8 +148,8 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   const long long b_i32 = align256((long long)(sizeof(int) * (im.i32.size() + 1)));
   const long long b_dat = align256((long long)(sizeof(double) * (im.dat.size() + 1)));
   R.input_bytes = b_desc + b_i64 + b_i32 + b_dat;
-  CUDA_TRY(cudaMallocHost(&R.h_input, (size_t)R.input_bytes));
-  CUDA_TRY(cudaMalloc(&R.d_input, (size_t)R.input_bytes));
+  CUDA_TRY(pool_new(&R.h_input, (size_t)R.input_bytes, true));
+  CUDA_TRY(pool_new(&R.d_input, (size_t)R.input_bytes));
   std::memset(R.h_input, 0, (size_t)R.input_bytes);
   std::memcpy(R.h_input, im.desc.data(), sizeof(InstDesc) * im.desc.size());
   const long long off_order = align256((long long)(sizeof(InstDesc) * im.desc.size()));
@@ -161,11 +162,11 @@ catn_status prepare(const Image& im, long long arena_bytes, int max_slots, Devic
   R.d_i64 = (long long*)(R.d_input + b_desc);
   R.d_i32 = (int*)(R.d_input + b_desc + b_i64);
   R.d_dat = (double*)(R.d_input + b_desc + b_i64 + b_i32);
-  CUDA_TRY(cudaMalloc(&R.d_slots, (size_t)(R.L.slot_bytes * ns)));
-  CUDA_TRY(cudaMalloc(&R.d_res, sizeof(catn_result) * im.desc.size()));
-  CUDA_TRY(cudaMalloc(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
-  CUDA_TRY(cudaMalloc(&R.d_queue, 4 * sizeof(int)));
-  if (R.ngrid > 1) CUDA_TRY(cudaMalloc(&R.d_board, sizeof(JacobiJob) * R.ngrid));
+  CUDA_TRY(pool_new(&R.d_slots, (size_t)(R.L.slot_bytes * ns)));
+  CUDA_TRY(pool_new(&R.d_res, sizeof(catn_result) * im.desc.size()));
+  CUDA_TRY(pool_new(&R.d_trace, sizeof(int) * (im.trace_total + 8)));
+  CUDA_TRY(pool_new(&R.d_queue, 4 * sizeof(int)));
+  if (R.ngrid > 1) CUDA_TRY(pool_new(&R.d_board, sizeof(JacobiJob) * R.ngrid));
   return CATN_OK;
 }
 
@@ -222,7 +223,8 @@ long long default_arena(long long a, const catn_params& p) {
   }
   arena = std::min(arena, 48LL << 30);
   size_t freeb = 0, totalb = 0;
-  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess) arena = std::min(arena, (long long)(freeb / 4));
+  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess)
+    arena = std::min(arena, (long long)((freeb + pool_cached_bytes(false)) / 4));
   return std::max(arena, 1LL << 30);
 }
 
@@ -281,10 +283,10 @@ catn_status params_prepare(catn_batch* b, const double* weights, const double* f
   P.nh = nh;
   P.nb = nb;
   if (P.nrec == 0) return CATN_OK;
-  CUDA_TRY(cudaMalloc(&P.d_rec, sizeof(IsingSiteRecipe) * P.nrec));
-  CUDA_TRY(cudaMalloc(&P.d_w, sizeof(double) * std::max(nw, 1LL)));
-  CUDA_TRY(cudaMalloc(&P.d_h, sizeof(double) * std::max(nh, 1LL)));
-  CUDA_TRY(cudaMalloc(&P.d_beta, sizeof(double) * std::max(nb, 1LL)));
+  CUDA_TRY(pool_new(&P.d_rec, sizeof(IsingSiteRecipe) * P.nrec));
+  CUDA_TRY(pool_new(&P.d_w, sizeof(double) * std::max(nw, 1LL)));
+  CUDA_TRY(pool_new(&P.d_h, sizeof(double) * std::max(nh, 1LL)));
+  CUDA_TRY(pool_new(&P.d_beta, sizeof(double) * std::max(nb, 1LL)));
   CUDA_TRY(cudaMemcpy(P.d_rec, b->im.recipes.data(), sizeof(IsingSiteRecipe) * P.nrec, cudaMemcpyHostToDevice));
   return params_restore(b, nullptr);
 }

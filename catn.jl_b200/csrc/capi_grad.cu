@@ -71,8 +71,10 @@ __global__ void __launch_bounds__(kThreads) catn_grad_kernel(
 long long grad_arena(long long forward_arena, int slots) {
   long long a = forward_arena / 2 * 5;
   size_t freeb = 0, totalb = 0;
-  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && slots > 0)
+  if (cudaMemGetInfo(&freeb, &totalb) == cudaSuccess && slots > 0) {
+    freeb += pool_cached_bytes(false);   // cached blocks are given back when an allocation needs them
     a = std::min(a, (long long)(freeb / 2 / (size_t)slots) & ~255LL);
+  }
   return a;
 }
 
@@ -87,8 +89,8 @@ catn_status grad_prepare(const Image& im, long long arena, int max_slots, GradRu
     return s;
   }
   const size_t gbytes = sizeof(double) * (im.dat.size() + 1);
-  CUDA_TRY(cudaMalloc(&g->d_gimg, gbytes));
-  CUDA_TRY(cudaMallocHost(&g->h_gimg, gbytes));
+  CUDA_TRY(pool_new(&g->d_gimg, gbytes));
+  CUDA_TRY(pool_new(&g->h_gimg, gbytes, true));
   CUDA_TRY(cudaFuncSetAttribute(catn_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytesTc));
   return CATN_OK;
 }
@@ -147,8 +149,8 @@ namespace catn_capi {
 void grad_release(GradRun* g) {
   if (!g) return;
   g->R.release();
-  cudaFree(g->d_gimg);
-  cudaFreeHost(g->h_gimg);
+  pool_free(g->d_gimg);
+  pool_free(g->h_gimg);
   delete g;
 }
 

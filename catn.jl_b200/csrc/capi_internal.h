@@ -63,6 +63,17 @@ const char* status_text(int s);
 // Argument checks shared by every create/contract entry point.
 catn_status check_params(const catn_params* p);
 
+// Blocks of the process-wide cache (pool.cu): device memory, or pinned host
+// memory with `host`.  pool_free keeps the block for a later request (or
+// frees it); pointers that did not come from pool_alloc are ignored.
+cudaError_t pool_alloc(void** p, size_t bytes, bool host = false);
+void pool_free(void* p);
+size_t pool_cached_bytes(bool host);
+template <typename T>
+inline cudaError_t pool_new(T** p, size_t bytes, bool host = false) {
+  return pool_alloc((void**)p, bytes, host);
+}
+
 // Device copy of an Image plus slots and results.  The input image is packed
 // into one pinned host buffer and one device buffer, so an upload is a single
 // host-to-device copy.
@@ -89,8 +100,9 @@ struct DeviceRun {
   long long input_bytes = 0;
 
   void release() {
-    cudaFreeHost(h_input);
-    cudaFree(d_input); cudaFree(d_slots); cudaFree(d_res); cudaFree(d_trace); cudaFree(d_queue); cudaFree(d_board);
+    pool_free(h_input);
+    pool_free(d_input); pool_free(d_slots); pool_free(d_res); pool_free(d_trace); pool_free(d_queue);
+    pool_free(d_board);
     h_input = nullptr; d_input = nullptr; d_slots = nullptr; d_res = nullptr; d_trace = nullptr; d_queue = nullptr;
     d_board = nullptr;
     d_desc = nullptr; d_order = nullptr; d_i64 = nullptr; d_i32 = nullptr; d_dat = nullptr;
@@ -153,7 +165,7 @@ struct IsingParams {
   long long nrec = 0, nw = 0, nh = 0, nb = 0;
   bool on_device = false;
   void release() {
-    cudaFree(d_rec); cudaFree(d_w); cudaFree(d_h); cudaFree(d_beta);
+    pool_free(d_rec); pool_free(d_w); pool_free(d_h); pool_free(d_beta);
     d_rec = nullptr; d_w = d_h = d_beta = nullptr;
   }
 };

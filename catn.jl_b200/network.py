@@ -214,3 +214,14 @@ def tc_matmul(A, B):
     lib = L.load()
     L.check(lib, lib.catn_tc_matmul(M, N, K, L.ptr(A), L.ptr(B), L.ptr(C)))
     return C
+
+
+def release_cached_memory():
+    """Free the device and pinned host blocks the library keeps from
+    destroyed networks and batches (``catn_release_cached_memory``), e.g.
+    before handing the memory to another library.  Returns the device bytes
+    that were kept."""
+    lib = L.load()
+    kept = int(lib.catn_cached_bytes(0))
+    L.check(lib, lib.catn_release_cached_memory())
+    return kept

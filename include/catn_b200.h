@@ -371,6 +371,17 @@ catn_status catn_batch_grad_results(catn_batch* b, catn_result* results, double*
                                     void* stream);
 
 /* Thread-local message of the last failure (always NUL-terminated). */
+/* Device and pinned host blocks of destroyed networks and batches are kept
+ * by the library for the next network or batch (no reference counterpart:
+ * Julia's GC owns the reference's arrays).  A network created and destroyed
+ * in a loop then pays no cudaMalloc / cudaFree per iteration.  Up to 8 blocks
+ * per device and kind are kept; an allocation that finds the device full
+ * frees them first.  catn_release_cached_memory frees every kept block (for
+ * callers that hand the memory to other libraries); catn_cached_bytes
+ * reports the bytes kept (host != 0: pinned host memory). */
+catn_status catn_release_cached_memory(void);
+int64_t catn_cached_bytes(int32_t host);
+
 size_t catn_last_error(char* buf, size_t cap);
 
 /* Library build string (arch, version). */
