@@ -13,6 +13,11 @@
 
 using namespace catn;
 
+// Shared-memory workspace that the block route's items and the blocked QR's
+// panel items use (the library's kernels always have at least this much).
+static constexpr long long kItemWsDoubles =
+    kBlockWsDoubles > kPanelWsDoubles + kPanelW ? kBlockWsDoubles : kPanelWsDoubles + kPanelW;
+
 static int run_image(Image& im, long long arena_bytes, catn_result* res, int* trace) {
   if (im.desc.empty()) return CATN_EINVAL;
   SlotLayout L = make_layout(im.nmax, default_maxs(im), im.emax + 64, arena_bytes);
@@ -31,8 +36,9 @@ static int run_image(Image& im, long long arena_bytes, catn_result* res, int* tr
   // CATN_HOSTCHECK_SWS overrides the capacity (0 sends every SVD through the
   // large-matrix path, including its rank-revealing truncation)
   if (const char* e = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(e);
-  // at least the block route's item workspace, whatever capacity is reported
-  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
+  // at least the block route's and the blocked QR's item workspaces (as the
+  // library's shared memory always holds), whatever capacity is reported
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kItemWsDoubles));
   // CATN_HOSTCHECK_JOB=1 sends the Jacobi sweeps of every SVD on the global
   // path through the shared-job protocol (no helpers: the team claims all);
   // CATN_HOSTCHECK_BLOCK_MIN sets the smallest factor on the block route
@@ -92,8 +98,9 @@ int catn_hostcheck_ising_grad(const catn_params* p, int n, int n_edges, const in
   T.tmem = 0;
   long long sws_doubles = (98 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
   if (const char* ev = std::getenv("CATN_HOSTCHECK_SWS")) sws_doubles = std::atoll(ev);
-  // at least the block route's item workspace, whatever capacity is reported
-  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
+  // at least the block route's and the blocked QR's item workspaces (as the
+  // library's shared memory always holds), whatever capacity is reported
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kItemWsDoubles));
   std::vector<double> gimg(im.dat.size() + 1, 0.0);
   run_instance_grad(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, gimg.data(),
                     sws.data(), sws_doubles);
@@ -120,7 +127,7 @@ int catn_hostcheck_braket(const catn_params* p, int n, const int* ndims, const l
   T.tcs = nullptr;
   T.tmem = 0;
   long long sws_doubles = (98 * 1024 - 64 * 8 - GEMM_STAGE_BYTES) / 8;
-  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kBlockWsDoubles));
+  std::vector<double> sws((size_t)std::max<long long>(sws_doubles, kItemWsDoubles));
   std::vector<int> tr((size_t)im.trace_total + 8);
   run_instance_braket(T, sp, L, im.desc[0], im.i64.data(), im.i32.data(), im.dat.data(), res, tr.data(), sws.data(),
                       sws_doubles);

@@ -170,6 +170,15 @@ for L, kw in [(6, dict(Dmax=8, chi=32)), (6, dict(Dmax=4, chi=16, compress=True)
     e = X.square_edges(L)
     st, res, rows = T.run_ising(lib, L*L, e, r.normal(size=len(e)), r.normal(0, .1, L*L), 1.0, **kw)
     assert st == 0, st
+# every SVD on the global path, the block route and the blocked QR through the
+# shared-job protocol (the item workspaces at their smallest)
+import os
+os.environ.update(CATN_HOSTCHECK_SWS="0", CATN_HOSTCHECK_BLOCK_MIN="16", CATN_HOSTCHECK_JOB="1",
+                  CATN_HOSTCHECK_BLOCKED_QR_MIN="16")
+e = X.square_edges(10)
+st, res, rows = T.run_ising(lib, 100, e, r.normal(size=len(e)), r.normal(0, .1, 100), 1.3, Dmax=16, chi=96,
+                            svd_route="block")
+assert st == 0, st
 print("asan-ok")
 """
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1",
