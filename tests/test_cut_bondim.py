@@ -216,3 +216,28 @@ def test_gpu_cut_of_a_low_rank_bond_is_exact(catn, opt):
     if got.shape != ref.shape or not np.allclose(got, ref, atol=1e-8):
         got = got.T
     np.testing.assert_allclose(got, ref, atol=1e-8)
+
+
+@pytest.mark.gpu
+def test_gpu_cut_on_an_ising_network_and_gradient_rejection(catn):
+    """Cuts apply to Ising networks too (catn_ising_create's MPS form): the
+    same cuts on the oracle's Ising network give the same errors and lnZ.  A
+    gradient run of a cut network is rejected (the cuts are not taped)."""
+    from oracle import exact as X
+    from oracle import ising as OI
+    r = np.random.default_rng(8)
+    L_ = 5
+    n = L_ * L_
+    e = X.square_edges(L_)
+    w, h = r.normal(size=len(e)), r.normal(0, 0.1, n)
+    kw = dict(Dmax=1, chi=16)
+    cuts = [(7, 1, 1), (13, 2, 1)]
+    ref = OI.ising_network(n, e, w, h, 0.7, **kw)
+    errs = [ON.cut_bondim_opt(ref, i, k) for i, k, _ in cuts]
+    lz, _, _ = ON.contraction(ref)
+    net = catn.ising_network(n, e, w, h, 0.7, **kw)
+    got = [catn.cut_bondim_opt(net, i, k) for i, k, _ in cuts]
+    assert got == pytest.approx(errs, rel=1e-10, abs=1e-13)
+    with pytest.raises(catn.CatnError):
+        catn.gradient(net)
+    assert catn.contraction(net)[0] == pytest.approx(lz, rel=1e-10)
