@@ -286,7 +286,7 @@ def main():
                     help="also run the 32x32 Gaussian lattice at full size (forward, checkpointed adjoint, one "
                          "central difference, 8 pinned edges; several minutes)")
     ap.add_argument("--no-configs", action="store_true",
-                    help="skip the 8x8 ferromagnet and the reduced 32x32 Gaussian-lattice legs")
+                    help="skip the 8x8 ferromagnet, the reduced 32x32 Gaussian-lattice and the reduced PEPS legs")
     ap.add_argument("--c2-scalar", action="store_true",
                     help="also time the n=200 leg on the scalar Jacobi route (about 40 s per beta)")
     ap.add_argument("--no-c2-oracle", action="store_true",
@@ -476,6 +476,7 @@ def main():
     if world == 1 and not args.no_configs:
         out["ferro8"] = c1_leg(catn)
         out["gaussian_lattice_reduced"] = c4_reduced_leg(catn)
+        out["peps_reduced"] = peps_reduced_leg(catn)
     print(json.dumps(out))
     if dist:
         dist.barrier()
@@ -657,6 +658,31 @@ def c4_reduced_leg(catn, L=10, seed=4):
             "timing": "host wall clock around the public calls (network upload, launches and read-back inside), "
                       "after one warm-up call of each; pinning batched = one IsingBatch.run() over every pinned network, "
                       "sequential = ising_network + contraction per pinned network"}
+
+
+def peps_reduced_leg(catn, L=6, D=3, Dmax=64, chi=128, seed=506):
+    """The 16 x 16 PEPS norm configuration reduced: the fused double layer of
+    a random real L x L PEPS (d = 2, bond D, graphs.peps_double_layer, the
+    construction of examples/peps_norm.jl:71-81) contracted as a
+    TensorNetwork at Dmax / chi, in FP64 on the scalar and the block Jacobi
+    routes and in split precision, each timed through the public calls; the
+    split form's lnZ against the FP64 one."""
+    from catn_b200 import graphs
+    _, _, et, ei = graphs.peps_double_layer(L, D, 2, np.random.default_rng(seed))
+    out = {"workload": f"{L}x{L} PEPS double layer, d=2, D={D} (bonds {D * D}), Dmax={Dmax}, chi={chi}, seed {seed}",
+           "timing": "host wall clock around TensorNetwork + catn.contraction", "forms": {}}
+    ref = None
+    for name, kw in (("fp64_scalar", dict(svd_route="scalar")), ("fp64_block", dict(svd_route="block")),
+                     ("split", dict(precision="split"))):
+        t0 = time.perf_counter()
+        net = catn.TensorNetwork(et, ei, Dmax=Dmax, chi=chi, **kw)
+        lnZ, err, psi = catn.contraction(net)
+        dt = time.perf_counter() - t0
+        ref = lnZ if ref is None else ref
+        out["forms"][name] = {"s": round(dt, 3), "lnZ": lnZ, "truncation_err": err, "psi": psi,
+                              "abs_dlnZ_vs_fp64_scalar": abs(lnZ - ref),
+                              "algorithmic_tflops": round(net.result.flops / dt / 1e12, 5)}
+    return out
 
 
 def c4_full_leg(catn, L=32, seed=32, fd_edges=1, pin_edges=4):
