@@ -119,7 +119,10 @@ struct GradRun {
 };
 
 // Sizes slots and packs the image (capi.cu).
-catn_status prepare(const catn::Image& im, long long arena_bytes, int max_slots, DeviceRun& R);
+// `single_forward`: R is one network that catn_contract launches (its auto
+// SVD route may then take the block route, see capi.cu).
+catn_status prepare(const catn::Image& im, long long arena_bytes, int max_slots, DeviceRun& R,
+                    bool single_forward = false);
 catn_status upload(DeviceRun& R, cudaStream_t st);
 // Helper pool and sharing thresholds of a launch of R from the tuning table
 // in force (capi.cu); `grad` selects the gradient launches' pool.  One

@@ -78,8 +78,12 @@ typedef struct {
                         * every singular-value cutoff test, the Dmax cut
                         * and lnZ stay FP64                              */
   int32_t svd_route;   /* large SVDs (not held in shared memory):
-                        * 0 = auto (precision 0: scalar Jacobi; precision 1:
-                        *     block Jacobi from the tuning table's size on),
+                        * 0 = auto (precision 0: block Jacobi from the tuning
+                        *     table's size on for a network that
+                        *     catn_contract contracts on its own, the whole
+                        *     GPU helping it; scalar Jacobi in batches and
+                        *     gradient runs; precision 1: block Jacobi from
+                        *     the tuning table's size on),
                         * 1 = scalar one-sided Jacobi on the pivoted-QR
                         *     factor (the FP64 route of earlier releases,
                         *     bit for bit),
