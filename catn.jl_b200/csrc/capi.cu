@@ -450,6 +450,7 @@ catn_status catn_braket_create(const catn_params* p, int32_t n, const int32_t* n
 catn_status catn_contract(catn_net* net, catn_result* res, int32_t* trace, int32_t trace_cap) {
   if (!net || !res) return fail(CATN_EINVAL, "NULL argument");
   if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
+  if (net->unusable) return fail(CATN_ESTATE, "network lost its device copy in a failed cut_bondim!");
   cudaStream_t st = 0;
   if (catn_status s = upload(net->R, st)) return s;
   if (net->im.desc[0].kind == 2) {
@@ -473,6 +474,7 @@ catn_status catn_cut_bondim(catn_net* net, int32_t i, int32_t idx_j_in_i, int32_
   if (!net || !err) return fail(CATN_EINVAL, "NULL argument");
   *err = 0.0;
   if (net->contracted) return fail(CATN_ESTATE, "network already contracted (contraction! consumes tn)");
+  if (net->unusable) return fail(CATN_ESTATE, "network lost its device copy in a failed cut_bondim!");
   const InstDesc& D0 = net->im.desc[0];
   if (D0.kind == 2) return fail(CATN_EINVAL, "cut_bondim!: BraKet networks have no bond cuts");
   if (D0.P.Dmax < 0) return CATN_OK;   // tensor_network.jl:344 (and :401): a no-op returning 0.0
@@ -502,7 +504,7 @@ catn_status catn_cut_bondim(catn_net* net, int32_t i, int32_t idx_j_in_i, int32_
   if (s != CATN_OK) {
     net->im.set_cuts(net->cuts);
     net->R.release();
-    if (prepare(net->im, net->arena, 1, net->R, true) != CATN_OK) net->contracted = true;   // unusable from here
+    if (prepare(net->im, net->arena, 1, net->R, true) != CATN_OK) net->unusable = true;
     return s;
   }
   cudaStream_t st = 0;

@@ -152,6 +152,7 @@ struct catn_net {
   long long arena = 0;      // arena bytes of the slot (after defaults)
   std::vector<int> cuts;    // cut_bondim! calls so far: i, idx_j_in_i, opt
   bool contracted = false;
+  bool unusable = false;    // a failed cut left no device copy to contract
   catn_capi::GradRun* grad = nullptr;
 };
 

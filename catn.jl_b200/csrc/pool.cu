@@ -8,7 +8,7 @@
 // contract networks one after another (the reference's pinning loops, a
 // Julia loop over disorder samples) pay that every time.  A freed block is
 // kept here instead, per device and kind, and handed to the next request it
-// covers (the smallest such block).  At most kPoolBlocks blocks per device
+// covers (the smallest such block, at most twice the request).  At most kPoolBlocks blocks per device
 // and kind are kept; an allocation that runs out of device memory frees the
 // cached blocks of its device and tries again; catn_release_cached_memory()
 // frees them all.  Blocks are handed out with their old contents: every
@@ -70,7 +70,10 @@ cudaError_t pool_alloc(void** p, size_t bytes, bool host) {
   int best = -1;
   for (size_t q = 0; q < g_free.size(); ++q) {
     const Block& b = g_free[q];
-    if (b.dev == dev && b.host == host && b.bytes >= bytes && (best < 0 || b.bytes < g_free[best].bytes))
+    // a block at most twice the request (plus 1 MiB): a small request never
+    // takes a large block that a later large request would need
+    if (b.dev == dev && b.host == host && b.bytes >= bytes && b.bytes <= 2 * bytes + (1u << 20) &&
+        (best < 0 || b.bytes < g_free[best].bytes))
       best = (int)q;
   }
   if (best >= 0) {
