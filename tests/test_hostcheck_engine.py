@@ -179,6 +179,13 @@ e = X.square_edges(10)
 st, res, rows = T.run_ising(lib, 100, e, r.normal(size=len(e)), r.normal(0, .1, 100), 1.3, Dmax=16, chi=96,
                             svd_route="block")
 assert st == 0, st
+for k in ("CATN_HOSTCHECK_SWS", "CATN_HOSTCHECK_BLOCK_MIN", "CATN_HOSTCHECK_JOB", "CATN_HOSTCHECK_BLOCKED_QR_MIN"):
+    del os.environ[k]
+# cut_bondim! / cut_bondim_opt! replayed before a contraction
+import test_cut_bondim as TC
+ts, ixs = TC.grid(3, 4, 11)
+st, res, _ = TC.host_run(lib, ts, ixs, TC.CUTS, 0, **TC.KW)
+assert st == 0, st
 print("asan-ok")
 """
     env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:abort_on_error=1", UBSAN_OPTIONS="halt_on_error=1",
