@@ -692,6 +692,6 @@ size_t catn_last_error(char* buf, size_t cap) {
   return n;
 }
 
-const char* catn_version(void) { return "catn_b200 0.1 (sm_100a, fp64 engine)"; }
+const char* catn_version(void) { return "catn_b200 0.2 (sm_100a: FP64 engine, 3xTF32 tcgen05 split precision)"; }
 
 }  // extern "C"
