@@ -511,17 +511,20 @@ catn_status catn_cut_bondim(catn_net* net, int32_t i, int32_t idx_j_in_i, int32_
   catn_result res;
   std::memset(&res, 0, sizeof(res));
   if ((s = upload(net->R, st)) == CATN_OK && (s = launch(net->R, st)) == CATN_OK) {
-    CUDA_TRY(cudaMemcpyAsync(&res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    cudaError_t e = cudaMemcpyAsync(&res, net->R.d_res, sizeof(catn_result), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) s = cuda_fail(e, "cut_bondim! result");
   }
-  // the host copy of the image goes back to contraction launches
-  ((InstDesc*)net->R.h_input)[0].cut_only = 0;
-  if (s != CATN_OK) return s;
-  if (res.status != CATN_OK) {
-    // the failed cut is dropped: the uploaded descriptor replays the others
+  if (s == CATN_OK && res.status != CATN_OK)
+    s = fail((catn_status)res.status, std::string(name) + " failed: " + status_text(res.status));
+  // the host copy of the image goes back to contraction launches, without
+  // the new cut when it did not complete (the earlier cuts are replayed)
+  InstDesc* hd = (InstDesc*)net->R.h_input;
+  hd[0].cut_only = 0;
+  if (s != CATN_OK) {
     net->im.set_cuts(net->cuts);
-    ((InstDesc*)net->R.h_input)[0].n_cuts = net->im.desc[0].n_cuts;
-    return fail((catn_status)res.status, std::string(name) + " failed: " + status_text(res.status));
+    hd[0].n_cuts = net->im.desc[0].n_cuts;
+    return s;
   }
   net->cuts = cuts;
   *err = res.err;
