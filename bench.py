@@ -599,19 +599,45 @@ def c1_leg(catn):
             "timing": "CUDA events around catn.contraction (upload, one launch, read-back), mean of 3 after one warm-up"}
 
 
-def c4_reduced_leg(catn, L=10, seed=4):
+def _oracle_fixture_time(name):
+    """FP64 oracle on a frozen configuration (spawned process, all host cores
+    to BLAS); returns (lnZ, seconds)."""
+    from oracle import ising as OI, network as ON
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", name + ".json")))
+    t0 = time.perf_counter()
+    if name == "peps6":
+        import __graft_entry__
+        __graft_entry__.load_package()
+        from catn_b200 import graphs
+        _, _, et, ei = graphs.peps_double_layer(d["L"], d["D"], d["d"], np.random.default_rng(d["seed"]))
+        tn = ON.TensorNetwork.from_tensors(et, ei, **d["params"])
+    else:
+        tn = OI.ising_network(d["n"], d["edges"], d["weights"], d["fields"], d["beta"], **d["params"])
+    lnZ, _, _ = ON.contraction(tn)
+    return lnZ, time.perf_counter() - t0
+
+
+def _time_oracle(name):
+    with mp.get_context("spawn").Pool(1) as pool:
+        lz, secs = pool.apply(_oracle_fixture_time, (name,))
+    return {"s": round(secs, 3), "lnZ": lz, "cores": host_cores(),
+            "what": "the oracle port (numpy/OpenBLAS, all cores to BLAS), same network"}
+
+
+def c4_reduced_leg(catn):
     """The 32 x 32 Gaussian lattice configuration (J ~ N(0,1), h ~ N(0,0.2^2),
-    beta 1, Dmax 48, chi 256) at L = 10: the forward contraction, the device
-    adjoint of lnZ (whole tape, and checkpointed every 64 steps), and the
-    reference's pinning definition of every <s_k> and <s_i s_j> (1 + 2n +
-    4|E| networks, all of them: as one batch, and one network at a time as
-    the reference's loop runs them), each timed through the public calls;
-    the observables of the two routes are compared on every spin and edge."""
-    from catn_b200.graphs import square_edges
-    r = np.random.default_rng(seed)
-    n = L * L
-    edges = square_edges(L)
-    w, h, beta = r.normal(size=len(edges)), r.normal(0, 0.2, n), 1.0
+    beta 1, Dmax 48, chi 256) at L = 10 (inputs and the FP64 oracle's lnZ and
+    trace frozen in tests/golden/gaussian10.json): the forward contraction
+    against the oracle, the device adjoint of lnZ (whole tape, and
+    checkpointed every 64 steps), and the reference's pinning definition of
+    every <s_k> and <s_i s_j> (1 + 2n + 4|E| networks, all of them: as one
+    batch, and one network at a time as the reference's loop runs them),
+    each timed through the public calls; the observables of the two routes
+    are compared on every spin and edge."""
+    d = json.load(open(os.path.join(ROOT, "tests", "golden", "gaussian10.json")))
+    L, seed, n, beta = d["L"], 4, d["n"], d["beta"]
+    edges = [tuple(e) for e in d["edges"]]
+    w, h = np.array(d["weights"]), np.array(d["fields"])
     kw = dict(Dmax=48, chi=256)
     catn.contraction(catn.ising_network(n, edges, w, h, beta, **kw))   # warm-up
     t0 = time.perf_counter()
@@ -643,9 +669,15 @@ def c4_reduced_leg(catn, L=10, seed=4):
     lz_seq = [catn.contraction(catn.ising_network(n, edges, w, h, beta, pos1=p1, val1=v1, pos2=p2, val2=v2, **kw))[0]
               for (p1, v1, p2, v2) in pins]
     t_seq = time.perf_counter() - t0
+    tn = catn.ising_network(n, edges, w, h, beta, **kw)
+    catn.adapt(catn.B200, tn, trace=True)
+    lz_t = catn.contraction(tn, trace=True)[0]
+    rows = [[int(x) for x in r_[:7]] for r_ in tn.trace]
+    vs_oracle = {"abs_dlnZ_per_site": abs(lz_t - d["oracle"]["lnZ"]) / n,
+                 "trace_identical": rows == d["oracle"]["trace"], "oracle_cpu": _time_oracle("gaussian10")}
     return {"workload": f"{L}x{L} open lattice (the 32x32 configuration reduced), J~N(0,1), h~N(0,0.2^2), beta=1, "
-                        f"Dmax=48, chi=256, seed {seed}",
-            "forward_s": round(t_fwd, 4), "lnZ": lnZ, "err": err,
+                        f"Dmax=48, chi=256, seed {seed} (tests/golden/gaussian10.json)",
+            "forward_s": round(t_fwd, 4), "lnZ": lnZ, "err": err, "vs_oracle": vs_oracle,
             "adjoint_s": round(t_adj, 4), "adjoint_ckpt64_s": round(grads[64][0], 4),
             "ckpt64_gradients_identical": bool(np.array_equal(grads[64][2], dw) and np.array_equal(grads[64][3], dh)),
             "pinning_networks": len(pins), "pinning_s": round(t_pin, 4),
@@ -660,15 +692,18 @@ def c4_reduced_leg(catn, L=10, seed=4):
                       "sequential = ising_network + contraction per pinned network"}
 
 
-def peps_reduced_leg(catn, L=6, D=3, Dmax=64, chi=128, seed=506):
+def peps_reduced_leg(catn):
     """The 16 x 16 PEPS norm configuration reduced: the fused double layer of
     a random real L x L PEPS (d = 2, bond D, graphs.peps_double_layer, the
     construction of examples/peps_norm.jl:71-81) contracted as a
     TensorNetwork at Dmax / chi, in FP64 on the scalar and the block Jacobi
-    routes and in split precision, each timed through the public calls; the
-    split form's lnZ against the FP64 one."""
+    routes and in split precision, each timed through the public calls; every
+    form's lnZ and trace against the FP64 oracle's (frozen in
+    tests/golden/peps6.json), whose own time on the host cores is measured."""
     from catn_b200 import graphs
-    _, _, et, ei = graphs.peps_double_layer(L, D, 2, np.random.default_rng(seed))
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "peps6.json")))
+    L, D, seed, Dmax, chi = g["L"], g["D"], g["seed"], g["params"]["Dmax"], g["params"]["chi"]
+    _, _, et, ei = graphs.peps_double_layer(L, D, g["d"], np.random.default_rng(seed))
     out = {"workload": f"{L}x{L} PEPS double layer, d=2, D={D} (bonds {D * D}), Dmax={Dmax}, chi={chi}, seed {seed}",
            "timing": "host wall clock around TensorNetwork + catn.contraction", "forms": {}}
     ref = None
@@ -676,12 +711,17 @@ def peps_reduced_leg(catn, L=6, D=3, Dmax=64, chi=128, seed=506):
                      ("split", dict(precision="split"))):
         t0 = time.perf_counter()
         net = catn.TensorNetwork(et, ei, Dmax=Dmax, chi=chi, **kw)
-        lnZ, err, psi = catn.contraction(net)
+        catn.adapt(catn.B200, net, trace=True)
+        lnZ, err, psi = catn.contraction(net, trace=True)
         dt = time.perf_counter() - t0
         ref = lnZ if ref is None else ref
+        rows = [[int(x) for x in r_[:7]] for r_ in net.trace]
         out["forms"][name] = {"s": round(dt, 3), "lnZ": lnZ, "truncation_err": err, "psi": psi,
                               "abs_dlnZ_vs_fp64_scalar": abs(lnZ - ref),
+                              "abs_dlnZ_vs_oracle": abs(lnZ - g["oracle"]["lnZ"]),
+                              "trace_identical_to_oracle": rows == g["oracle"]["trace"],
                               "algorithmic_tflops": round(net.result.flops / dt / 1e12, 5)}
+    out["oracle_cpu"] = _time_oracle("peps6")
     return out
 
 

@@ -17,6 +17,14 @@ Fixtures (seeded synthetic inputs with the workload shapes):
                          chi 128): oracle lnZ/err/psi/maxdim/trace (about 35 s
                          of oracle time per beta, hence frozen here)
 
+  gaussian10.json        the 32x32 Gaussian configuration reduced to L = 10
+                         (J~N(0,1), h~N(0,0.2^2), beta 1, Dmax 48, chi 256,
+                         seed 4, the bench's reduced leg): inputs and oracle
+                         lnZ/err/psi/maxdim/trace
+  peps6.json             the 16x16 PEPS norm configuration reduced to a 6x6
+                         double layer (d 2, D 3, Dmax 64, chi 128, seed 506,
+                         graphs.peps_double_layer): oracle lnZ/err/psi/trace
+
     python tests/golden/make_golden.py [name ...]   # regenerate only these
 The trace row format is the device's (see include/catn_b200.h).
 """
@@ -62,6 +70,36 @@ def spinglass(count, seed):
     return out
 
 
+def _trace_rows():
+    return [[i, j, int(ri) | (int(rj) << 1), len(d), fnv(d), len(s), fnv(s)] for (i, j, ri, rj, d, s) in ON.TRACE]
+
+
+def gaussian10():
+    rng = np.random.default_rng(4)
+    L = 10
+    e = X.square_edges(L)
+    w = rng.normal(size=len(e)).tolist()
+    h = rng.normal(0, 0.2, L * L).tolist()
+    d = dict(L=L, n=L * L, edges=e, weights=w, fields=h, beta=1.0, params=dict(Dmax=48, chi=256, cutoff=1e-15))
+    d["oracle"] = run(L * L, e, w, h, 1.0, Dmax=48, chi=256)
+    json.dump(d, open(os.path.join(HERE, "gaussian10.json"), "w"))
+
+
+def peps6():
+    import __graft_entry__
+    __graft_entry__.load_package()
+    from catn_b200 import graphs
+    d = dict(L=6, D=3, d=2, seed=506, params=dict(Dmax=64, chi=128, cutoff=1e-15))
+    _, _, et, ei = graphs.peps_double_layer(6, 3, 2, np.random.default_rng(506))
+    ON.TRACE = []
+    tn = ON.TensorNetwork.from_tensors(et, ei, Dmax=64, chi=128)
+    lnZ, err, psi = ON.contraction(tn)
+    rows = _trace_rows()
+    ON.TRACE = None
+    d["oracle"] = dict(lnZ=lnZ, err=err, psi=psi, maxdim=tn.maxdim_intermediate, steps=len(rows), trace=rows)
+    json.dump(d, open(os.path.join(HERE, "peps6.json"), "w"))
+
+
 def rrg200():
     rng = np.random.default_rng(200)
     e = X.random_regular_graph(200, 3, rng)
@@ -77,6 +115,10 @@ def main():
     if only:
         if "rrg200" in only:
             rrg200()
+        if "gaussian10" in only:
+            gaussian10()
+        if "peps6" in only:
+            peps6()
         print("golden fixtures written:", " ".join(sorted(only)))
         return
     e = X.square_edges(8)
