@@ -11,7 +11,9 @@
 // covers (the smallest such block, at most twice the request).  At most kPoolBlocks blocks per device
 // and kind are kept; an allocation that runs out of device memory frees the
 // cached blocks of its device and tries again; catn_release_cached_memory()
-// frees them all.  Blocks are handed out with their old contents: every
+// frees them all (a program that resets the device calls it before the
+// reset: the kept addresses do not survive a reset, and nothing here can
+// tell).  Blocks are handed out with their old contents: every
 // user initialises what it reads (the engine resets a slot before loading an
 // instance, the host image is cleared before packing).
 #include <cuda_runtime.h>

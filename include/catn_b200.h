@@ -382,7 +382,9 @@ catn_status catn_batch_grad_results(catn_batch* b, catn_result* results, double*
  * per device and kind are kept; an allocation that finds the device full
  * frees them first.  catn_release_cached_memory frees every kept block (for
  * callers that hand the memory to other libraries); catn_cached_bytes
- * reports the bytes kept (host != 0: pinned host memory). */
+ * reports the bytes kept (host != 0: pinned host memory).  A program that
+ * resets a device (cudaDeviceReset) calls catn_release_cached_memory before
+ * the reset: kept blocks do not survive it, and the library cannot tell. */
 catn_status catn_release_cached_memory(void);
 int64_t catn_cached_bytes(int32_t host);
 
