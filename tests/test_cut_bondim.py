@@ -241,3 +241,36 @@ def test_gpu_cut_on_an_ising_network_and_gradient_rejection(catn):
     with pytest.raises(catn.CatnError):
         catn.gradient(net)
     assert catn.contraction(net)[0] == pytest.approx(lz, rel=1e-10)
+
+
+def _random_cuts(ts, ixs, count, seed):
+    """`count` random (node, leg, opt) cuts of real bonds with a spectral gap
+    at Dmax on the oracle's state (the first seed from `seed` on that has
+    one)."""
+    nbr_counts = [len(ix) for ix in ixs]
+    for s in range(seed, seed + 50):
+        r = np.random.default_rng(s)
+        cuts = []
+        for _ in range(count):
+            i = int(r.integers(1, len(ts) + 1))
+            cuts.append((i, int(r.integers(1, nbr_counts[i - 1] + 1)), int(r.integers(0, 2))))
+        if min(cut_gaps(ts, ixs, cuts, KW["Dmax"])) > 1e-3:
+            return cuts
+    raise AssertionError("no gapped cut sequence found")
+
+
+def test_host_random_cut_sequences_match_oracle(host):
+    """Twelve random cuts on a closed 4 x 4 grid (bond dimension 4, Dmax 3),
+    replayed before the contraction: each cut's discarded sum, then the cut
+    network's trace and lnZ, against the oracle."""
+    ts, ixs = grid(4, 4, 23)
+    cuts = _random_cuts(ts, ixs, 12, 100)
+    errs, (lz, err, psi), orows = oracle_run(ts, ixs, cuts, **KW)
+    for k in (3, 7, 11):
+        st, res, _ = host_run(host, ts, ixs, cuts[: k + 1], 1, **KW)
+        assert st == 0
+        assert res.err == pytest.approx(errs[k], rel=1e-10, abs=1e-13)
+    st, res, trows = host_run(host, ts, ixs, cuts, 0, **KW)
+    assert st == 0
+    assert trows == orows
+    assert res.lnZ == pytest.approx(lz, rel=1e-10)
