@@ -106,3 +106,23 @@ def test_random_regular_spin_glass_block_route_golden(catn, precision, bar):
         assert psi == ref["psi"]
         assert maxdim == ref["maxdim"]
         assert abs(err - ref["err"]) <= 1e-6 + (1e-6 if precision == "fp64" else 1e-3) * abs(ref["err"])
+
+
+def test_gaussian_lattice_reduced_golden(catn):
+    """The 32 x 32 Gaussian configuration at L = 10 (Dmax 48, chi 256)."""
+    d = _load("gaussian10.json")
+    _check(_contract(catn, d, d["beta"], dict(Dmax=48, chi=256)), d["oracle"], d["n"])
+
+
+def test_peps_double_layer_6x6_golden(catn):
+    """The 16 x 16 PEPS norm configuration reduced to a 6 x 6 double layer
+    (d 2, D 3, Dmax 64, chi 128), contracted as one network on the default
+    route."""
+    import numpy as np
+    from catn_b200 import graphs
+    d = _load("peps6.json")
+    _, _, et, ei = graphs.peps_double_layer(d["L"], d["D"], d["d"], np.random.default_rng(d["seed"]))
+    tn = catn.TensorNetwork(et, ei, Dmax=d["params"]["Dmax"], chi=d["params"]["chi"])
+    lnZ, err, psi = catn.contraction(tn, trace=True)
+    rows = [[int(x) for x in r[:7]] for r in tn.trace]
+    _check((lnZ, err, psi, tn.maxdim_intermediate, rows), d["oracle"], d["L"] * d["L"])
