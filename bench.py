@@ -202,6 +202,15 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def _secondary(out, key, fn):
+    """Run one secondary leg into out[key]; a failure is recorded there
+    instead of ending the run before the headline line is printed."""
+    try:
+        out[key] = fn()
+    except Exception as e:  # noqa: BLE001 -- any failure of a side leg is reported, not raised
+        out[key] = {"error": f"{type(e).__name__}: {e}"}
+
+
 def load_bf16_peak(key="bf16_tflops_sustained"):
     """Dense bf16 GEMM TFLOP/s from MEASURED_PEAKS.json (the sustained figure
     by default: the launches it is compared with run for seconds), or None."""
@@ -460,23 +469,26 @@ def main():
     if cpu:
         out["cpu_baseline"] = cpu
     if world == 1 and not args.no_grad:
-        out["grad"] = grad_leg(catn, batch, insts, value, stream, sh)
-    if world == 1 and args.plain_seconds > 0:
+        _secondary(out, "grad", lambda: grad_leg(catn, batch, insts, value, stream, sh))
+
+    def plain_leg():
         rate, cnt, dev = plain_form_rate(insts, [r.lnZ for r in res], args.plain_seconds)
-        out["plain_gpu_form"] = {
+        return {
             "value": round(rate, 3), "unit": "instances/s", "value_over_plain": round(value / rate, 1),
             "max_abs_dlnZ_per_spin_vs_engine": dev,
             "sample": f"first {cnt} of the {args.instances} workload instances in order, one at a time, "
                       f"PyTorch FP64 on cuda:{local} (torch.linalg.svd/qr + einsum per op, host loop), "
                       f"~{args.plain_seconds:.0f} s wall clock"}
+    if world == 1 and args.plain_seconds > 0:
+        _secondary(out, "plain_gpu_form", plain_leg)
     if world == 1 and not args.no_c2:
-        out["rrg200"] = c2_leg(catn, args, fp64_peak, load_bf16_peak())
+        _secondary(out, "rrg200", lambda: c2_leg(catn, args, fp64_peak, load_bf16_peak()))
     if world == 1 and args.c4_full:
-        out["gaussian_lattice_32"] = c4_full_leg(catn)
+        _secondary(out, "gaussian_lattice_32", lambda: c4_full_leg(catn))
     if world == 1 and not args.no_configs:
-        out["ferro8"] = c1_leg(catn)
-        out["gaussian_lattice_reduced"] = c4_reduced_leg(catn)
-        out["peps_reduced"] = peps_reduced_leg(catn)
+        _secondary(out, "ferro8", lambda: c1_leg(catn))
+        _secondary(out, "gaussian_lattice_reduced", lambda: c4_reduced_leg(catn))
+        _secondary(out, "peps_reduced", lambda: peps_reduced_leg(catn))
     print(json.dumps(out))
     if dist:
         dist.barrier()

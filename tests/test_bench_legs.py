@@ -99,3 +99,14 @@ def test_full_size_lattice_leg():
     out = bench.c4_full_leg(_fake([], 1.0), L=4, pin_edges=2)
     assert out["pinning_subset_networks"] == 1 + 4 * 2
     json.dumps(out)
+
+
+def test_a_failing_leg_is_recorded_not_raised():
+    out = {}
+    bench._secondary(out, "ok", lambda: {"value": 1})
+
+    def boom():
+        raise RuntimeError("device lost")
+    bench._secondary(out, "bad", boom)
+    assert out["ok"] == {"value": 1}
+    assert out["bad"] == {"error": "RuntimeError: device lost"}
