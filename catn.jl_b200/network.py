@@ -76,9 +76,9 @@ class TensorNetwork:
                 t, k = occ[0]
                 nbr[t][k] = sentinel
         self.kind = "dense"
-        self.tensors = [np.asarray(t, dtype=np.float64) for t in tensors]
         if any(np.iscomplexobj(t) for t in tensors):
             raise NotImplementedError("complex tensors are not supported by the device engine yet")
+        self.tensors = [np.asarray(t, dtype=np.float64) for t in tensors]
         self.neighbors = nbr
         self.n = n
         self.beta = 1.0
